@@ -1,0 +1,175 @@
+/*
+ * sabertooth_b200 — C ABI of the B200 (sm_100a) alignment hot path.
+ *
+ * Drop-in boundary for the reference crate raw-lab/sabertooth v0.4.0 (Rust).
+ * Each entry point names the reference function it replaces (path:line in the
+ * reference crate).  All entry points return an int status: ST_OK (0) on
+ * success, a negative ST_E* code otherwise; st_last_error() returns a
+ * thread-local message for the last failure on the calling thread.  The
+ * reference functions are infallible, so a Rust shim turns a non-zero status
+ * into a panic with that message; there is no CPU fallback.
+ *
+ * Conventions (as in the reference):
+ *   - residue codes 0..20 (A C D E F G H I K L M N P Q R S T V W Y X,
+ *     src/alphabet.rs:8-10); target codes >= 21 score 0 (src/align.rs:180-186);
+ *   - score rows are int32 [m][21] ScoreTable rows (src/align.rs:105-192);
+ *   - gap costs: a gap of length L costs open + (L-1)*extend (src/align.rs:198-223);
+ *   - every score is the exact optimal Smith-Waterman-Gotoh local score, equal
+ *     bit for bit to the reference's scalar i32 kernel (src/simd.rs:342-390).
+ *
+ * Threading: a context may be used from several host threads; calls on one
+ * context are serialised internally.  Use one context per thread (each with
+ * its own stream) for concurrent submission.
+ */
+#ifndef SABERTOOTH_B200_H
+#define SABERTOOTH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ST_OK 0
+#define ST_EINVAL -1    /* bad argument (null pointer, unknown id, size out of range) */
+#define ST_ECUDA -2     /* CUDA runtime error */
+#define ST_ENOMEM -3    /* device memory budget exceeded or allocation failure */
+#define ST_ETIMEOUT -4  /* a bounded device wait expired (error status, context stays usable) */
+#define ST_ESTATE -5    /* call order error (e.g. no database uploaded) */
+
+/* Which kernel produced a score (src/simd.rs:40-49 Kernel, extended). */
+#define ST_KERNEL_NONE 0     /* empty query or target: score 0 without a launch */
+#define ST_KERNEL_GPU16 1    /* packed 16-bit DPX kernel, exact (no cell above the headroom) */
+#define ST_KERNEL_GPU32 2    /* exact 32-bit kernel: rescore after 16-bit headroom, wide rows, gaps outside the 16-bit range, or band */
+
+typedef struct st_ctx st_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+/* hbm_budget_bytes = 0: no budget.  Replaces the rayon worker scratch set-up
+ * (src/search.rs:708-712, SimdScratch src/simd.rs:142-156). */
+st_ctx* st_init(int device, size_t hbm_budget_bytes);
+void st_shutdown(st_ctx* ctx);
+const char* st_last_error(void);
+/* Launch everything of this context on a caller-owned cudaStream_t (NULL = the context's own stream). */
+int st_set_stream(st_ctx* ctx, void* cuda_stream);
+int st_synchronize(st_ctx* ctx);
+/* Bytes of device memory the context holds. */
+int st_mem_used(st_ctx* ctx, uint64_t* bytes);
+
+/* ---- device-resident target database ----------------------------------- */
+/* Residue arena + offsets, the layout of SeedIndex::seq/all_residues
+ * (src/index.rs:1975-1979, 2324-2334) and SeqDb (src/fasta.rs).
+ * offsets has n_seqs+1 entries; sequence s is residues[offsets[s] .. offsets[s+1]). */
+int st_db_upload(st_ctx* ctx, const uint8_t* residues, const uint64_t* offsets, uint32_t n_seqs);
+int st_db_info(st_ctx* ctx, uint32_t* n_seqs, uint64_t* n_residues);
+
+/* ---- query profiles ----------------------------------------------------- */
+/* QueryProfile::from_rows (src/simd.rs:172-210) / DiagProfile::build (src/ungapped.rs:214-255):
+ * rows = int32 [m][21].  m = 0 is allowed (every score is then 0). */
+int st_profile_create(st_ctx* ctx, const int32_t* rows, uint32_t m, uint32_t* id);
+int st_profile_free(st_ctx* ctx, uint32_t id);
+/* Batch form: n_profiles profiles from one rows arena; row_offsets[k]..row_offsets[k+1]
+ * are the rows of profile k; ids written to ids[0..n_profiles). */
+int st_profiles_create(st_ctx* ctx, const int32_t* rows, const uint64_t* row_offsets, uint32_t n_profiles,
+                       uint32_t* ids);
+
+/* ---- (G) Smith-Waterman-Gotoh score -------------------------------------- */
+/* Plain per-call drop-in for QueryProfile::sw_score_with (src/simd.rs:252-292)
+ * and sw_score (src/simd.rs:245): one host target, one launch, blocking.
+ * kernel may be NULL. */
+int st_sw_score(st_ctx* ctx, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
+                int32_t* score, uint32_t* kernel);
+
+/* One alignment task of the batched form: profile id, database ordinal and an
+ * optional heuristic band (local_align_in_band, src/align.rs:954-970 with the
+ * band rule of src/align.rs:439-447): band_radius < 0 = full local alignment,
+ * else only cells with |j - i - band_center| <= band_radius (1-based i, j). */
+typedef struct {
+  uint32_t profile;
+  uint32_t target;
+  int32_t band_center;
+  int32_t band_radius;
+} st_pair;
+
+/* Batched scoring of many (profile, database target) pairs with host buffers:
+ * copies pairs in and scores out, plans (length bins + autotuned tiles), runs
+ * the persistent kernels and waits.  Replaces the per-candidate loop
+ * Engine::search_query::score_one (src/search.rs:534-577).  kernels may be NULL. */
+int st_sw_score_pairs(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* scores,
+                      uint32_t* kernels);
+
+/* Planned form over device buffers: a plan binds a pair list (copied at plan
+ * time), gap costs and device output buffers; st_plan_run replays the captured
+ * CUDA graph (asynchronous on the context stream). */
+typedef struct st_plan st_plan;
+int st_plan_create(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* d_scores,
+                   uint32_t* d_kernels, st_plan** plan);
+int st_plan_run(st_plan* plan);
+int st_plan_stats(st_plan* plan, uint64_t* cells, uint64_t* rescored_pairs, uint32_t* n_launch_classes);
+void st_plan_destroy(st_plan* plan);
+
+/* ---- (U) ungapped diagonal scoring --------------------------------------- */
+/* One diagonal of score_batch (src/ungapped.rs:265-270 Lane): database
+ * ordinal, diagonal d = target_pos - query_pos, query positions [lo, hi)
+ * inside diag_range (src/ungapped.rs:38-46). */
+typedef struct {
+  uint32_t target;
+  uint32_t lo;
+  uint32_t hi;
+  int32_t diag;
+} st_lane;
+
+/* Drop-in for ungapped::score_batch (src/ungapped.rs:285-386): out[i] =
+ * kadane_score (src/ungapped.rs:53-62) of lanes[i] against the profile.  Host
+ * buffers, blocking; any number of lanes per call. */
+int st_ungapped_score(st_ctx* ctx, uint32_t profile, const st_lane* lanes, uint32_t n, int32_t* out);
+
+/* A prefilter seed hit: query profile id, database ordinal, diagonal.  The
+ * scored window is the whole diagonal (diag_range; diag_window = 0 semantics). */
+typedef struct {
+  uint32_t query;
+  uint32_t target;
+  int32_t diag;
+} st_hit;
+
+/* Batched hits (the score_and_gate stage, src/prefilter.rs:1498-1660) with
+ * host buffers: per_hit[i] = best ungapped segment score of hit i;
+ * pair_best / pair_query / pair_target (capacity n) receive one entry per run
+ * of consecutive hits with the same (query, target), in hit order, and
+ * *n_pairs their count.  pair_* may be NULL to skip the per-pair output. */
+int st_ungapped_hits(st_ctx* ctx, const st_hit* hits, uint64_t n, int32_t* per_hit, int32_t* pair_best,
+                     uint32_t* pair_query, uint32_t* pair_target, uint64_t* n_pairs);
+/* Same over device buffers, asynchronous on the context stream (d_n_pairs is a device uint64). */
+int st_ungapped_hits_device(st_ctx* ctx, const st_hit* d_hits, uint64_t n, int32_t* d_per_hit,
+                            int32_t* d_pair_best, uint32_t* d_pair_query, uint32_t* d_pair_target,
+                            uint64_t* d_n_pairs);
+
+/* ---- tile classes and autotuning ----------------------------------------- */
+/* The packed 16-bit kernel runs in tile classes: G lanes per alignment x R
+ * query rows per lane.  A per-context table maps (query-length bin, mean
+ * target-length bin) to a class; -1 entries use the built-in cost model.
+ * Query bins: <=32, <=64, ..., <=8192, >8192 (10); target bins: <=64, <=128,
+ * ..., <=4096, >4096 (8); the table is row-major [10][8].  (No reference
+ * counterpart: the reference picks SIMD widths at run time, src/simd.rs:59-124.) */
+int st_tune_num_classes(void);
+int st_tune_class_shape(int cls, int* lanes_per_alignment, int* rows_per_lane);
+int st_tune_get(st_ctx* ctx, int32_t* table);
+int st_tune_set(st_ctx* ctx, const int32_t* table);
+/* Times every feasible class on samples (whole queries, up to max_pairs_per_bin
+ * pairs) of each length bin present in the pairs and stores the fastest. */
+int st_autotune(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                uint32_t max_pairs_per_bin, uint32_t* bins_tuned);
+
+/* ---- measurement helpers -------------------------------------------------- */
+/* Device-wide throughput of the packed s16x2 DPX add-max instruction
+ * (__viaddmax_s16x2), in lane-operations per second, measured on the current
+ * device with CUDA events (the denominator of the SW roofline). */
+int st_probe_dpx(st_ctx* ctx, double* ops_per_s);
+/* Number of kernel launches this context issued since creation. */
+int st_launch_count(st_ctx* ctx, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,63 @@
+/*
+ * CPU oracle for the Sabertooth alignment hot path — TEST INFRASTRUCTURE ONLY.
+ *
+ * This is a plain-C restatement of the reference's scalar (exact) kernels, used
+ * as the checker for the CUDA path and, in bench.py's CPU-baseline leg only, as
+ * the timed CPU baseline.  Nothing in the product (the sabertooth_b200 package
+ * or libsabertooth_b200.so) may link, import or call it.
+ *
+ * Reference (raw-lab/sabertooth v0.4.0, Rust), followed line by line:
+ *   diag_range          src/ungapped.rs:38-46
+ *   kadane_score        src/ungapped.rs:53-62
+ *   kadane_segment      src/ungapped.rs:69-88
+ *   gotoh_score_end     src/simd.rs:347-390   (scalar_gotoh_score_end, column-major-first end)
+ *   gotoh_score         src/simd.rs:252-255, 342-345 (m == 0 or empty target -> 0)
+ *   reference_score     src/simd.rs:1124-1142 and src/align.rs:1150-1166 (three full matrices)
+ *   band_score          src/align.rs:408-493  (local_full_tb with band = Some((center, radius)))
+ *
+ * Score rows are the reference's ScoreTable rows: int32 [m][21], residue codes
+ * 0..20 (A..Y, X); target codes >= 21 score 0 (src/align.rs:180-186,
+ * src/simd.rs:367-368).  Parity pins: see tests/test_oracle.py.
+ */
+#ifndef SABERTOOTH_ORACLE_H
+#define SABERTOOTH_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OR_NPROF 21
+
+void or_diag_range(uint64_t m, uint64_t n, int64_t d, uint64_t* lo, uint64_t* hi);
+int32_t or_kadane_score(const int32_t* rows, const uint8_t* t, int64_t d, uint64_t lo, uint64_t hi);
+int32_t or_kadane_segment(const int32_t* rows, const uint8_t* t, int64_t d, uint64_t lo, uint64_t hi,
+                          uint64_t* q_start, uint64_t* q_end);
+
+/* returns 1 and fills (score, query_end, target_end) when best > 0, else 0 */
+int or_gotoh_score_end(const int32_t* rows, uint32_t m, const uint8_t* t, uint32_t n, int32_t open,
+                       int32_t ext, int32_t* score, uint32_t* qi, uint32_t* tj);
+int32_t or_gotoh_score(const int32_t* rows, uint32_t m, const uint8_t* t, uint32_t n, int32_t open,
+                       int32_t ext);
+int32_t or_reference_score(const int32_t* rows, uint32_t m, const uint8_t* t, uint32_t n, int32_t open,
+                           int32_t ext);
+int32_t or_band_score(const int32_t* rows, uint32_t m, const uint8_t* t, uint32_t n, int32_t open,
+                      int32_t ext, int64_t center, int64_t radius);
+
+/* Batched forms (OpenMP over pairs) for larger parity cases.
+ * rows_arena: concatenated int32 [m_q][21] rows; row_off[q] = first row of query q; qlen[q] = m_q.
+ * tgt_arena: concatenated target codes; tgt_off[t] .. tgt_off[t+1].
+ * pair k = (pq[k], pt[k]); radius[k] < 0 -> full SW, else band (center[k], radius[k]). */
+void or_sw_pairs(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
+                 const uint8_t* tgt_arena, const uint64_t* tgt_off, const uint32_t* pq, const uint32_t* pt,
+                 const int64_t* center, const int64_t* radius, uint64_t n_pairs, int32_t open, int32_t ext,
+                 int32_t* out, int nthreads);
+
+/* hit k = (hq[k], ht[k], hd[k]); score over the whole diagonal (diag_range). */
+void or_ungapped_hits(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
+                      const uint8_t* tgt_arena, const uint64_t* tgt_off, const uint32_t* hq, const uint32_t* ht,
+                      const int32_t* hd, uint64_t n_hits, int32_t* out, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,137 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so) — TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+the checker / CPU baseline; never by the sabertooth_b200 package.  Each
+function follows the reference file:line cited in oracle.h.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+NPROF = 21
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load():
+    if not os.path.exists(LIB):
+        build()
+    lib = C.CDLL(LIB)
+    P, u32, i32, u64, i64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64, C.c_int64
+    lib.or_diag_range.argtypes = [u64, u64, i64, P, P]
+    lib.or_kadane_score.restype = i32
+    lib.or_kadane_score.argtypes = [P, P, i64, u64, u64]
+    lib.or_kadane_segment.restype = i32
+    lib.or_kadane_segment.argtypes = [P, P, i64, u64, u64, P, P]
+    lib.or_gotoh_score_end.restype = C.c_int
+    lib.or_gotoh_score_end.argtypes = [P, u32, P, u32, i32, i32, P, P, P]
+    lib.or_gotoh_score.restype = i32
+    lib.or_gotoh_score.argtypes = [P, u32, P, u32, i32, i32]
+    lib.or_reference_score.restype = i32
+    lib.or_reference_score.argtypes = [P, u32, P, u32, i32, i32]
+    lib.or_band_score.restype = i32
+    lib.or_band_score.argtypes = [P, u32, P, u32, i32, i32, i64, i64]
+    lib.or_sw_pairs.argtypes = [P, P, P, P, P, P, P, P, P, u64, i32, i32, P, C.c_int]
+    lib.or_ungapped_hits.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
+    return lib
+
+
+lib = _load()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _rows(rows):
+    return np.ascontiguousarray(rows, dtype=np.int32).reshape(-1, NPROF)
+
+
+def _t(t):
+    return np.ascontiguousarray(t, dtype=np.uint8)
+
+
+def diag_range(m, n, d):
+    lo, hi = C.c_uint64(), C.c_uint64()
+    lib.or_diag_range(m, n, d, C.byref(lo), C.byref(hi))
+    return lo.value, hi.value
+
+
+def kadane_score(rows, t, d, lo, hi):
+    r, tt = _rows(rows), _t(t)
+    return lib.or_kadane_score(_p(r), _p(tt), d, lo, hi)
+
+
+def kadane_segment(rows, t, d, lo, hi):
+    r, tt = _rows(rows), _t(t)
+    a, b = C.c_uint64(), C.c_uint64()
+    s = lib.or_kadane_segment(_p(r), _p(tt), d, lo, hi, C.byref(a), C.byref(b))
+    return s, a.value, b.value
+
+
+def gotoh_score(rows, t, open_, ext):
+    r, tt = _rows(rows), _t(t)
+    return lib.or_gotoh_score(_p(r), r.shape[0], _p(tt) if tt.size else None, tt.size, open_, ext)
+
+
+def gotoh_score_end(rows, t, open_, ext):
+    r, tt = _rows(rows), _t(t)
+    s, qi, tj = C.c_int32(), C.c_uint32(), C.c_uint32()
+    ok = lib.or_gotoh_score_end(_p(r), r.shape[0], _p(tt) if tt.size else None, tt.size, open_, ext,
+                                C.byref(s), C.byref(qi), C.byref(tj))
+    return (s.value, qi.value, tj.value) if ok else None
+
+
+def reference_score(rows, t, open_, ext):
+    r, tt = _rows(rows), _t(t)
+    return lib.or_reference_score(_p(r), r.shape[0], _p(tt) if tt.size else None, tt.size, open_, ext)
+
+
+def band_score(rows, t, open_, ext, center, radius):
+    r, tt = _rows(rows), _t(t)
+    return lib.or_band_score(_p(r), r.shape[0], _p(tt) if tt.size else None, tt.size, open_, ext, center, radius)
+
+
+class Arena:
+    """Concatenated query rows and targets, the layout of the batched oracle calls."""
+
+    def __init__(self, rows_list, targets):
+        self.qlen = np.array([len(r) for r in rows_list], dtype=np.uint32)
+        self.row_off = np.zeros(len(rows_list), dtype=np.uint64)
+        if len(rows_list) > 1:
+            self.row_off[1:] = np.cumsum(self.qlen.astype(np.uint64))[:-1]
+        parts = [_rows(r) for r in rows_list if len(r)]
+        self.rows = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros((1, NPROF), np.int32))
+        self.tgt_off = np.zeros(len(targets) + 1, dtype=np.uint64)
+        self.tgt_off[1:] = np.cumsum([len(t) for t in targets])
+        tp = [_t(t) for t in targets if len(t)]
+        self.tgt = np.ascontiguousarray(np.concatenate(tp) if tp else np.zeros(1, np.uint8))
+
+
+def sw_pairs(arena: Arena, pq, pt, open_, ext, center=None, radius=None, threads=0):
+    pq = np.ascontiguousarray(pq, dtype=np.uint32)
+    pt = np.ascontiguousarray(pt, dtype=np.uint32)
+    n = len(pq)
+    c = None if center is None else np.ascontiguousarray(center, dtype=np.int64)
+    r = None if radius is None else np.ascontiguousarray(radius, dtype=np.int64)
+    out = np.zeros(n, dtype=np.int32)
+    lib.or_sw_pairs(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(arena.tgt), _p(arena.tgt_off), _p(pq),
+                    _p(pt), _p(c), _p(r), n, open_, ext, _p(out), threads or os.cpu_count() or 1)
+    return out
+
+
+def ungapped_hits(arena: Arena, hq, ht, hd, threads=0):
+    hq = np.ascontiguousarray(hq, dtype=np.uint32)
+    ht = np.ascontiguousarray(ht, dtype=np.uint32)
+    hd = np.ascontiguousarray(hd, dtype=np.int32)
+    n = len(hq)
+    out = np.zeros(n, dtype=np.int32)
+    lib.or_ungapped_hits(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(arena.tgt), _p(arena.tgt_off),
+                         _p(hq), _p(ht), _p(hd), n, _p(out), threads or os.cpu_count() or 1)
+    return out

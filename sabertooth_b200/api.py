@@ -1,0 +1,355 @@
+"""Python mirror of the reference's hot-path interface over the C ABI.
+
+Names and argument meaning follow the reference crate (raw-lab/sabertooth
+v0.4.0): GapCosts (src/align.rs:198-223), QueryProfile.from_rows / build /
+sw_score / sw_score_with (src/simd.rs:128-292), Kernel (src/simd.rs:40-49,
+with GPU variants), diag_range / kadane_score / Lane / DiagProfile /
+score_batch (src/ungapped.rs:38-386).  Every score is computed on the GPU by
+libsabertooth_b200.so; there is no CPU path.  Targets of the batched forms
+are ordinals of the device-resident database (Context.upload_db).
+"""
+import ctypes as C
+import enum
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import HIT_DTYPE, LANE_DTYPE, PAIR_DTYPE, check, lib, ptr
+
+ALPHABET_SIZE = 21
+
+
+@dataclass(frozen=True)
+class GapCosts:
+    """A gap of length L costs open + (L-1)*extend."""
+
+    open: int
+    extend: int
+
+    @staticmethod
+    def sequence_default():
+        return GapCosts(11, 1)
+
+    @staticmethod
+    def profile_default():
+        return GapCosts(44, 4)
+
+    def cost(self, length):
+        return 0 if length == 0 else self.open + (length - 1) * self.extend
+
+
+class Kernel(enum.IntEnum):
+    """Which kernel produced a score."""
+
+    NONE = 0    # empty query or target: 0 without a launch
+    GPU16 = 1   # packed 16-bit DPX kernel (exact below its headroom)
+    GPU32 = 2   # exact 32-bit kernel (rescore, wide rows, any gap costs, band)
+
+
+def diag_range(m, n, d):
+    """Query positions [lo, hi) where diagonal d = target_pos - query_pos lies in both sequences."""
+    lo = max(-d, 0)
+    hi = min(m, n - d)
+    return (0, 0) if hi <= lo else (lo, hi)
+
+
+class Context:
+    """A device, its stream, the device-resident target database and query profiles."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0):
+        h = lib.st_init(device, hbm_budget_bytes)
+        if not h:
+            raise _lib.StError(-2, lib.st_last_error().decode())
+        self._h = C.c_void_p(h)
+        self.device = device
+        self.n_seqs = 0
+        self.db_lengths = np.zeros(0, dtype=np.uint32)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib.st_shutdown(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, cuda_stream_ptr):
+        """Launch on a caller-owned cudaStream_t (an int address, e.g. torch.cuda.Stream.cuda_stream)."""
+        check(lib.st_set_stream(self._h, C.c_void_p(cuda_stream_ptr) if cuda_stream_ptr else None))
+
+    def synchronize(self):
+        check(lib.st_synchronize(self._h))
+
+    def mem_used(self):
+        v = C.c_uint64()
+        check(lib.st_mem_used(self._h, C.byref(v)))
+        return v.value
+
+    def launch_count(self):
+        v = C.c_uint64()
+        check(lib.st_launch_count(self._h, C.byref(v)))
+        return v.value
+
+    # -- database ---------------------------------------------------------
+    def upload_db(self, residues, offsets):
+        """residues: uint8 codes; offsets: n_seqs+1 uint64 (sequence s = residues[offsets[s]:offsets[s+1]])."""
+        residues = np.ascontiguousarray(residues, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        n = len(offsets) - 1
+        check(lib.st_db_upload(self._h, ptr(residues) if residues.size else None, ptr(offsets), n))
+        self.n_seqs = n
+        self.db_lengths = np.diff(offsets).astype(np.uint32)
+
+    def upload_db_list(self, seqs):
+        offs = np.zeros(len(seqs) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([len(s) for s in seqs])
+        res = np.concatenate([np.asarray(s, dtype=np.uint8) for s in seqs]) if seqs else np.zeros(0, np.uint8)
+        self.upload_db(res, offs)
+
+    # -- profiles -----------------------------------------------------------
+    def create_profiles(self, rows_list):
+        """Profiles from a list of int32 [m][21] row arrays; returns their ids."""
+        if not rows_list:
+            return np.zeros(0, dtype=np.uint32)
+        arrs = [np.ascontiguousarray(r, dtype=np.int32).reshape(-1, ALPHABET_SIZE) for r in rows_list]
+        offs = np.zeros(len(arrs) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([a.shape[0] for a in arrs])
+        arena = np.concatenate(arrs, axis=0) if offs[-1] else np.zeros((1, ALPHABET_SIZE), np.int32)
+        arena = np.ascontiguousarray(arena)
+        ids = np.zeros(len(arrs), dtype=np.uint32)
+        check(lib.st_profiles_create(self._h, ptr(arena), ptr(offs), len(arrs), ptr(ids)))
+        return ids
+
+    def free_profile(self, pid):
+        check(lib.st_profile_free(self._h, int(pid)))
+
+    # -- (G) batched -------------------------------------------------------
+    def sw_score_pairs(self, pairs, gaps: GapCosts, with_kernels=False):
+        """Scores of many (profile, db target[, band]) pairs; host buffers in and out."""
+        pairs = as_pairs(pairs)
+        n = len(pairs)
+        scores = np.zeros(n, dtype=np.int32)
+        kernels = np.zeros(n, dtype=np.uint32) if with_kernels else None
+        if n:
+            check(lib.st_sw_score_pairs(self._h, ptr(pairs), n, gaps.open, gaps.extend, ptr(scores),
+                                        ptr(kernels)))
+        return (scores, kernels) if with_kernels else scores
+
+    def plan(self, pairs, gaps: GapCosts, d_scores, d_kernels=None):
+        return Plan(self, pairs, gaps, d_scores, d_kernels)
+
+    # -- (U) ---------------------------------------------------------------
+    def ungapped_hits(self, hits, with_pairs=True):
+        """Per-hit best ungapped segment score, and per (query, target) run: (best, query, target)."""
+        hits = as_hits(hits)
+        n = len(hits)
+        per_hit = np.zeros(n, dtype=np.int32)
+        if not with_pairs:
+            check(lib.st_ungapped_hits(self._h, ptr(hits), n, ptr(per_hit), None, None, None, None))
+            return per_hit
+        pb = np.zeros(max(n, 1), dtype=np.int32)
+        pq = np.zeros(max(n, 1), dtype=np.uint32)
+        pt = np.zeros(max(n, 1), dtype=np.uint32)
+        npairs = C.c_uint64()
+        check(lib.st_ungapped_hits(self._h, ptr(hits), n, ptr(per_hit), ptr(pb), ptr(pq), ptr(pt),
+                                   C.byref(npairs)))
+        k = npairs.value
+        return per_hit, (pb[:k].copy(), pq[:k].copy(), pt[:k].copy())
+
+    def ungapped_hits_device(self, d_hits_ptr, n, d_per_hit_ptr, d_pair_best=None, d_pair_query=None,
+                             d_pair_target=None, d_n_pairs=None):
+        check(lib.st_ungapped_hits_device(self._h, C.c_void_p(d_hits_ptr), n, C.c_void_p(d_per_hit_ptr),
+                                          _vp(d_pair_best), _vp(d_pair_query), _vp(d_pair_target),
+                                          _vp(d_n_pairs)))
+
+    # -- tuning / measurement ---------------------------------------------------
+    def autotune(self, pairs, gaps: GapCosts, max_pairs_per_bin=4096):
+        pairs = as_pairs(pairs)
+        nb = C.c_uint32()
+        check(lib.st_autotune(self._h, ptr(pairs), len(pairs), gaps.open, gaps.extend, max_pairs_per_bin,
+                              C.byref(nb)))
+        return nb.value
+
+    def tuning_table(self):
+        t = np.zeros((10, 8), dtype=np.int32)
+        check(lib.st_tune_get(self._h, ptr(t)))
+        return t
+
+    def set_tuning_table(self, table):
+        t = np.ascontiguousarray(table, dtype=np.int32).reshape(10, 8)
+        check(lib.st_tune_set(self._h, ptr(t)))
+
+    def probe_dpx(self):
+        v = C.c_double()
+        check(lib.st_probe_dpx(self._h, C.byref(v)))
+        return v.value
+
+
+def _vp(x):
+    return C.c_void_p(x) if x else None
+
+
+def tile_classes():
+    out = []
+    for c in range(lib.st_tune_num_classes()):
+        g, r = C.c_int(), C.c_int()
+        check(lib.st_tune_class_shape(c, C.byref(g), C.byref(r)))
+        out.append((g.value, r.value))
+    return out
+
+
+def as_pairs(pairs):
+    if isinstance(pairs, np.ndarray) and pairs.dtype == PAIR_DTYPE:
+        return np.ascontiguousarray(pairs)
+    arr = np.zeros(len(pairs), dtype=PAIR_DTYPE)
+    for i, p in enumerate(pairs):
+        prof, tgt = p[0], p[1]
+        c, r = (p[2], p[3]) if len(p) > 2 else (0, -1)
+        arr[i] = (prof, tgt, c, r)
+    return arr
+
+
+def as_hits(hits):
+    if isinstance(hits, np.ndarray) and hits.dtype == HIT_DTYPE:
+        return np.ascontiguousarray(hits)
+    arr = np.zeros(len(hits), dtype=HIT_DTYPE)
+    for i, h in enumerate(hits):
+        arr[i] = tuple(h)
+    return arr
+
+
+class Plan:
+    """A captured batch over device buffers (d_scores / d_kernels: device pointers as ints)."""
+
+    def __init__(self, ctx: Context, pairs, gaps: GapCosts, d_scores, d_kernels=None):
+        pairs = as_pairs(pairs)
+        self.ctx = ctx
+        self.n = len(pairs)
+        h = C.c_void_p()
+        check(lib.st_plan_create(ctx.handle, ptr(pairs), self.n, gaps.open, gaps.extend, C.c_void_p(d_scores),
+                                 _vp(d_kernels), C.byref(h)))
+        self._h = h
+
+    def run(self):
+        check(lib.st_plan_run(self._h))
+
+    def stats(self):
+        cells, resc, ncls = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        check(lib.st_plan_stats(self._h, C.byref(cells), C.byref(resc), C.byref(ncls)))
+        return {"cells": cells.value, "rescored_pairs": resc.value, "launch_classes": ncls.value}
+
+    def close(self):
+        if self._h:
+            lib.st_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# -- process-wide default context (like the reference's process-wide kernel choice) --
+_default = None
+_default_lock = threading.Lock()
+
+
+def default_context() -> Context:
+    global _default
+    with _default_lock:
+        if _default is None:
+            _default = Context(0)
+        return _default
+
+
+class QueryProfile:
+    """A query (sequence or PSSM) prepared for repeated scoring (src/simd.rs:128-139)."""
+
+    def __init__(self, rows, ctx: Context = None):
+        self.ctx = ctx or default_context()
+        self._rows = np.ascontiguousarray(rows, dtype=np.int32).reshape(-1, ALPHABET_SIZE)
+        self.m = self._rows.shape[0]
+        self.id = int(self.ctx.create_profiles([self._rows])[0])
+
+    @staticmethod
+    def from_rows(rows, ctx: Context = None):
+        return QueryProfile(rows, ctx)
+
+    @staticmethod
+    def build(scorer_rows, ctx: Context = None):
+        return QueryProfile(scorer_rows, ctx)
+
+    def query_len(self):
+        return self.m
+
+    def rows(self):
+        return self._rows
+
+    def sw_score(self, target, gaps: GapCosts) -> int:
+        return self.sw_score_with(target, gaps)[0]
+
+    def sw_score_with(self, target, gaps: GapCosts, scratch=None):
+        """(score, Kernel) of one host target: the plain per-call drop-in."""
+        t = np.ascontiguousarray(target, dtype=np.uint8)
+        s, k = C.c_int32(), C.c_uint32()
+        check(lib.st_sw_score(self.ctx.handle, self.id, ptr(t) if t.size else None, t.size, gaps.open,
+                              gaps.extend, C.byref(s), C.byref(k)))
+        return s.value, Kernel(k.value)
+
+    def free(self):
+        self.ctx.free_profile(self.id)
+
+
+@dataclass
+class Lane:
+    """One diagonal: database ordinal of the target, diagonal, query window [lo, hi)."""
+
+    target: int
+    diag: int
+    lo: int
+    hi: int
+
+
+class DiagProfile:
+    """Ungapped scoring profile of a query (src/ungapped.rs:188-255); any score range works on the GPU."""
+
+    def __init__(self, qp: QueryProfile):
+        self.qp = qp
+
+    @staticmethod
+    def build(rows, ctx: Context = None):
+        if len(rows) == 0:
+            return None  # the reference refuses empty profiles too (src/ungapped.rs:225)
+        return DiagProfile(QueryProfile(rows, ctx))
+
+    def query_len(self):
+        return self.qp.m
+
+
+def score_batch(prof: DiagProfile, lanes, out=None):
+    """out[i] = best ungapped segment score of lanes[i] (src/ungapped.rs:285-386), any number of lanes."""
+    n = len(lanes)
+    arr = np.zeros(n, dtype=LANE_DTYPE)
+    for i, l in enumerate(lanes):
+        arr[i] = (l.target, l.lo, l.hi, l.diag)
+    res = np.zeros(n, dtype=np.int32)
+    if n:
+        check(lib.st_ungapped_score(prof.qp.ctx.handle, prof.qp.id, ptr(arr), n, ptr(res)))
+    if out is not None:
+        out[:n] = res
+    return res
+
+
+def kadane_score(prof: DiagProfile, target, d, lo, hi) -> int:
+    """Best ungapped segment of one diagonal window (src/ungapped.rs:53-62), on the GPU."""
+    return int(score_batch(prof, [Lane(target, d, lo, hi)])[0])

@@ -1,0 +1,1334 @@
+// Runtime behind the C ABI (include/sabertooth_b200.h): context, device-resident
+// target database and query profiles, the batch planner (length bins, tile
+// classes, persistent-kernel work lists, CUDA-graph capture) and the plain
+// per-call paths that replace the reference's QueryProfile::sw_score_with and
+// ungapped::score_batch.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/sabertooth_b200.h"
+#include "st_common.cuh"
+#include "st_sw16.cuh"
+#include "st_sw32.cuh"
+#include "st_tuning.h"
+#include "st_ungapped.cuh"
+
+using namespace st;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define ST_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return fail(ST_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                       __FILE__, __LINE__);                                        \
+  } while (0)
+
+#define ST_TRY(expr)          \
+  do {                        \
+    int r_ = (expr);          \
+    if (r_ != ST_OK) return r_; \
+  } while (0)
+
+extern "C" const char* st_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------------------
+// device memory with budget accounting
+// ---------------------------------------------------------------------------
+struct MemTracker {
+  size_t used = 0;
+  size_t budget = 0;  // 0 = unlimited
+};
+
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  MemTracker* mt = nullptr;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  DevMem(DevMem&& o) noexcept { *this = std::move(o); }
+  DevMem& operator=(DevMem&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      bytes = o.bytes;
+      mt = o.mt;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevMem() { release(); }
+  void release() {
+    if (p) {
+      cudaFree(p);
+      if (mt) mt->used -= bytes;
+    }
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+static int dev_alloc(MemTracker* mt, DevMem& m, size_t bytes) {
+  m.release();
+  if (bytes == 0) bytes = 16;
+  if (mt->budget && mt->used + bytes > mt->budget)
+    return fail(ST_ENOMEM, "device memory budget exceeded: %zu used + %zu requested > %zu budget", mt->used,
+                bytes, mt->budget);
+  cudaError_t e = cudaMalloc(&m.p, bytes);
+  if (e != cudaSuccess) {
+    m.p = nullptr;
+    return fail(ST_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  m.bytes = bytes;
+  m.mt = mt;
+  mt->used += bytes;
+  return ST_OK;
+}
+
+// pinned host staging buffer that only grows
+struct Pinned {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~Pinned() {
+    if (p) cudaFreeHost(p);
+  }
+  int reserve(size_t n) {
+    if (n <= bytes) return ST_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(n, 1 << 20);
+    ST_CUDA(cudaMallocHost(&p, want));
+    bytes = want;
+    return ST_OK;
+  }
+  template <class T>
+  T* as(size_t off = 0) const {
+    return reinterpret_cast<T*>(static_cast<char*>(p) + off);
+  }
+};
+
+static inline size_t up16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+static inline size_t up256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// ---------------------------------------------------------------------------
+// kernel classes
+// ---------------------------------------------------------------------------
+constexpr int kWarps16 = 8;
+constexpr int kWarps32 = 4;
+constexpr int kMaxSmem = 226 * 1024;  // dynamic shared memory per CTA (the 227 KB opt-in less room for static shared)
+
+using Sw16Fn = void (*)(const Sw16Params);
+
+struct Sw16Class {
+  int G, R;
+  Sw16Fn fn;
+};
+
+#define ST_CLASS(g, r) {g, r, sw16_kernel<g, r, kWarps16>}
+static const Sw16Class kClasses[] = {
+    ST_CLASS(4, 8),  ST_CLASS(8, 8),  ST_CLASS(16, 8),  ST_CLASS(32, 8),  ST_CLASS(4, 16), ST_CLASS(8, 16),
+    ST_CLASS(16, 16), ST_CLASS(32, 16), ST_CLASS(4, 32), ST_CLASS(8, 32), ST_CLASS(16, 32), ST_CLASS(32, 32),
+};
+#undef ST_CLASS
+constexpr int kNumClasses = sizeof(kClasses) / sizeof(kClasses[0]);
+
+int st_tuning_num_classes() { return kNumClasses; }
+void st_tuning_class_shape(int c, int* G, int* R) {
+  *G = kClasses[c].G;
+  *R = kClasses[c].R;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct ProfileBlock {
+  DevMem mem;
+  uint32_t live = 0;
+};
+
+struct ProfileMeta {
+  uint32_t m = 0;
+  int32_t max_score = 0;
+  bool fits8 = false;
+  bool live = false;
+  int block = -1;
+  const int8_t* p8 = nullptr;
+  const int32_t* p32 = nullptr;
+  uint32_t stride8 = 0, stride32 = 0;
+};
+
+struct st_ctx {
+  int device = 0;
+  int sms = 0;
+  MemTracker mt;
+  cudaStream_t own = nullptr;     // the context's stream (also used for graph capture)
+  cudaStream_t stream = nullptr;  // where work is launched
+  std::recursive_mutex mu;
+  uint64_t launches = 0;
+  // database
+  DevMem db_arena, db_off, db_len;
+  std::vector<uint32_t> h_db_len;
+  uint32_t n_seqs = 0;
+  uint64_t n_res = 0;
+  bool has_db = false;
+  // profiles
+  std::vector<ProfileMeta> profs;
+  std::vector<std::unique_ptr<ProfileBlock>> blocks;
+  DevMem d_p8, d_p32, d_stride8, d_stride32, d_qlen, d_maxs, d_fits8;
+  bool prof_dirty = true;
+  uint32_t max_m = 0;
+  // staging for the per-call paths
+  Pinned pin;
+  DevMem stage;
+  DevMem scratch_small;
+  Tuning tuning;
+};
+
+static DeviceDb db_view(st_ctx* c) {
+  DeviceDb d;
+  d.arena = c->db_arena.as<uint8_t>();
+  d.offset = c->db_off.as<uint64_t>();
+  d.length = c->db_len.as<uint32_t>();
+  d.n_seqs = c->n_seqs;
+  return d;
+}
+
+static int sync_profiles(st_ctx* c) {
+  if (!c->prof_dirty) return ST_OK;
+  const size_t n = std::max<size_t>(c->profs.size(), 1);
+  std::vector<const int8_t*> p8(n, nullptr);
+  std::vector<const int32_t*> p32(n, nullptr);
+  std::vector<uint32_t> s8(n, 0), s32(n, 0), ql(n, 0);
+  std::vector<int32_t> mx(n, 0);
+  std::vector<uint8_t> f8(n, 0);
+  uint32_t max_m = 0;
+  for (size_t i = 0; i < c->profs.size(); ++i) {
+    const ProfileMeta& p = c->profs[i];
+    if (!p.live) continue;
+    p8[i] = p.p8;
+    p32[i] = p.p32;
+    s8[i] = p.stride8;
+    s32[i] = p.stride32;
+    ql[i] = p.m;
+    mx[i] = p.max_score;
+    f8[i] = p.fits8 ? 1 : 0;
+    max_m = std::max(max_m, p.m);
+  }
+  auto up = [&](DevMem& d, const void* src, size_t bytes) -> int {
+    if (d.bytes < bytes) ST_TRY(dev_alloc(&c->mt, d, bytes * 2));
+    ST_CUDA(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, c->own));
+    return ST_OK;
+  };
+  ST_TRY(up(c->d_p8, p8.data(), n * sizeof(void*)));
+  ST_TRY(up(c->d_p32, p32.data(), n * sizeof(void*)));
+  ST_TRY(up(c->d_stride8, s8.data(), n * 4));
+  ST_TRY(up(c->d_stride32, s32.data(), n * 4));
+  ST_TRY(up(c->d_qlen, ql.data(), n * 4));
+  ST_TRY(up(c->d_maxs, mx.data(), n * 4));
+  ST_TRY(up(c->d_fits8, f8.data(), n));
+  ST_CUDA(cudaStreamSynchronize(c->own));
+  c->max_m = max_m;
+  c->prof_dirty = false;
+  return ST_OK;
+}
+
+static DeviceProfiles prof_view(st_ctx* c) {
+  DeviceProfiles p;
+  p.p8 = c->d_p8.as<const int8_t* const>();
+  p.p32 = c->d_p32.as<const int32_t* const>();
+  p.stride8 = c->d_stride8.as<uint32_t>();
+  p.stride32 = c->d_stride32.as<uint32_t>();
+  p.qlen = c->d_qlen.as<uint32_t>();
+  p.max_score = c->d_maxs.as<int32_t>();
+  p.fits8 = c->d_fits8.as<uint8_t>();
+  return p;
+}
+
+static int set_smem_limits() {
+  for (int i = 0; i < kNumClasses; ++i)
+    ST_CUDA(cudaFuncSetAttribute(kClasses[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+  ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+  ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+  return ST_OK;
+}
+
+extern "C" st_ctx* st_init(int device, size_t hbm_budget_bytes) {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    fail(ST_ECUDA, "no CUDA device available: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (device < 0 || device >= ndev) {
+    fail(ST_EINVAL, "device %d out of range (have %d)", device, ndev);
+    return nullptr;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    fail(ST_ECUDA, "cudaSetDevice(%d) failed", device);
+    return nullptr;
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  if (prop.major < 10) {
+    fail(ST_ECUDA, "device %d is sm_%d%d; this library is built for sm_100a (B200)", device, prop.major,
+         prop.minor);
+    return nullptr;
+  }
+  auto c = std::make_unique<st_ctx>();
+  c->device = device;
+  c->sms = prop.multiProcessorCount;
+  c->mt.budget = hbm_budget_bytes;
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+    fail(ST_ECUDA, "cudaStreamCreate failed");
+    return nullptr;
+  }
+  c->stream = c->own;
+  if (set_smem_limits() != ST_OK) return nullptr;
+  tuning_defaults(&c->tuning);
+  return c.release();
+}
+
+extern "C" void st_shutdown(st_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaStreamSynchronize(c->own);
+  cudaStream_t own = c->own;
+  delete c;
+  cudaStreamDestroy(own);
+}
+
+#define CTX_GUARD(c)                                               \
+  if (!(c)) return fail(ST_EINVAL, "null context");                \
+  std::lock_guard<std::recursive_mutex> lk_((c)->mu);              \
+  do {                                                             \
+    if (cudaSetDevice((c)->device) != cudaSuccess)                 \
+      return fail(ST_ECUDA, "cudaSetDevice(%d) failed", (c)->device); \
+  } while (0)
+
+extern "C" int st_set_stream(st_ctx* c, void* s) {
+  CTX_GUARD(c);
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own;
+  return ST_OK;
+}
+
+extern "C" int st_synchronize(st_ctx* c) {
+  CTX_GUARD(c);
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->own));
+  return ST_OK;
+}
+
+extern "C" int st_mem_used(st_ctx* c, uint64_t* bytes) {
+  CTX_GUARD(c);
+  if (!bytes) return fail(ST_EINVAL, "null output");
+  *bytes = c->mt.used;
+  return ST_OK;
+}
+
+extern "C" int st_launch_count(st_ctx* c, uint64_t* launches) {
+  CTX_GUARD(c);
+  if (!launches) return fail(ST_EINVAL, "null output");
+  *launches = c->launches;
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// database
+// ---------------------------------------------------------------------------
+extern "C" int st_db_upload(st_ctx* c, const uint8_t* residues, const uint64_t* offsets, uint32_t n_seqs) {
+  CTX_GUARD(c);
+  if (!offsets || (!residues && n_seqs && offsets[n_seqs] > offsets[0]))
+    return fail(ST_EINVAL, "st_db_upload: null input");
+  std::vector<uint64_t> off(n_seqs + 1);
+  std::vector<uint32_t> len(n_seqs);
+  uint64_t total = 0;
+  for (uint32_t s = 0; s < n_seqs; ++s) {
+    if (offsets[s + 1] < offsets[s]) return fail(ST_EINVAL, "st_db_upload: offsets decrease at %u", s);
+    const uint64_t l = offsets[s + 1] - offsets[s];
+    if (l >= (1ull << 31)) return fail(ST_EINVAL, "st_db_upload: sequence %u longer than 2^31", s);
+    off[s] = total;
+    len[s] = static_cast<uint32_t>(l);
+    total += up16(l);
+  }
+  off[n_seqs] = total;
+  const size_t arena_bytes = total + 32;
+  ST_TRY(c->pin.reserve(arena_bytes));
+  uint8_t* h = c->pin.as<uint8_t>();
+  memset(h, kSentinel, arena_bytes);
+  for (uint32_t s = 0; s < n_seqs; ++s) {
+    const uint8_t* src = residues + offsets[s];
+    uint8_t* dst = h + off[s];
+    for (uint32_t i = 0; i < len[s]; ++i) dst[i] = src[i] < kSentinel ? src[i] : kSentinel;
+  }
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  ST_TRY(dev_alloc(&c->mt, c->db_arena, arena_bytes));
+  ST_TRY(dev_alloc(&c->mt, c->db_off, (n_seqs + 1) * sizeof(uint64_t)));
+  ST_TRY(dev_alloc(&c->mt, c->db_len, std::max<size_t>(n_seqs, 1) * sizeof(uint32_t)));
+  ST_CUDA(cudaMemcpyAsync(c->db_arena.p, h, arena_bytes, cudaMemcpyHostToDevice, c->own));
+  ST_CUDA(cudaMemcpyAsync(c->db_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, c->own));
+  if (n_seqs) ST_CUDA(cudaMemcpyAsync(c->db_len.p, len.data(), len.size() * 4, cudaMemcpyHostToDevice, c->own));
+  ST_CUDA(cudaStreamSynchronize(c->own));
+  c->h_db_len = std::move(len);
+  c->n_seqs = n_seqs;
+  c->n_res = offsets[n_seqs] - offsets[0];
+  c->has_db = true;
+  return ST_OK;
+}
+
+extern "C" int st_db_info(st_ctx* c, uint32_t* n_seqs, uint64_t* n_residues) {
+  CTX_GUARD(c);
+  if (n_seqs) *n_seqs = c->n_seqs;
+  if (n_residues) *n_residues = c->n_res;
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// profiles
+// ---------------------------------------------------------------------------
+// Builds the residue-major int8 and int32 layouts from int32 [m][21] rows.
+__global__ void build_profile_kernel(const int32_t* rows, uint32_t m, int8_t* p8, uint32_t stride8, int32_t* p32,
+                                     uint32_t stride32, int fits8) {
+  const uint32_t total = kProfRows * stride32;
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const uint32_t r = idx / stride32;
+    const uint32_t i = idx - r * stride32;
+    const int32_t v = (i < m && r < static_cast<uint32_t>(kAlpha)) ? rows[static_cast<size_t>(i) * kAlpha + r] : 0;
+    p32[idx] = v;
+    if (i < stride8) p8[static_cast<size_t>(r) * stride8 + i] = fits8 ? static_cast<int8_t>(v) : 0;
+  }
+}
+
+extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t* row_offsets, uint32_t n_profiles,
+                                  uint32_t* ids) {
+  CTX_GUARD(c);
+  if (!row_offsets || !ids || (!rows && n_profiles && row_offsets[n_profiles] > row_offsets[0]))
+    return fail(ST_EINVAL, "st_profiles_create: null input");
+  struct Item {
+    uint32_t m, stride8, stride32;
+    int32_t mx;
+    bool fits8;
+    size_t o8, o32, orows;
+  };
+  std::vector<Item> it(n_profiles);
+  size_t bytes8 = 0, bytes32 = 0, rows_total = 0;
+  for (uint32_t k = 0; k < n_profiles; ++k) {
+    if (row_offsets[k + 1] < row_offsets[k]) return fail(ST_EINVAL, "st_profiles_create: offsets decrease");
+    const uint64_t m = row_offsets[k + 1] - row_offsets[k];
+    if (m > (1u << 20)) return fail(ST_EINVAL, "st_profiles_create: query of %llu rows exceeds 2^20",
+                                    static_cast<unsigned long long>(m));
+    Item& x = it[k];
+    x.m = static_cast<uint32_t>(m);
+    int32_t lo = 0, hi = 0;  // residues >= 21 score 0
+    const int32_t* r = rows + row_offsets[k] * kAlpha;
+    for (size_t i = 0; i < m * kAlpha; ++i) {
+      lo = std::min(lo, r[i]);
+      hi = std::max(hi, r[i]);
+    }
+    x.mx = hi;
+    x.fits8 = lo >= -128 && hi <= 127;
+    x.stride8 = static_cast<uint32_t>(std::max<size_t>(up16(m), 16));
+    x.stride32 = static_cast<uint32_t>(std::max<size_t>(up256(m), kSw32Rows));
+    x.o8 = bytes8;
+    bytes8 += up16(static_cast<size_t>(kProfRows) * x.stride8);
+    x.o32 = bytes32;
+    bytes32 += static_cast<size_t>(kProfRows) * x.stride32 * 4;
+    x.orows = rows_total;
+    rows_total += m;
+  }
+  auto blk = std::make_unique<ProfileBlock>();
+  const size_t src_bytes = rows_total * kAlpha * 4;
+  ST_TRY(dev_alloc(&c->mt, blk->mem, bytes32 + bytes8 + src_bytes + 64));
+  char* base = blk->mem.as<char>();
+  int32_t* d_src = reinterpret_cast<int32_t*>(base + bytes32 + bytes8);
+  if (src_bytes)
+    ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->own));
+  for (uint32_t k = 0; k < n_profiles; ++k) {
+    const Item& x = it[k];
+    int32_t* p32 = reinterpret_cast<int32_t*>(base + x.o32);
+    int8_t* p8 = reinterpret_cast<int8_t*>(base + bytes32 + x.o8);
+    const uint32_t total = kProfRows * x.stride32;
+    const int grid = std::min<uint32_t>((total + 255) / 256, 1024);
+    build_profile_kernel<<<grid, 256, 0, c->own>>>(d_src + x.orows * kAlpha, x.m, p8, x.stride8, p32, x.stride32,
+                                                    x.fits8 ? 1 : 0);
+    ++c->launches;
+  }
+  ST_CUDA(cudaGetLastError());
+  ST_CUDA(cudaStreamSynchronize(c->own));
+  const int bi = static_cast<int>(c->blocks.size());
+  for (uint32_t k = 0; k < n_profiles; ++k) {
+    const Item& x = it[k];
+    ProfileMeta pm;
+    pm.m = x.m;
+    pm.max_score = x.mx;
+    pm.fits8 = x.fits8;
+    pm.live = true;
+    pm.block = bi;
+    pm.p32 = reinterpret_cast<const int32_t*>(base + x.o32);
+    pm.p8 = reinterpret_cast<const int8_t*>(base + bytes32 + x.o8);
+    pm.stride8 = x.stride8;
+    pm.stride32 = x.stride32;
+    ids[k] = static_cast<uint32_t>(c->profs.size());
+    c->profs.push_back(pm);
+  }
+  blk->live = n_profiles;
+  c->blocks.push_back(std::move(blk));
+  c->prof_dirty = true;
+  return ST_OK;
+}
+
+extern "C" int st_profile_create(st_ctx* c, const int32_t* rows, uint32_t m, uint32_t* id) {
+  const uint64_t off[2] = {0, m};
+  return st_profiles_create(c, rows, off, 1, id);
+}
+
+extern "C" int st_profile_free(st_ctx* c, uint32_t id) {
+  CTX_GUARD(c);
+  if (id >= c->profs.size() || !c->profs[id].live) return fail(ST_EINVAL, "unknown profile id %u", id);
+  ProfileMeta& p = c->profs[id];
+  p.live = false;
+  ProfileBlock* b = c->blocks[p.block].get();
+  if (--b->live == 0) {
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    b->mem.release();
+  }
+  c->prof_dirty = true;
+  return ST_OK;
+}
+
+static int check_profile(st_ctx* c, uint32_t id) {
+  if (id >= c->profs.size() || !c->profs[id].live) return fail(ST_EINVAL, "unknown profile id %u", id);
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------
+static inline bool gaps16_ok(int32_t open, int32_t ext) {
+  // E, F >= -open-ext and H - open >= -open must stay inside int16
+  return open >= 0 && ext >= 0 && static_cast<int64_t>(open) + ext <= 16384;
+}
+
+static uint64_t band_cells(uint32_t m, uint32_t n, int64_t center, int64_t radius) {
+  // cells (i, j), 1-based, with |j - i - center| <= radius
+  uint64_t cells = 0;
+  for (uint32_t i = 1; i <= m; ++i) {
+    const int64_t lo = std::max<int64_t>(1, i + center - radius);
+    const int64_t hi = std::min<int64_t>(n, i + center + radius);
+    if (hi >= lo) cells += static_cast<uint64_t>(hi - lo + 1);
+  }
+  return cells;
+}
+
+struct ClassPlan {
+  int cls = -1;
+  std::vector<Sw16CtaTask> cta;
+  std::vector<Sw16WarpTask> wt;
+  std::vector<uint32_t> slots;
+  DevMem d_cta, d_wt, d_slots, d_scratch;
+  uint32_t grid = 0;
+  uint32_t smem = 0;
+  uint32_t scratch_stride = 0;
+};
+
+struct st_plan {
+  st_ctx* ctx = nullptr;
+  uint64_t n = 0;
+  int32_t open = 0, ext = 0;
+  int32_t* d_scores = nullptr;
+  uint32_t* d_kernels = nullptr;
+  std::vector<ClassPlan> classes;
+  DevMem d_pair_q, d_pair_t, d_pair_c, d_pair_r;
+  DevMem d_list, d_counters, d_counters_init, d_scratch32;
+  uint32_t n_static32 = 0;
+  uint32_t grid32 = 0, scratch32_stride = 0;
+  uint64_t cells = 0;
+  uint32_t kernels_per_run = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static int occupancy_grid(st_ctx* c, const void* fn, int threads, size_t smem, uint32_t work, uint32_t* grid) {
+  int nb = 0;
+  ST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem));
+  if (nb < 1) return fail(ST_EINVAL, "kernel does not fit on an SM (smem %zu)", smem);
+  *grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(static_cast<uint64_t>(nb) * c->sms, work)));
+  return ST_OK;
+}
+
+// Shape of the work for one query in one class: warp tasks of S = 64/G targets
+// (two per lane group), targets in descending length.
+static void emit_query(ClassPlan& cp, const Sw16Class& k, uint32_t q, uint32_t m, const std::vector<uint32_t>& pairs,
+                       const std::vector<uint32_t>& tlen, uint32_t max_wt_per_cta) {
+  const uint32_t S = 64 / k.G;
+  const uint32_t rows = static_cast<uint32_t>(k.G * k.R);
+  const uint32_t P = std::max<uint32_t>(1, (m + rows - 1) / rows);
+  const uint32_t m_pad = P * rows;
+  uint32_t first_wt = static_cast<uint32_t>(cp.wt.size());
+  for (size_t i = 0; i < pairs.size(); i += S) {
+    Sw16WarpTask w;
+    w.slot_begin = static_cast<uint32_t>(cp.slots.size());
+    uint32_t ncols = 32;
+    for (uint32_t s = 0; s < S; ++s) {
+      const size_t j = i + s;
+      if (j < pairs.size()) {
+        cp.slots.push_back(pairs[j]);
+        ncols = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(tlen[j])));
+      } else {
+        cp.slots.push_back(kNoPair);
+      }
+    }
+    w.ncols = ncols;
+    cp.wt.push_back(w);
+    const uint32_t done = static_cast<uint32_t>(cp.wt.size()) - first_wt;
+    if (done == max_wt_per_cta || i + S >= pairs.size()) {
+      Sw16CtaTask t;
+      t.query = q;
+      t.wt_begin = first_wt;
+      t.wt_end = static_cast<uint32_t>(cp.wt.size());
+      t.m_pad = m_pad;
+      cp.cta.push_back(t);
+      first_wt = static_cast<uint32_t>(cp.wt.size());
+    }
+  }
+}
+
+static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* d_scores,
+                      uint32_t* d_kernels, st_plan** out) {
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  if (n > 0xFFFFFFF0ull) return fail(ST_EINVAL, "too many pairs (%llu)", static_cast<unsigned long long>(n));
+  ST_TRY(sync_profiles(c));
+  auto plan = std::make_unique<st_plan>();
+  plan->ctx = c;
+  plan->n = n;
+  plan->open = open;
+  plan->ext = ext;
+  plan->d_scores = d_scores;
+  plan->d_kernels = d_kernels;
+  const bool g16 = gaps16_ok(open, ext);
+
+  std::vector<uint32_t> pq(n), pt(n);
+  std::vector<int32_t> pc(n), pr(n);
+  std::vector<uint32_t> list32;
+  // per query: pairs for the 16-bit kernel
+  std::vector<std::vector<uint32_t>> byq(c->profs.size());
+  uint32_t max_len = 0, max_m32 = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const st_pair& p = pairs[i];
+    if (p.profile >= c->profs.size() || !c->profs[p.profile].live)
+      return fail(ST_EINVAL, "pair %llu: unknown profile id %u", static_cast<unsigned long long>(i), p.profile);
+    if (p.target >= c->n_seqs)
+      return fail(ST_EINVAL, "pair %llu: target %u outside the database (%u sequences)",
+                  static_cast<unsigned long long>(i), p.target, c->n_seqs);
+    pq[i] = p.profile;
+    pt[i] = p.target;
+    pc[i] = p.band_center;
+    pr[i] = p.band_radius;
+    const ProfileMeta& pm = c->profs[p.profile];
+    const uint32_t tl = c->h_db_len[p.target];
+    if (pm.m == 0 || tl == 0) continue;  // score 0, kernel NONE
+    max_len = std::max(max_len, tl);
+    if (p.band_radius >= 0) {
+      plan->cells += band_cells(pm.m, tl, p.band_center, p.band_radius);
+      list32.push_back(static_cast<uint32_t>(i));
+      max_m32 = std::max(max_m32, pm.m);
+    } else {
+      plan->cells += static_cast<uint64_t>(pm.m) * tl;
+      // every 16-bit pair may be rescored in 32 bits
+      max_m32 = std::max(max_m32, pm.m);
+      if (g16 && pm.fits8)
+        byq[p.profile].push_back(static_cast<uint32_t>(i));
+      else
+        list32.push_back(static_cast<uint32_t>(i));
+    }
+  }
+
+  // classes: tiles chosen per query length (tuning table)
+  std::vector<ClassPlan> cps(kNumClasses);
+  for (int k = 0; k < kNumClasses; ++k) cps[k].cls = k;
+  std::vector<uint32_t> tl;
+  for (uint32_t q = 0; q < byq.size(); ++q) {
+    auto& v = byq[q];
+    if (v.empty()) continue;
+    std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) { return c->h_db_len[pt[a]] > c->h_db_len[pt[b]]; });
+    tl.resize(v.size());
+    uint64_t sum_n = 0;
+    for (size_t j = 0; j < v.size(); ++j) {
+      tl[j] = c->h_db_len[pt[v[j]]];
+      sum_n += tl[j];
+    }
+    const uint32_t m = c->profs[q].m;
+    const int k = tuning_pick(&c->tuning, m, static_cast<uint32_t>(sum_n / v.size()));
+    const uint32_t rows = kClasses[k].G * kClasses[k].R;
+    const uint32_t P = (m + rows - 1) / rows;
+    if (static_cast<uint64_t>(kProfRows) * P * rows > kMaxSmem)
+      return fail(ST_EINVAL, "query of %u rows does not fit the shared-memory profile", m);
+    emit_query(cps[k], kClasses[k], q, m, v, tl, 64);
+  }
+
+  // order CTA tasks by estimated cost, longest first
+  for (auto& cp : cps) {
+    if (cp.cta.empty()) continue;
+    const Sw16Class& k = kClasses[cp.cls];
+    std::vector<std::pair<uint64_t, uint32_t>> cost(cp.cta.size());
+    for (size_t i = 0; i < cp.cta.size(); ++i) {
+      uint64_t cst = 0;
+      const uint32_t P = cp.cta[i].m_pad / (k.G * k.R);
+      for (uint32_t w = cp.cta[i].wt_begin; w < cp.cta[i].wt_end; ++w)
+        cst += static_cast<uint64_t>(P * cp.wt[w].ncols + k.G) * (k.R + 6);
+      cost[i] = {cst, static_cast<uint32_t>(i)};
+    }
+    std::stable_sort(cost.begin(), cost.end(), [](auto& a, auto& b) { return a.first > b.first; });
+    std::vector<Sw16CtaTask> sorted(cp.cta.size());
+    for (size_t i = 0; i < cost.size(); ++i) sorted[i] = cp.cta[cost[i].second];
+    cp.cta.swap(sorted);
+  }
+
+  // device buffers
+  auto upload = [&](DevMem& d, const void* src, size_t bytes) -> int {
+    ST_TRY(dev_alloc(&c->mt, d, bytes));
+    if (bytes) ST_CUDA(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, c->own));
+    return ST_OK;
+  };
+  ST_TRY(upload(plan->d_pair_q, pq.data(), n * 4));
+  ST_TRY(upload(plan->d_pair_t, pt.data(), n * 4));
+  ST_TRY(upload(plan->d_pair_c, pc.data(), n * 4));
+  ST_TRY(upload(plan->d_pair_r, pr.data(), n * 4));
+  // 32-bit list: static entries first, then room for every 16-bit pair
+  plan->n_static32 = static_cast<uint32_t>(list32.size());
+  ST_TRY(dev_alloc(&c->mt, plan->d_list, std::max<size_t>(n, 1) * 4));
+  if (!list32.empty())
+    ST_CUDA(cudaMemcpyAsync(plan->d_list.p, list32.data(), list32.size() * 4, cudaMemcpyHostToDevice, c->own));
+  // counters: [0, kNumClasses) class work, [kNumClasses] 32-bit work, [kNumClasses+1] list count
+  std::vector<uint32_t> cinit(kNumClasses + 2, 0);
+  cinit[kNumClasses + 1] = plan->n_static32;
+  ST_TRY(upload(plan->d_counters_init, cinit.data(), cinit.size() * 4));
+  ST_TRY(dev_alloc(&c->mt, plan->d_counters, cinit.size() * 4));
+
+  const DeviceDb db = db_view(c);
+  const DeviceProfiles pv = prof_view(c);
+  uint32_t* counters = plan->d_counters.as<uint32_t>();
+  for (auto& cp : cps) {
+    if (cp.cta.empty()) continue;
+    const Sw16Class& k = kClasses[cp.cls];
+    uint32_t max_mpad = 0, max_cols = 0;
+    bool multi = false;
+    for (auto& t : cp.cta) {
+      max_mpad = std::max(max_mpad, t.m_pad);
+      if (t.m_pad > static_cast<uint32_t>(k.G * k.R)) multi = true;
+    }
+    for (auto& w : cp.wt) max_cols = std::max(max_cols, w.ncols);
+    cp.smem = kProfRows * max_mpad;
+    ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(k.fn), kWarps16 * 32, cp.smem,
+                          static_cast<uint32_t>(cp.cta.size()), &cp.grid));
+    ST_TRY(upload(cp.d_cta, cp.cta.data(), cp.cta.size() * sizeof(Sw16CtaTask)));
+    ST_TRY(upload(cp.d_wt, cp.wt.data(), cp.wt.size() * sizeof(Sw16WarpTask)));
+    ST_TRY(upload(cp.d_slots, cp.slots.data(), cp.slots.size() * 4));
+    cp.scratch_stride = multi ? max_cols : 0;
+    const size_t groups = static_cast<size_t>(cp.grid) * kWarps16 * (32 / k.G);
+    ST_TRY(dev_alloc(&c->mt, cp.d_scratch, multi ? groups * max_cols * sizeof(uint2) : 16));
+  }
+  for (auto& cp : cps)
+    if (!cp.cta.empty()) plan->classes.push_back(std::move(cp));
+
+  // 32-bit kernel: a few persistent CTAs (rescoring is rare)
+  ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0,
+                        2 * c->sms, &plan->grid32));
+  plan->grid32 = std::min<uint32_t>(plan->grid32, 2 * c->sms);
+  plan->scratch32_stride = max_m32 > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
+  ST_TRY(dev_alloc(&c->mt, plan->d_scratch32,
+                   plan->scratch32_stride
+                       ? static_cast<size_t>(plan->grid32) * kWarps32 * plan->scratch32_stride * sizeof(int2)
+                       : 16));
+  ST_CUDA(cudaStreamSynchronize(c->own));
+
+  // capture the run into a CUDA graph (on the context's own stream)
+  ST_CUDA(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+  int cap_err = ST_OK;
+  do {
+    if (n) {
+      if (cudaMemsetAsync(d_scores, 0, n * 4, c->own) != cudaSuccess) { cap_err = ST_ECUDA; break; }
+      if (d_kernels && cudaMemsetAsync(d_kernels, 0, n * 4, c->own) != cudaSuccess) { cap_err = ST_ECUDA; break; }
+    }
+    if (cudaMemcpyAsync(counters, plan->d_counters_init.p, (kNumClasses + 2) * 4, cudaMemcpyDeviceToDevice,
+                        c->own) != cudaSuccess) { cap_err = ST_ECUDA; break; }
+    uint32_t nk = 0;
+    for (auto& cp : plan->classes) {
+      const Sw16Class& k = kClasses[cp.cls];
+      Sw16Params prm;
+      prm.db = db;
+      prm.prof = pv;
+      prm.cta_tasks = cp.d_cta.as<Sw16CtaTask>();
+      prm.n_cta_tasks = static_cast<uint32_t>(cp.cta.size());
+      prm.warp_tasks = cp.d_wt.as<Sw16WarpTask>();
+      prm.slot_pair = cp.d_slots.as<uint32_t>();
+      prm.pair_target = plan->d_pair_t.as<uint32_t>();
+      prm.scores = d_scores;
+      prm.kernels = d_kernels;
+      prm.ovf_count = counters + kNumClasses + 1;
+      prm.ovf_pairs = plan->d_list.as<uint32_t>();
+      prm.work_counter = counters + cp.cls;
+      prm.scratch = cp.d_scratch.as<uint2>();
+      prm.scratch_stride = cp.scratch_stride;
+      prm.open = open;
+      prm.ext = ext;
+      k.fn<<<cp.grid, kWarps16 * 32, cp.smem, c->own>>>(prm);
+      ++nk;
+    }
+    Sw32Params p32;
+    p32.db = db;
+    p32.prof = pv;
+    p32.list = plan->d_list.as<uint32_t>();
+    p32.list_count = counters + kNumClasses + 1;
+    p32.pair_query = plan->d_pair_q.as<uint32_t>();
+    p32.pair_target = plan->d_pair_t.as<uint32_t>();
+    p32.pair_center = plan->d_pair_c.as<int32_t>();
+    p32.pair_radius = plan->d_pair_r.as<int32_t>();
+    p32.scores = d_scores;
+    p32.kernels = d_kernels;
+    p32.work_counter = counters + kNumClasses;
+    p32.scratch = plan->d_scratch32.as<int2>();
+    p32.scratch_stride = plan->scratch32_stride;
+    p32.open = open;
+    p32.ext = ext;
+    sw32_kernel<kWarps32><<<plan->grid32, kWarps32 * 32, 0, c->own>>>(p32);
+    ++nk;
+    plan->kernels_per_run = nk;
+  } while (0);
+  cudaError_t ce = cudaStreamEndCapture(c->own, &plan->graph);
+  if (cap_err != ST_OK || ce != cudaSuccess)
+    return fail(ST_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce != cudaSuccess ? ce : cudaGetLastError()));
+  ST_CUDA(cudaGraphInstantiate(&plan->exec, plan->graph, 0));
+  *out = plan.release();
+  return ST_OK;
+}
+
+static int plan_run(st_plan* p) {
+  st_ctx* c = p->ctx;
+  ST_CUDA(cudaGraphLaunch(p->exec, c->stream));
+  c->launches += p->kernels_per_run;
+  return ST_OK;
+}
+
+static void plan_free(st_plan* p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  delete p;
+}
+
+extern "C" int st_plan_create(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                              int32_t* d_scores, uint32_t* d_kernels, st_plan** plan) {
+  CTX_GUARD(c);
+  if (!plan || (n && (!pairs || !d_scores))) return fail(ST_EINVAL, "st_plan_create: null argument");
+  return plan_build(c, pairs, n, open, ext, d_scores, d_kernels, plan);
+}
+
+extern "C" int st_plan_run(st_plan* p) {
+  if (!p) return fail(ST_EINVAL, "null plan");
+  st_ctx* c = p->ctx;
+  CTX_GUARD(c);
+  return plan_run(p);
+}
+
+extern "C" int st_plan_stats(st_plan* p, uint64_t* cells, uint64_t* rescored, uint32_t* n_classes) {
+  if (!p) return fail(ST_EINVAL, "null plan");
+  st_ctx* c = p->ctx;
+  CTX_GUARD(c);
+  if (cells) *cells = p->cells;
+  if (n_classes) *n_classes = static_cast<uint32_t>(p->classes.size());
+  if (rescored) {
+    uint32_t cnt = 0;
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    ST_CUDA(cudaMemcpy(&cnt, p->d_counters.as<uint32_t>() + kNumClasses + 1, 4, cudaMemcpyDeviceToHost));
+    *rescored = cnt >= p->n_static32 ? cnt - p->n_static32 : 0;
+  }
+  return ST_OK;
+}
+
+extern "C" void st_plan_destroy(st_plan* p) {
+  if (!p) return;
+  st_ctx* c = p->ctx;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  plan_free(p);
+}
+
+extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                                 int32_t* scores, uint32_t* kernels) {
+  CTX_GUARD(c);
+  if (n && (!pairs || !scores)) return fail(ST_EINVAL, "st_sw_score_pairs: null argument");
+  if (n == 0) return ST_OK;
+  DevMem d_out;
+  ST_TRY(dev_alloc(&c->mt, d_out, n * 8));
+  int32_t* d_scores = d_out.as<int32_t>();
+  uint32_t* d_kern = reinterpret_cast<uint32_t*>(d_scores + n);
+  st_plan* p = nullptr;
+  ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p));
+  std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
+  ST_TRY(plan_run(p));
+  ST_CUDA(cudaMemcpyAsync(scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (kernels) ST_CUDA(cudaMemcpyAsync(kernels, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plain per-call SW (one pair, one launch of each kernel, blocking)
+// ---------------------------------------------------------------------------
+extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
+                           int32_t* score, uint32_t* kernel) {
+  CTX_GUARD(c);
+  if (!score || (n && !target)) return fail(ST_EINVAL, "st_sw_score: null argument");
+  ST_TRY(check_profile(c, profile));
+  ST_TRY(sync_profiles(c));
+  const ProfileMeta& pm = c->profs[profile];
+  if (pm.m == 0 || n == 0) {  // src/simd.rs:253-255
+    *score = 0;
+    if (kernel) *kernel = ST_KERNEL_NONE;
+    return ST_OK;
+  }
+  // staging block (one host->device copy per call):
+  //   [target codes, padded] [db offset u64] [db length u32] [pair: target u32, query u32, center i32, radius i32]
+  //   [cta task] [warp task] [slots x64] [counters x(kNumClasses+2)] [32-bit list u32] [score i32, kernel u32]
+  const size_t tbytes = up16(n) + 32;
+  size_t o = tbytes;
+  const size_t o_off = o; o += 8;
+  const size_t o_len = o; o += 4;
+  const size_t o_pt = o; o += 4;
+  const size_t o_pq = o; o += 4;
+  const size_t o_pc = o; o += 4;
+  const size_t o_pr = o; o += 4;
+  o = up16(o);
+  const size_t o_cta = o; o += sizeof(Sw16CtaTask);
+  const size_t o_wt = o; o += sizeof(Sw16WarpTask);
+  const size_t o_slots = o; o += 64 * 4;
+  const size_t o_cnt = o; o += (kNumClasses + 2) * 4;
+  const size_t o_list = o; o += 4;
+  const size_t o_res = o; o += 8;
+  const size_t total = up16(o);
+  const bool use16 = pm.fits8 && gaps16_ok(open, ext);
+  int k = 0;
+  uint32_t P = 1, rows = 0;
+  if (use16) {
+    k = tuning_pick_single(&c->tuning, pm.m, n);
+    rows = kClasses[k].G * kClasses[k].R;
+    P = (pm.m + rows - 1) / rows;
+    if (static_cast<size_t>(kProfRows) * P * rows > kMaxSmem) return fail(ST_EINVAL, "query too long");
+  }
+  // any warp of the CTA may take the task: room for every group of the CTA
+  const size_t scratch_need = static_cast<size_t>(kWarps16) * 8 * (up16(n) + 32) * sizeof(uint2);
+  ST_TRY(c->pin.reserve(total));
+  if (c->stage.bytes < total) ST_TRY(dev_alloc(&c->mt, c->stage, total * 2));
+  if (c->scratch_small.bytes < scratch_need) ST_TRY(dev_alloc(&c->mt, c->scratch_small, scratch_need * 2));
+  char* h = c->pin.as<char>();
+  ST_CUDA(cudaStreamSynchronize(c->stream));  // the pinned block is reused per call
+  memset(h, 0, total);
+  for (uint32_t i = 0; i < n; ++i) h[i] = static_cast<char>(target[i] < kSentinel ? target[i] : kSentinel);
+  memset(h + n, kSentinel, tbytes - n);
+  *reinterpret_cast<uint64_t*>(h + o_off) = 0;
+  *reinterpret_cast<uint32_t*>(h + o_len) = n;
+  *reinterpret_cast<uint32_t*>(h + o_pt) = 0;
+  *reinterpret_cast<uint32_t*>(h + o_pq) = profile;
+  *reinterpret_cast<int32_t*>(h + o_pc) = 0;
+  *reinterpret_cast<int32_t*>(h + o_pr) = -1;  // no band
+  Sw16CtaTask ct{profile, 0, 1, P * std::max<uint32_t>(rows, 1)};
+  Sw16WarpTask wt{0, std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)))};
+  memcpy(h + o_cta, &ct, sizeof(ct));
+  memcpy(h + o_wt, &wt, sizeof(wt));
+  uint32_t* slots = reinterpret_cast<uint32_t*>(h + o_slots);
+  for (int s = 0; s < 64; ++s) slots[s] = kNoPair;
+  slots[0] = 0;
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(h + o_cnt);
+  if (!use16) cnt[kNumClasses + 1] = 1;  // the pair goes straight to the 32-bit list
+  *reinterpret_cast<uint32_t*>(h + o_list) = 0;
+  char* d = c->stage.as<char>();
+  ST_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, c->stream));
+  DeviceDb db;
+  db.arena = reinterpret_cast<const uint8_t*>(d);
+  db.offset = reinterpret_cast<const uint64_t*>(d + o_off);
+  db.length = reinterpret_cast<const uint32_t*>(d + o_len);
+  db.n_seqs = 1;
+  const DeviceProfiles pv = prof_view(c);
+  uint32_t* d_cnt = reinterpret_cast<uint32_t*>(d + o_cnt);
+  int32_t* d_score = reinterpret_cast<int32_t*>(d + o_res);
+  uint32_t* d_kern = reinterpret_cast<uint32_t*>(d + o_res + 4);
+  uint32_t* d_list = reinterpret_cast<uint32_t*>(d + o_list);
+  if (use16) {
+    Sw16Params prm;
+    prm.db = db;
+    prm.prof = pv;
+    prm.cta_tasks = reinterpret_cast<const Sw16CtaTask*>(d + o_cta);
+    prm.n_cta_tasks = 1;
+    prm.warp_tasks = reinterpret_cast<const Sw16WarpTask*>(d + o_wt);
+    prm.slot_pair = reinterpret_cast<const uint32_t*>(d + o_slots);
+    prm.pair_target = reinterpret_cast<const uint32_t*>(d + o_pt);
+    prm.scores = d_score;
+    prm.kernels = d_kern;
+    prm.ovf_count = d_cnt + kNumClasses + 1;
+    prm.ovf_pairs = d_list;
+    prm.work_counter = d_cnt + k;
+    prm.scratch = c->scratch_small.as<uint2>();
+    prm.scratch_stride = static_cast<uint32_t>(up16(n) + 32);
+    prm.open = open;
+    prm.ext = ext;
+    kClasses[k].fn<<<1, kWarps16 * 32, kProfRows * P * rows, c->stream>>>(prm);
+    ++c->launches;
+  }
+  // the 32-bit kernel scores the pair only when it is in the list (headroom reached, or not 16-bit eligible)
+  Sw32Params p32;
+  p32.db = db;
+  p32.prof = pv;
+  p32.list = d_list;
+  p32.list_count = d_cnt + kNumClasses + 1;
+  p32.pair_query = reinterpret_cast<const uint32_t*>(d + o_pq);
+  p32.pair_target = reinterpret_cast<const uint32_t*>(d + o_pt);
+  p32.pair_center = reinterpret_cast<const int32_t*>(d + o_pc);
+  p32.pair_radius = reinterpret_cast<const int32_t*>(d + o_pr);
+  p32.scores = d_score;
+  p32.kernels = d_kern;
+  p32.work_counter = d_cnt + kNumClasses;
+  p32.scratch = reinterpret_cast<int2*>(c->scratch_small.p);
+  p32.scratch_stride = static_cast<uint32_t>(up16(n) + 32);
+  p32.open = open;
+  p32.ext = ext;
+  sw32_kernel<kWarps32><<<1, kWarps32 * 32, 0, c->stream>>>(p32);
+  ++c->launches;
+  ST_CUDA(cudaGetLastError());
+  int32_t res[2];
+  ST_CUDA(cudaMemcpyAsync(res, d_score, 8, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  *score = res[0];
+  if (kernel) *kernel = static_cast<uint32_t>(res[1]);
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ungapped
+// ---------------------------------------------------------------------------
+static uint32_t ung_stride(st_ctx* c) { return static_cast<uint32_t>(up16(c->max_m) + 32); }
+
+static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n, int32_t* d_out) {
+  if (n == 0) return ST_OK;
+  UngappedParams prm;
+  prm.db = db_view(c);
+  prm.prof = prof_view(c);
+  prm.jobs = d_jobs;
+  prm.n = n;
+  prm.out = d_out;
+  prm.max_m_pad = ung_stride(c);
+  const size_t smem = 16 + static_cast<size_t>(kProfRows) * prm.max_m_pad + 16;
+  if (smem > kMaxSmem) return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", c->max_m);
+  const uint64_t grid = (n + kUngChunk - 1) / kUngChunk;
+  if (grid > 0x7FFFFFFFull) return fail(ST_EINVAL, "too many ungapped jobs");
+  if (hits)
+    ungapped_kernel<true><<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
+  else
+    ungapped_kernel<false><<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
+  ++c->launches;
+  ST_CUDA(cudaGetLastError());
+  return ST_OK;
+}
+
+extern "C" int st_ungapped_score(st_ctx* c, uint32_t profile, const st_lane* lanes, uint32_t n, int32_t* out) {
+  CTX_GUARD(c);
+  if (n && (!lanes || !out)) return fail(ST_EINVAL, "st_ungapped_score: null argument");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  ST_TRY(check_profile(c, profile));
+  ST_TRY(sync_profiles(c));
+  if (n == 0) return ST_OK;
+  const uint32_t m = c->profs[profile].m;
+  const size_t jb = up16(static_cast<size_t>(n) * sizeof(UngappedJob));
+  ST_TRY(c->pin.reserve(jb + static_cast<size_t>(n) * 4));
+  if (c->stage.bytes < jb + static_cast<size_t>(n) * 4) ST_TRY(dev_alloc(&c->mt, c->stage, (jb + n * 4ull) * 2));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  UngappedJob* h = c->pin.as<UngappedJob>();
+  for (uint32_t i = 0; i < n; ++i) {
+    const st_lane& l = lanes[i];
+    if (l.target >= c->n_seqs) return fail(ST_EINVAL, "lane %u: target %u outside the database", i, l.target);
+    const int64_t tn = c->h_db_len[l.target];
+    // the window must lie inside diag_range (src/ungapped.rs:300-310)
+    const int64_t lo = std::max<int64_t>(-static_cast<int64_t>(l.diag), 0);
+    const int64_t hi = std::min<int64_t>(m, tn - l.diag);
+    UngappedJob j{profile, l.target, l.diag, l.lo, l.hi};
+    if (l.lo >= l.hi) {
+      j.lo = j.hi = 0;
+    } else if (static_cast<int64_t>(l.lo) < lo || static_cast<int64_t>(l.hi) > hi) {
+      return fail(ST_EINVAL, "lane %u: window [%u, %u) outside the diagonal's range [%lld, %lld)", i, l.lo, l.hi,
+                  static_cast<long long>(lo), static_cast<long long>(hi));
+    }
+    h[i] = j;
+  }
+  char* d = c->stage.as<char>();
+  ST_CUDA(cudaMemcpyAsync(d, h, static_cast<size_t>(n) * sizeof(UngappedJob), cudaMemcpyHostToDevice, c->stream));
+  int32_t* d_out = reinterpret_cast<int32_t*>(d + jb);
+  ST_TRY(launch_ungapped(c, false, d, n, d_out));
+  ST_CUDA(cudaMemcpyAsync(out, d_out, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  return ST_OK;
+}
+
+static int run_pairs_device(st_ctx* c, const st_hit* d_hits, uint64_t n, const int32_t* d_per_hit,
+                            int32_t* d_pair_best, uint32_t* d_pair_q, uint32_t* d_pair_t, uint64_t* d_n_pairs) {
+  const uint64_t nb = (n + kRunBlock - 1) / kRunBlock;
+  if (nb > 0xFFFFFFFFull) return fail(ST_EINVAL, "too many hits");
+  DevMem tmp;
+  ST_TRY(dev_alloc(&c->mt, tmp, nb * 12 + 16));
+  uint32_t* counts = tmp.as<uint32_t>();
+  uint64_t* offs = reinterpret_cast<uint64_t*>(tmp.as<char>() + up16(nb * 4));
+  const HitRec* h = reinterpret_cast<const HitRec*>(d_hits);
+  run_count_kernel<<<static_cast<uint32_t>(nb), kRunBlock, 0, c->stream>>>(h, n, counts);
+  run_scan_kernel<<<1, 1024, 0, c->stream>>>(counts, static_cast<uint32_t>(nb), offs, d_n_pairs);
+  run_write_kernel<<<static_cast<uint32_t>(nb), kRunBlock, 0, c->stream>>>(h, n, d_per_hit, offs, d_pair_best,
+                                                                            d_pair_q, d_pair_t);
+  c->launches += 3;
+  ST_CUDA(cudaGetLastError());
+  // tmp must outlive the kernels
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  return ST_OK;
+}
+
+static int check_hits_device(st_ctx* c) {
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  return sync_profiles(c);
+}
+
+extern "C" int st_ungapped_hits_device(st_ctx* c, const st_hit* d_hits, uint64_t n, int32_t* d_per_hit,
+                                       int32_t* d_pair_best, uint32_t* d_pair_query, uint32_t* d_pair_target,
+                                       uint64_t* d_n_pairs) {
+  CTX_GUARD(c);
+  if (n && (!d_hits || !d_per_hit)) return fail(ST_EINVAL, "st_ungapped_hits_device: null argument");
+  ST_TRY(check_hits_device(c));
+  if (n == 0) {
+    if (d_n_pairs) ST_CUDA(cudaMemsetAsync(d_n_pairs, 0, 8, c->stream));
+    return ST_OK;
+  }
+  ST_TRY(launch_ungapped(c, true, d_hits, n, d_per_hit));
+  if (d_pair_best && d_pair_query && d_pair_target && d_n_pairs)
+    ST_TRY(run_pairs_device(c, d_hits, n, d_per_hit, d_pair_best, d_pair_query, d_pair_target, d_n_pairs));
+  return ST_OK;
+}
+
+extern "C" int st_ungapped_hits(st_ctx* c, const st_hit* hits, uint64_t n, int32_t* per_hit, int32_t* pair_best,
+                                uint32_t* pair_query, uint32_t* pair_target, uint64_t* n_pairs) {
+  CTX_GUARD(c);
+  if (n && (!hits || !per_hit)) return fail(ST_EINVAL, "st_ungapped_hits: null argument");
+  ST_TRY(check_hits_device(c));
+  const bool want_pairs = pair_best && pair_query && pair_target && n_pairs;
+  if (n == 0) {
+    if (n_pairs) *n_pairs = 0;
+    return ST_OK;
+  }
+  for (uint64_t i = 0; i < n; ++i) {
+    if (hits[i].query >= c->profs.size() || !c->profs[hits[i].query].live)
+      return fail(ST_EINVAL, "hit %llu: unknown profile id %u", static_cast<unsigned long long>(i), hits[i].query);
+    if (hits[i].target >= c->n_seqs)
+      return fail(ST_EINVAL, "hit %llu: target %u outside the database", static_cast<unsigned long long>(i),
+                  hits[i].target);
+  }
+  DevMem buf;
+  const size_t hb = up16(n * sizeof(st_hit));
+  const size_t ob = up16(n * 4);
+  ST_TRY(dev_alloc(&c->mt, buf, hb + ob + (want_pairs ? 3 * ob + 16 : 0)));
+  char* d = buf.as<char>();
+  ST_CUDA(cudaMemcpyAsync(d, hits, n * sizeof(st_hit), cudaMemcpyHostToDevice, c->stream));
+  int32_t* d_out = reinterpret_cast<int32_t*>(d + hb);
+  ST_TRY(launch_ungapped(c, true, d, n, d_out));
+  if (want_pairs) {
+    int32_t* d_pb = reinterpret_cast<int32_t*>(d + hb + ob);
+    uint32_t* d_pq = reinterpret_cast<uint32_t*>(d + hb + 2 * ob);
+    uint32_t* d_pt = reinterpret_cast<uint32_t*>(d + hb + 3 * ob);
+    uint64_t* d_np = reinterpret_cast<uint64_t*>(d + hb + 4 * ob);
+    ST_TRY(run_pairs_device(c, reinterpret_cast<const st_hit*>(d), n, d_out, d_pb, d_pq, d_pt, d_np));
+    uint64_t np = 0;
+    ST_CUDA(cudaMemcpyAsync(&np, d_np, 8, cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    *n_pairs = np;
+    if (np) {
+      ST_CUDA(cudaMemcpyAsync(pair_best, d_pb, np * 4, cudaMemcpyDeviceToHost, c->stream));
+      ST_CUDA(cudaMemcpyAsync(pair_query, d_pq, np * 4, cudaMemcpyDeviceToHost, c->stream));
+      ST_CUDA(cudaMemcpyAsync(pair_target, d_pt, np * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
+  ST_CUDA(cudaMemcpyAsync(per_hit, d_out, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// DPX throughput probe (denominator of the SW roofline)
+// ---------------------------------------------------------------------------
+constexpr int kProbeChains = 8;
+constexpr int kProbeIters = 4096;
+
+__global__ void dpx_probe_kernel(uint32_t* sink, uint32_t seed) {
+  uint32_t a[kProbeChains];
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) a[k] = seed * (threadIdx.x + k + 1);
+  const uint32_t b = seed ^ 0x00050003u, cc = seed ^ 0x00020001u;
+  for (int i = 0; i < kProbeIters; ++i) {
+#pragma unroll
+    for (int k = 0; k < kProbeChains; ++k) a[k] = __viaddmax_s16x2(a[k], b, cc);
+  }
+  uint32_t r = 0;
+#pragma unroll
+  for (int k = 0; k < kProbeChains; ++k) r ^= a[k];
+  if (r == 0x9E3779B9u) sink[0] = r;  // keeps the chains live
+}
+
+extern "C" int st_probe_dpx(st_ctx* c, double* ops_per_s) {
+  CTX_GUARD(c);
+  if (!ops_per_s) return fail(ST_EINVAL, "null output");
+  DevMem sink;
+  ST_TRY(dev_alloc(&c->mt, sink, 16));
+  const int blocks = c->sms * 8, threads = 256;
+  cudaEvent_t e0, e1;
+  ST_CUDA(cudaEventCreate(&e0));
+  ST_CUDA(cudaEventCreate(&e1));
+  dpx_probe_kernel<<<blocks, threads, 0, c->stream>>>(sink.as<uint32_t>(), 7);
+  ST_CUDA(cudaEventRecord(e0, c->stream));
+  const int reps = 5;
+  for (int r = 0; r < reps; ++r) dpx_probe_kernel<<<blocks, threads, 0, c->stream>>>(sink.as<uint32_t>(), 11 + r);
+  ST_CUDA(cudaEventRecord(e1, c->stream));
+  ST_CUDA(cudaEventSynchronize(e1));
+  c->launches += reps + 1;
+  float ms = 0;
+  ST_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const double ops = static_cast<double>(reps) * blocks * threads * kProbeIters * kProbeChains;
+  *ops_per_s = ops / (ms * 1e-3);
+  return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tile classes and the autotuner
+// ---------------------------------------------------------------------------
+extern "C" int st_tune_num_classes(void) { return kNumClasses; }
+
+extern "C" int st_tune_class_shape(int cls, int* lanes, int* rows) {
+  if (cls < 0 || cls >= kNumClasses || !lanes || !rows) return fail(ST_EINVAL, "bad tile class %d", cls);
+  *lanes = kClasses[cls].G;
+  *rows = kClasses[cls].R;
+  return ST_OK;
+}
+
+extern "C" int st_tune_get(st_ctx* c, int32_t* table) {
+  CTX_GUARD(c);
+  if (!table) return fail(ST_EINVAL, "null table");
+  for (int i = 0; i < kTuneMBins; ++i)
+    for (int j = 0; j < kTuneNBins; ++j) table[i * kTuneNBins + j] = c->tuning.table[i][j];
+  return ST_OK;
+}
+
+extern "C" int st_tune_set(st_ctx* c, const int32_t* table) {
+  CTX_GUARD(c);
+  if (!table) return fail(ST_EINVAL, "null table");
+  for (int i = 0; i < kTuneMBins * kTuneNBins; ++i)
+    if (table[i] < -1 || table[i] >= kNumClasses) return fail(ST_EINVAL, "bad class %d in table", table[i]);
+  for (int i = 0; i < kTuneMBins; ++i)
+    for (int j = 0; j < kTuneNBins; ++j) c->tuning.table[i][j] = table[i * kTuneNBins + j];
+  return ST_OK;
+}
+
+extern "C" int st_autotune(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                           uint32_t max_pairs_per_bin, uint32_t* bins_tuned) {
+  CTX_GUARD(c);
+  if (n && !pairs) return fail(ST_EINVAL, "st_autotune: null pairs");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  ST_TRY(sync_profiles(c));
+  if (bins_tuned) *bins_tuned = 0;
+  if (!gaps16_ok(open, ext)) return ST_OK;  // nothing runs on the 16-bit kernel
+  // pairs of the 16-bit kernel, grouped by query
+  std::vector<std::vector<uint32_t>> byq(c->profs.size());
+  for (uint64_t i = 0; i < n; ++i) {
+    const st_pair& p = pairs[i];
+    if (p.profile >= c->profs.size() || !c->profs[p.profile].live || p.target >= c->n_seqs)
+      return fail(ST_EINVAL, "st_autotune: bad pair %llu", static_cast<unsigned long long>(i));
+    const ProfileMeta& pm = c->profs[p.profile];
+    if (p.band_radius >= 0 || !pm.fits8 || pm.m == 0 || c->h_db_len[p.target] == 0) continue;
+    byq[p.profile].push_back(static_cast<uint32_t>(i));
+  }
+  std::vector<std::vector<st_pair>> bins(kTuneMBins * kTuneNBins);
+  for (uint32_t q = 0; q < byq.size(); ++q) {
+    if (byq[q].empty()) continue;
+    uint64_t sum = 0;
+    for (uint32_t i : byq[q]) sum += c->h_db_len[pairs[i].target];
+    const int b = tune_mbin(c->profs[q].m) * kTuneNBins + tune_nbin(static_cast<uint32_t>(sum / byq[q].size()));
+    auto& v = bins[b];
+    if (v.size() >= max_pairs_per_bin) continue;
+    for (uint32_t i : byq[q]) v.push_back(pairs[i]);
+  }
+  DevMem out;
+  cudaEvent_t e0, e1;
+  ST_CUDA(cudaEventCreate(&e0));
+  ST_CUDA(cudaEventCreate(&e1));
+  uint32_t tuned = 0;
+  for (int b = 0; b < kTuneMBins * kTuneNBins; ++b) {
+    auto& v = bins[b];
+    if (v.empty()) continue;
+    if (out.bytes < v.size() * 8) ST_TRY(dev_alloc(&c->mt, out, v.size() * 8));
+    const int mb = b / kTuneNBins, nb = b % kTuneNBins;
+    uint32_t max_m = 0;
+    for (auto& p : v) max_m = std::max(max_m, c->profs[p.profile].m);
+    int best_c = -1;
+    float best_ms = 1e30f;
+    for (int k = 0; k < kNumClasses; ++k) {
+      if (tune_cost(&c->tuning, k, max_m, 64, false) >= 1e300) continue;
+      c->tuning.table[mb][nb] = k;
+      st_plan* p = nullptr;
+      ST_TRY(plan_build(c, v.data(), v.size(), open, ext, out.as<int32_t>(), nullptr, &p));
+      std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
+      cudaStream_t saved = c->stream;
+      c->stream = c->own;
+      ST_TRY(plan_run(p));  // warm-up
+      ST_CUDA(cudaEventRecord(e0, c->own));
+      const int reps = 3;
+      for (int r = 0; r < reps; ++r) ST_TRY(plan_run(p));
+      ST_CUDA(cudaEventRecord(e1, c->own));
+      ST_CUDA(cudaEventSynchronize(e1));
+      c->stream = saved;
+      float ms = 0;
+      ST_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_c = k;
+      }
+    }
+    c->tuning.table[mb][nb] = best_c;
+    ++tuned;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (bins_tuned) *bins_tuned = tuned;
+  return ST_OK;
+}

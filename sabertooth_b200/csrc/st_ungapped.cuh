@@ -1,0 +1,244 @@
+// Ungapped diagonal scoring (the reference's ungapped::score_batch /
+// kadane_score, src/ungapped.rs:53-62 and 285-386).
+//
+// One thread scores one diagonal: Kadane's running maximum
+//   cur = max(cur, 0) + s(q, t[q + d]),  best = max(best, cur),  best0 = 0
+// over query positions [lo, hi), exactly as kadane_score, in int32 (the GPU
+// needs no u8 headroom and no rescore).  Target residues are read as aligned
+// 16-byte vectors from the padded database arena; cells of a vector that lie
+// outside [lo, hi) score 0, which cannot change the result (the reference's
+// SENTINEL argument, src/ungapped.rs:28-33).
+//
+// A CTA takes a chunk of jobs; jobs are expected sorted by query (the order
+// the prefilter produces), and each run of one query inside the chunk stages
+// that query's int8 profile in shared memory (residue-major, 16 guard bytes on
+// each side of every row so out-of-window positions stay inside the array).
+#pragma once
+#include "st_common.cuh"
+
+namespace st {
+
+struct UngappedJob {  // explicit window (the drop-in lanes)
+  uint32_t query;
+  uint32_t target;
+  int32_t diag;
+  uint32_t lo;
+  uint32_t hi;
+};
+
+struct HitRec {  // a prefilter seed hit: the window is the whole diagonal
+  uint32_t query;
+  uint32_t target;
+  int32_t diag;
+};
+
+struct UngappedParams {
+  DeviceDb db;
+  DeviceProfiles prof;
+  const void* jobs;  // UngappedJob[] or HitRec[]
+  uint64_t n;
+  int32_t* out;
+  uint32_t max_m_pad;  // row stride of the staged profile (>= every query length + 32)
+};
+
+constexpr int kUngChunk = 1024;  // jobs per CTA chunk
+
+template <bool HITS>
+__device__ __forceinline__ void ung_job(const UngappedParams& prm, uint64_t k, uint32_t& q, uint32_t& t,
+                                        int32_t& d, int64_t& lo, int64_t& hi) {
+  if constexpr (HITS) {
+    const HitRec h = reinterpret_cast<const HitRec*>(prm.jobs)[k];
+    q = h.query;
+    t = h.target;
+    d = h.diag;
+    const int64_t m = prm.prof.qlen[q];
+    const int64_t n = prm.db.length[t];
+    // diag_range, src/ungapped.rs:38-46
+    lo = i64max(-static_cast<int64_t>(d), 0);
+    hi = i64min(m, n - d);
+    if (hi <= lo) lo = hi = 0;
+  } else {
+    const UngappedJob j = reinterpret_cast<const UngappedJob*>(prm.jobs)[k];
+    q = j.query;
+    t = j.target;
+    d = j.diag;
+    lo = j.lo;
+    hi = j.hi;
+  }
+}
+
+template <bool HITS>
+__device__ __forceinline__ uint32_t ung_query(const UngappedParams& prm, uint64_t k) {
+  if constexpr (HITS)
+    return reinterpret_cast<const HitRec*>(prm.jobs)[k].query;
+  else
+    return reinterpret_cast<const UngappedJob*>(prm.jobs)[k].query;
+}
+
+template <bool HITS>
+__global__ void __launch_bounds__(256) ungapped_kernel(const UngappedParams prm) {
+  extern __shared__ __align__(16) int8_t smem[];
+  __shared__ uint32_t s_run_end;
+  const uint32_t stride = prm.max_m_pad;
+  int8_t* base = smem + 16;  // 16 guard bytes before row 0
+  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kUngChunk;
+  if (c0 >= prm.n) return;
+  const uint64_t c1 = u64min(prm.n, c0 + kUngChunk);
+  uint64_t a = c0;
+  while (a < c1) {
+    const uint32_t q = ung_query<HITS>(prm, a);
+    // end of this query's run inside the chunk (warp 0 scans 32 jobs at a time)
+    if (threadIdx.x < 32) {
+      uint64_t e = a;
+      for (;;) {
+        const uint64_t k = e + threadIdx.x;
+        const bool same = (k < c1) && (ung_query<HITS>(prm, k) == q);
+        const uint32_t ball = __ballot_sync(0xFFFFFFFFu, same);
+        if (ball != 0xFFFFFFFFu) {
+          e += __ffs(~ball) - 1;
+          break;
+        }
+        e += 32;
+      }
+      if (threadIdx.x == 0) s_run_end = static_cast<uint32_t>(e - c0);
+    }
+    // stage the profile of q: rows 0..21, m entries each, zero elsewhere
+    const uint32_t m = prm.prof.qlen[q];
+    const uint32_t pstride = prm.prof.stride8[q];
+    const int8_t* src = prm.prof.p8[q];
+    for (uint32_t idx = threadIdx.x; idx < kProfRows * (stride / 16); idx += blockDim.x) {
+      const uint32_t r = idx / (stride / 16);
+      const uint32_t i = (idx - r * (stride / 16)) * 16;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (i < pstride) v = *reinterpret_cast<const uint4*>(src + static_cast<size_t>(r) * pstride + i);
+      *reinterpret_cast<uint4*>(base + static_cast<size_t>(r) * stride + i) = v;
+    }
+    if (threadIdx.x < 16) {  // guard bytes before row 0
+      smem[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    const uint64_t b = c0 + s_run_end;
+    // rows outside int8 (rare: composition-corrected or custom rows) read the int32 profile from global memory
+    const bool narrow = prm.prof.fits8[q] != 0;
+    const int32_t* p32 = prm.prof.p32[q];
+    const int32_t s32 = static_cast<int32_t>(prm.prof.stride32[q]);
+    const int32_t last_row = static_cast<int32_t>(m) - 1;
+    for (uint64_t k = a + threadIdx.x; k < b; k += blockDim.x) {
+      uint32_t qq, tt;
+      int32_t d;
+      int64_t lo, hi;
+      ung_job<HITS>(prm, k, qq, tt, d, lo, hi);
+      int32_t best = 0, cur = 0;
+      if (hi > lo) {
+        const uint8_t* tp = prm.db.arena + prm.db.offset[tt];
+        // target positions [p0, p1); sequences are shorter than 2^31
+        const int32_t p0 = static_cast<int32_t>(lo) + d, p1 = static_cast<int32_t>(hi) + d;
+        int32_t pa = p0 & ~15;
+        for (; pa < p1; pa += 16) {
+          const uint4 v = *reinterpret_cast<const uint4*>(tp + pa);
+          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+          const int32_t qa = pa - d;  // query row of the vector's first byte
+          const int8_t* rowbase = base + qa;
+#pragma unroll
+          for (int bb = 0; bb < 16; ++bb) {
+            const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+            const int32_t p = pa + bb;
+            const bool in = (p >= p0) && (p < p1);
+            int32_t sc;
+            if (narrow) {
+              sc = rowbase[static_cast<int32_t>(r * stride) + bb];
+            } else {
+              const int32_t row = min(max(qa + bb, 0), last_row);
+              sc = __ldg(p32 + static_cast<int32_t>(r) * s32 + row);
+            }
+            const int32_t s = in ? sc : 0;
+            cur = wadd(max(cur, 0), s);
+            best = max(best, cur);
+          }
+        }
+      }
+      prm.out[k] = best;
+    }
+    __syncthreads();
+    a = b;
+  }
+}
+
+// ---- per-(query, target) runs of hits ------------------------------------
+// A run starts at hit k when k == 0 or (query, target) differs from hit k-1.
+// Three deterministic phases: count run starts per block, scan the counts,
+// then write one (best, query, target) entry per run in hit order.
+constexpr int kRunBlock = 1024;
+
+__device__ __forceinline__ bool run_start(const HitRec* h, uint64_t k) {
+  if (k == 0) return true;
+  const HitRec a = h[k - 1], b = h[k];
+  return a.query != b.query || a.target != b.target;
+}
+
+__global__ void __launch_bounds__(kRunBlock) run_count_kernel(const HitRec* h, uint64_t n, uint32_t* counts) {
+  __shared__ uint32_t s_cnt;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  const uint64_t k = static_cast<uint64_t>(blockIdx.x) * kRunBlock + threadIdx.x;
+  const bool st = k < n && run_start(h, k);
+  const uint32_t ball = __ballot_sync(0xFFFFFFFFu, st);
+  if ((threadIdx.x & 31) == 0 && ball) atomicAdd(&s_cnt, __popc(ball));
+  __syncthreads();
+  if (threadIdx.x == 0) counts[blockIdx.x] = s_cnt;
+}
+
+// exclusive scan of counts[0..nb) in one CTA; writes offsets and the total
+__global__ void __launch_bounds__(1024) run_scan_kernel(const uint32_t* counts, uint32_t nb, uint64_t* offsets,
+                                                        uint64_t* total) {
+  __shared__ uint64_t s_part[1024];
+  __shared__ uint64_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < nb; base += 1024) {
+    const uint32_t i = base + threadIdx.x;
+    const uint64_t v = i < nb ? counts[i] : 0;
+    s_part[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t o = 1; o < 1024; o <<= 1) {
+      const uint64_t add = threadIdx.x >= o ? s_part[threadIdx.x - o] : 0;
+      __syncthreads();
+      s_part[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (i < nb) offsets[i] = s_carry + s_part[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry += s_part[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = s_carry;
+}
+
+__global__ void __launch_bounds__(kRunBlock) run_write_kernel(const HitRec* h, uint64_t n, const int32_t* per_hit,
+                                                              const uint64_t* offsets, int32_t* pair_best,
+                                                              uint32_t* pair_query, uint32_t* pair_target) {
+  __shared__ uint32_t s_warp[kRunBlock / 32];
+  const uint64_t k = static_cast<uint64_t>(blockIdx.x) * kRunBlock + threadIdx.x;
+  const bool st = k < n && run_start(h, k);
+  const uint32_t ball = __ballot_sync(0xFFFFFFFFu, st);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) s_warp[warp] = __popc(ball);
+  __syncthreads();
+  if (st) {
+    uint32_t pos = __popc(ball & ((1u << lane) - 1u));
+    for (int w = 0; w < warp; ++w) pos += s_warp[w];
+    const uint64_t o = offsets[blockIdx.x] + pos;
+    const HitRec a = h[k];
+    int32_t b = per_hit[k];
+    for (uint64_t j = k + 1; j < n; ++j) {
+      const HitRec c = h[j];
+      if (c.query != a.query || c.target != a.target) break;
+      b = max(b, per_hit[j]);
+    }
+    pair_best[o] = b;
+    pair_query[o] = a.query;
+    pair_target[o] = a.target;
+  }
+}
+
+}  // namespace st

@@ -1,0 +1,138 @@
+"""GPU parity of ungapped diagonal scoring against the CPU oracle.
+
+Cases follow the reference's tests (src/ungapped.rs:531-616): every diagonal
+of random pairs with sub-windows (seed 3), random and homologous lanes with
+windows and empty ranges (seed 17), and wide PSSM-like rows, plus the batched
+hit form with its per-(query, target) runs.  Bar: bit-exact int32.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sabertooth_b200 import DiagProfile, Lane, blosum62, score_batch
+from sabertooth_b200 import workloads as W
+from sabertooth_b200.api import diag_range
+from tests.refrng import SplitMix64
+
+pytestmark = pytest.mark.gpu
+
+
+def test_every_diagonal_and_subwindows(ctx):
+    rng = SplitMix64(3)
+    m = blosum62()
+    cases = []
+    for _ in range(60):
+        q = [rng.below(21) for _ in range(1 + rng.below(80))]
+        t = [rng.below(21) for _ in range(1 + rng.below(120))]
+        cases.append((q, t))
+    ctx.upload_db_list([np.array(t, np.uint8) for _, t in cases])
+    for k, (q, t) in enumerate(cases):
+        rows = m.sequence_rows(q)
+        prof = DiagProfile.build(rows, ctx)
+        lanes, want = [], []
+        for d in range(-len(q) - 2, len(t) + 2):
+            lo, hi = diag_range(len(q), len(t), d)
+            lanes.append(Lane(k, d, lo, hi))
+            want.append(O.kadane_score(rows, t, d, lo, hi))
+            if hi > lo + 2:
+                lanes.append(Lane(k, d, lo + 1, hi - 1))
+                want.append(O.kadane_score(rows, t, d, lo + 1, hi - 1))
+        got = score_batch(prof, lanes)
+        prof.qp.free()
+        assert np.array_equal(got, np.array(want, dtype=np.int32)), k
+
+
+def test_random_and_homologous_lanes(ctx):
+    rng = SplitMix64(17)
+    mat = blosum62()
+    for case in range(12):
+        qlen = 1 + rng.below(400 if case % 3 == 0 else 90)
+        q = [rng.below(21) for _ in range(qlen)]
+        rows = mat.sequence_rows(q)
+        targets = []
+        for k in range(70):
+            if k % 5 == 0:  # a copy of the query with a few substitutions: long, high-scoring
+                t = list(q)
+                for _ in range(qlen // 10):
+                    t[rng.below(qlen)] = rng.below(20)
+            else:
+                t = [rng.below(21) for _ in range(1 + rng.below(300))]
+            targets.append(t)
+        ctx.upload_db_list([np.array(t, np.uint8) for t in targets])
+        prof = DiagProfile.build(rows, ctx)
+        lanes, want = [], []
+        for k, t in enumerate(targets):
+            d = 0 if k % 5 == 0 else rng.below(len(t) + qlen + 4) - qlen - 2
+            lo, hi = diag_range(qlen, len(t), d)
+            if k % 3 == 1 and hi > lo + 4:
+                a = lo + rng.below(hi - lo)
+                b = a + rng.below(hi - a) + 1
+                lo, hi = a, b
+            lanes.append(Lane(k, d, lo, hi))
+            want.append(O.kadane_score(rows, t, d, lo, hi))
+        got = score_batch(prof, lanes)
+        prof.qp.free()
+        assert np.array_equal(got, np.array(want, dtype=np.int32)), case
+
+
+def test_wide_score_rows(ctx):
+    # rows the reference's u8 kernel rejects (src/ungapped.rs:608-616) are exact here
+    rows = np.zeros((50, 21), dtype=np.int32)
+    rows[::2, 0] = 200
+    rows[1::2, 1] = -100
+    t = np.array([0, 1] * 40 + [0] * 30, dtype=np.uint8)
+    ctx.upload_db_list([t])
+    prof = DiagProfile.build(rows, ctx)
+    lanes = [Lane(0, d, *diag_range(50, t.size, d)) for d in range(-49, t.size)]
+    want = [O.kadane_score(rows, t, l.diag, l.lo, l.hi) for l in lanes]
+    assert np.array_equal(score_batch(prof, lanes), np.array(want, dtype=np.int32))
+    prof.qp.free()
+
+
+def test_window_outside_the_diagonal_is_rejected(ctx):
+    from sabertooth_b200._lib import StError
+    t = np.zeros(10, dtype=np.uint8)
+    ctx.upload_db_list([t])
+    prof = DiagProfile.build(np.ones((5, 21), dtype=np.int32), ctx)
+    with pytest.raises(StError):
+        score_batch(prof, [Lane(0, 8, 0, 5)])  # diag 8 leaves only query positions 0..1
+    prof.qp.free()
+
+
+def test_hits_and_pair_runs_match_oracle(ctx):
+    w = W.config2(seed=2, n_queries=40, n_targets=3000, n_hits=60_000)
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    hits = w.hits.copy()
+    hits["query"] = ids[hits["query"]]
+    per_hit, (pb, pq, pt) = ctx.ungapped_hits(hits)
+    ar = O.Arena(w.rows, [w.db_residues[int(a):int(b)] for a, b in zip(w.db_offsets[:-1], w.db_offsets[1:])])
+    want = O.ungapped_hits(ar, w.hits["query"], w.hits["target"], w.hits["diag"])
+    assert np.array_equal(per_hit, want)
+    # runs of equal (query, target) in hit order
+    key = w.hits["query"].astype(np.int64) * (1 << 32) + w.hits["target"]
+    start = np.ones(len(key), dtype=bool)
+    start[1:] = key[1:] != key[:-1]
+    idx = np.nonzero(start)[0]
+    run_best = np.maximum.reduceat(want, idx)
+    assert np.array_equal(pb, run_best)
+    assert np.array_equal(pq, ids[w.hits["query"][idx]])
+    assert np.array_equal(pt, w.hits["target"][idx])
+    for i in ids:
+        ctx.free_profile(i)
+
+
+def test_unsorted_hits_are_still_exact(ctx):
+    w = W.config2(seed=4, n_queries=30, n_targets=2000, n_hits=20_000)
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    perm = np.random.default_rng(0).permutation(len(w.hits))
+    hits = w.hits[perm].copy()
+    want = O.ungapped_hits(O.Arena(w.rows, [w.db_residues[int(a):int(b)] for a, b in
+                                             zip(w.db_offsets[:-1], w.db_offsets[1:])]),
+                           hits["query"], hits["target"], hits["diag"])
+    hits["query"] = ids[hits["query"]]
+    got = ctx.ungapped_hits(hits, with_pairs=False)
+    assert np.array_equal(got, want)
+    for i in ids:
+        ctx.free_profile(i)
