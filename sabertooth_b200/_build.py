@@ -1,6 +1,6 @@
 """Build the native library in-tree.
 
-    python -m sabertooth_b200._build          # libsabertooth_b200.so for sm_100a
+    python sabertooth_b200/_build.py          # libsabertooth_b200.so for sm_100a
 
 nvcc compiles the CUDA runtime and kernels for sm_100a (B200) and the host
 utilities into one shared library next to this file, so the built .so travels

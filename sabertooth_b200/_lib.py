@@ -81,7 +81,7 @@ SIGNATURES = {
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m sabertooth_b200._build` "
+            f"{LIB_PATH} is missing: build it with `python sabertooth_b200/_build.py` "
             "(the package has no CPU fallback)")
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():
