@@ -161,6 +161,25 @@ int st_tune_set(st_ctx* ctx, const int32_t* table);
 int st_autotune(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
                 uint32_t max_pairs_per_bin, uint32_t* bins_tuned);
 
+/* ---- allocation-free scoring ----------------------------------------------- */
+/* Exact SW-Gotoh score of ONE pair over caller-owned device buffers, with no
+ * device memory allocation: for callers that cannot call cudaMalloc/cudaFree
+ * (code running inside a global-mode stream capture, latency-bound serving
+ * threads that cannot take the implicit synchronisation of cudaFree, processes
+ * whose device memory belongs to another allocator's pool).  No counterpart in
+ * the reference: it is an addition of this library.
+ *   d_rows:   device int32 [m][21] score rows (the ScoreTable layout), m <= 2^20
+ *   d_target: device residue codes, n <= 65536 (longer targets: ST_EINVAL)
+ *   d_score:  device int32 receiving the score (0 when m or n is 0)
+ * Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).  The
+ * kernel's scratch is a fixed 512 KiB static device array that every GPU
+ * loading the library holds until exit; all calls on a device share it, so
+ * calls that overlap on the GPU race and must be ordered by the caller.  The
+ * first call on a device resolves the array's address; make it before any
+ * stream capture.  Same scores as st_sw_score for every gap cost. */
+int st_sw_score_noalloc(const int32_t* d_rows, uint32_t m, const uint8_t* d_target, uint32_t n, int32_t open,
+                        int32_t ext, int32_t* d_score, void* stream);
+
 /* ---- measurement helpers -------------------------------------------------- */
 /* Device-wide throughput of the packed s16x2 DPX add-max instruction
  * (__viaddmax_s16x2), in lane-operations per second, measured on the current

@@ -70,6 +70,7 @@ SIGNATURES = {
     "st_tune_get": (C.c_int, [_P, _P]),
     "st_tune_set": (C.c_int, [_P, _P]),
     "st_autotune": (C.c_int, [_P, _P, _u64, _i32, _i32, _u32, _P]),
+    "st_sw_score_noalloc": (C.c_int, [_P, _u32, _P, _u32, _i32, _i32, _P, _P]),
     "st_probe_dpx": (C.c_int, [_P, _P]),
     "st_launch_count": (C.c_int, [_P, _P]),
     "st_pssm_from_msa": (C.c_int, [_P, _u32, _u32, _P, _P, C.c_float, C.c_float, C.c_float, _P, _P]),

@@ -53,6 +53,9 @@ static int fail(int code, const char* fmt, ...) {
 
 extern "C" const char* st_last_error(void) { return g_last_error.c_str(); }
 
+// Lets other translation units of the library report through st_last_error().
+__attribute__((visibility("hidden"))) void st_internal_set_error(const char* msg) { g_last_error = msg; }
+
 // ---------------------------------------------------------------------------
 // device memory with budget accounting
 // ---------------------------------------------------------------------------
