@@ -57,6 +57,14 @@ void or_ungapped_hits(const int32_t* rows_arena, const uint64_t* row_off, const 
                       const uint8_t* tgt_arena, const uint64_t* tgt_off, const uint32_t* hq, const uint32_t* ht,
                       const int32_t* hd, uint64_t n_hits, int32_t* out, int nthreads);
 
+/* CPU baseline (striped.c): the reference's default AVX2 path (u8 striped -> i16 striped ->
+ * scalar) over pairs grouped by query; query q's targets are tlist[qstart[q] .. qstart[q+1]).
+ * used[k] (may be NULL): 1 = u8 pass decided, 2 = i16, 3 = scalar, 0 = empty input. */
+void or_striped_queries(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen, uint32_t n_queries,
+                        const uint8_t* tgt_arena, const uint64_t* tgt_off, const uint64_t* qstart,
+                        const uint32_t* tlist, int32_t open, int32_t ext, int32_t* out, uint8_t* used,
+                        int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,6 +39,7 @@ def _load():
     lib.or_band_score.argtypes = [P, u32, P, u32, i32, i32, i64, i64]
     lib.or_sw_pairs.argtypes = [P, P, P, P, P, P, P, P, P, u64, i32, i32, P, C.c_int]
     lib.or_ungapped_hits.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
+    lib.or_striped_queries.argtypes = [P, P, P, u32, P, P, P, P, i32, i32, P, P, C.c_int]
     return lib
 
 
@@ -135,3 +136,24 @@ def ungapped_hits(arena: Arena, hq, ht, hd, threads=0):
     lib.or_ungapped_hits(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(arena.tgt), _p(arena.tgt_off),
                          _p(hq), _p(ht), _p(hd), n, _p(out), threads or os.cpu_count() or 1)
     return out
+
+
+def striped_pairs(arena: Arena, pq, pt, open_, ext, threads=0, with_kinds=False):
+    """The reference's default AVX2 CPU path over pairs (grouped by query internally), results in pair order."""
+    pq = np.asarray(pq, dtype=np.uint32)
+    pt = np.asarray(pt, dtype=np.uint32)
+    order = np.argsort(pq, kind="stable")
+    nq = len(arena.qlen)
+    counts = np.bincount(pq, minlength=nq).astype(np.uint64)
+    qstart = np.zeros(nq + 1, dtype=np.uint64)
+    qstart[1:] = np.cumsum(counts)
+    tlist = np.ascontiguousarray(pt[order])
+    out = np.zeros(len(pq), dtype=np.int32)
+    used = np.zeros(len(pq), dtype=np.uint8)
+    lib.or_striped_queries(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), nq, _p(arena.tgt), _p(arena.tgt_off),
+                           _p(qstart), _p(tlist), open_, ext, _p(out), _p(used), threads or os.cpu_count() or 1)
+    res = np.zeros_like(out)
+    res[order] = out
+    kinds = np.zeros_like(used)
+    kinds[order] = used
+    return (res, kinds) if with_kinds else res

@@ -151,3 +151,36 @@ def test_diag_range():
     assert O.diag_range(10, 5, 2) == (0, 3)
     assert O.diag_range(10, 5, 5) == (0, 0)
     assert O.diag_range(10, 5, -10) == (0, 0)
+
+
+def test_striped_cpu_baseline_equals_scalar_oracle():
+    """The AVX2 restatement of the reference's CPU path (the timed CPU baseline) gives the oracle's scores,
+    including u8 headroom fallbacks, i16 saturation and gap costs that force the scalar path."""
+    from sabertooth_b200 import workloads as W
+    m = blosum62()
+    rng = XorShift(777)
+    rows_list, targets, pq, pt = [], [], [], []
+    for i in range(120):
+        q = rand_seq(rng, 1 + rng.range(140), 2 + rng.range(19))
+        t = rand_seq(rng, 1 + rng.range(200), 2 + rng.range(19))
+        if i % 5 == 0:
+            p = rng.range(len(t) + 1)
+            t = t[:p] + q + t[p:]
+        rows_list.append(m.sequence_rows(q))
+        targets.append(t)
+        pq.append(i)
+        pt.append(i)
+    w = np.full(4000, int(encode("W")[0]), dtype=np.uint8)
+    rows_list.append(m.sequence_rows(w))
+    targets.append(w)
+    pq.append(len(rows_list) - 1)
+    pt.append(len(targets) - 1)
+    ar = O.Arena(rows_list, targets)
+    for open_, ext in [(11, 1), (6, 2), (5, 5), (1, 1), (44, 4), (300, 1)]:
+        want = O.sw_pairs(ar, pq, pt, open_, ext)
+        got, kinds = O.striped_pairs(ar, pq, pt, open_, ext, with_kinds=True)
+        assert np.array_equal(got, want), (open_, ext)
+    assert kinds[-1] == 3  # the saturating W x 4000 pair falls back to the scalar path
+    pw = W.config3(seed=5, n_queries=10, db_residues=30_000, per_query=30)
+    ar = O.Arena(pw.rows, pw.targets())
+    assert np.array_equal(O.striped_pairs(ar, pw.pair_q, pw.pair_t, 44, 4), O.sw_pairs(ar, pw.pair_q, pw.pair_t, 44, 4))
