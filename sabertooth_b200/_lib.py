@@ -61,6 +61,7 @@ SIGNATURES = {
     "st_plan_create": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P, _P]),
     "st_plan_run": (C.c_int, [_P]),
     "st_plan_stats": (C.c_int, [_P, _P, _P, _P]),
+    "st_plan_profile": (C.c_int, [_P, _u32, _P, _P, _P, _P]),
     "st_plan_destroy": (None, [_P]),
     "st_ungapped_score": (C.c_int, [_P, _u32, _P, _u32, _P]),
     "st_ungapped_hits": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),

@@ -129,6 +129,15 @@ class Context:
         check(lib.st_profiles_create(self._h, ptr(arena), ptr(offs), len(arrs), ptr(ids)))
         return ids
 
+    def create_profiles_arena(self, rows_arena, row_offsets):
+        """Profiles from one int32 [total_rows][21] arena; profile k = rows row_offsets[k]..row_offsets[k+1]."""
+        arena = np.ascontiguousarray(rows_arena, dtype=np.int32)
+        offs = np.ascontiguousarray(row_offsets, dtype=np.uint64)
+        ids = np.zeros(len(offs) - 1, dtype=np.uint32)
+        if len(ids):
+            check(lib.st_profiles_create(self._h, ptr(arena), ptr(offs), len(ids), ptr(ids)))
+        return ids
+
     def free_profile(self, pid):
         check(lib.st_profile_free(self._h, int(pid)))
 
@@ -246,6 +255,17 @@ class Plan:
         cells, resc, ncls = C.c_uint64(), C.c_uint64(), C.c_uint32()
         check(lib.st_plan_stats(self._h, C.byref(cells), C.byref(resc), C.byref(ncls)))
         return {"cells": cells.value, "rescored_pairs": resc.value, "launch_classes": ncls.value}
+
+    def profile(self):
+        """Each launch alone: [(tile class (G, R) or None for the 32-bit kernel, cells, ms)]."""
+        cap = 32
+        cls = np.zeros(cap, dtype=np.int32)
+        cells = np.zeros(cap, dtype=np.uint64)
+        ms = np.zeros(cap, dtype=np.float32)
+        n = C.c_uint32()
+        check(lib.st_plan_profile(self._h, cap, ptr(cls), ptr(cells), ptr(ms), C.byref(n)))
+        shapes = tile_classes()
+        return [(shapes[cls[i]] if cls[i] >= 0 else None, int(cells[i]), float(ms[i])) for i in range(n.value)]
 
     def close(self):
         if self._h:

@@ -213,7 +213,31 @@ struct st_ctx {
   DevMem stage;
   DevMem scratch_small;
   Tuning tuning;
+  std::vector<DevMem> pool;  // device arenas of finished plans, reused by later plans
 };
+
+// A device buffer of at least `bytes` from the context's pool (or a new allocation).
+static int pool_get(st_ctx* c, size_t bytes, DevMem& out) {
+  int best = -1;
+  for (size_t i = 0; i < c->pool.size(); ++i)
+    if (c->pool[i].bytes >= bytes && c->pool[i].bytes <= 4 * bytes + (64 << 20) &&
+        (best < 0 || c->pool[i].bytes < c->pool[best].bytes))
+      best = static_cast<int>(i);
+  if (best >= 0) {
+    out = std::move(c->pool[best]);
+    c->pool.erase(c->pool.begin() + best);
+    return ST_OK;
+  }
+  return dev_alloc(&c->mt, out, bytes + bytes / 8);
+}
+
+static void pool_put(st_ctx* c, DevMem&& m) {
+  if (!m.p) return;
+  c->pool.push_back(std::move(m));
+  while (c->pool.size() > 4) {  // keep the four most recent arenas
+    c->pool.erase(c->pool.begin());
+  }
+}
 
 static DeviceDb db_view(st_ctx* c) {
   DeviceDb d;
@@ -417,16 +441,27 @@ extern "C" int st_db_info(st_ctx* c, uint32_t* n_seqs, uint64_t* n_residues) {
 // ---------------------------------------------------------------------------
 // profiles
 // ---------------------------------------------------------------------------
-// Builds the residue-major int8 and int32 layouts from int32 [m][21] rows.
-__global__ void build_profile_kernel(const int32_t* rows, uint32_t m, int8_t* p8, uint32_t stride8, int32_t* p32,
-                                     uint32_t stride32, int fits8) {
-  const uint32_t total = kProfRows * stride32;
-  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
-    const uint32_t r = idx / stride32;
-    const uint32_t i = idx - r * stride32;
-    const int32_t v = (i < m && r < static_cast<uint32_t>(kAlpha)) ? rows[static_cast<size_t>(i) * kAlpha + r] : 0;
+// Builds the residue-major int8 and int32 layouts of many profiles from their
+// int32 [m][21] rows: one CTA per profile.
+struct ProfBuildDesc {
+  uint64_t src_row;  // first row in the uploaded rows
+  uint64_t o8, o32;  // byte offsets of the int8 / int32 layouts in the block
+  uint32_t m, stride8, stride32, fits8;
+};
+
+__global__ void __launch_bounds__(256) build_profiles_kernel(const int32_t* __restrict__ rows,
+                                                             const ProfBuildDesc* __restrict__ desc, char* base) {
+  const ProfBuildDesc d = desc[blockIdx.x];
+  const int32_t* src = rows + d.src_row * kAlpha;
+  int32_t* p32 = reinterpret_cast<int32_t*>(base + d.o32);
+  int8_t* p8 = reinterpret_cast<int8_t*>(base + d.o8);
+  const uint32_t total = kProfRows * d.stride32;
+  for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+    const uint32_t r = idx / d.stride32;
+    const uint32_t i = idx - r * d.stride32;
+    const int32_t v = (i < d.m && r < static_cast<uint32_t>(kAlpha)) ? src[static_cast<size_t>(i) * kAlpha + r] : 0;
     p32[idx] = v;
-    if (i < stride8) p8[static_cast<size_t>(r) * stride8 + i] = fits8 ? static_cast<int8_t>(v) : 0;
+    if (i < d.stride8) p8[static_cast<size_t>(r) * d.stride8 + i] = d.fits8 ? static_cast<int8_t>(v) : 0;
   }
 }
 
@@ -435,68 +470,70 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   CTX_GUARD(c);
   if (!row_offsets || !ids || (!rows && n_profiles && row_offsets[n_profiles] > row_offsets[0]))
     return fail(ST_EINVAL, "st_profiles_create: null input");
-  struct Item {
-    uint32_t m, stride8, stride32;
-    int32_t mx;
-    bool fits8;
-    size_t o8, o32, orows;
-  };
-  std::vector<Item> it(n_profiles);
-  size_t bytes8 = 0, bytes32 = 0, rows_total = 0;
+  if (n_profiles == 0) return ST_OK;
+  std::vector<ProfBuildDesc> desc(n_profiles);
+  std::vector<int32_t> mx(n_profiles);
   for (uint32_t k = 0; k < n_profiles; ++k) {
     if (row_offsets[k + 1] < row_offsets[k]) return fail(ST_EINVAL, "st_profiles_create: offsets decrease");
+    if (row_offsets[k + 1] - row_offsets[k] > (1u << 20))
+      return fail(ST_EINVAL, "st_profiles_create: query of %llu rows exceeds 2^20",
+                  static_cast<unsigned long long>(row_offsets[k + 1] - row_offsets[k]));
+  }
+  // score range per profile (residues >= 21 score 0), in parallel over profiles
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) {
     const uint64_t m = row_offsets[k + 1] - row_offsets[k];
-    if (m > (1u << 20)) return fail(ST_EINVAL, "st_profiles_create: query of %llu rows exceeds 2^20",
-                                    static_cast<unsigned long long>(m));
-    Item& x = it[k];
-    x.m = static_cast<uint32_t>(m);
-    int32_t lo = 0, hi = 0;  // residues >= 21 score 0
+    int32_t lo = 0, hi = 0;
     const int32_t* r = rows + row_offsets[k] * kAlpha;
     for (size_t i = 0; i < m * kAlpha; ++i) {
       lo = std::min(lo, r[i]);
       hi = std::max(hi, r[i]);
     }
-    x.mx = hi;
-    x.fits8 = lo >= -128 && hi <= 127;
-    x.stride8 = static_cast<uint32_t>(std::max<size_t>(up16(m), 16));
-    x.stride32 = static_cast<uint32_t>(std::max<size_t>(up256(m), kSw32Rows));
-    x.o8 = bytes8;
-    bytes8 += up16(static_cast<size_t>(kProfRows) * x.stride8);
+    mx[k] = hi;
+    desc[k].m = static_cast<uint32_t>(m);
+    desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
+  }
+  size_t bytes8 = 0, bytes32 = 0;
+  for (uint32_t k = 0; k < n_profiles; ++k) {
+    ProfBuildDesc& x = desc[k];
+    x.src_row = row_offsets[k] - row_offsets[0];
+    x.stride8 = static_cast<uint32_t>(std::max<size_t>(up16(x.m), 16));
+    x.stride32 = static_cast<uint32_t>(std::max<size_t>(up256(x.m), kSw32Rows));
     x.o32 = bytes32;
     bytes32 += static_cast<size_t>(kProfRows) * x.stride32 * 4;
-    x.orows = rows_total;
-    rows_total += m;
   }
-  auto blk = std::make_unique<ProfileBlock>();
+  for (uint32_t k = 0; k < n_profiles; ++k) {
+    desc[k].o8 = bytes32 + bytes8;
+    bytes8 += up16(static_cast<size_t>(kProfRows) * desc[k].stride8);
+  }
+  const size_t rows_total = row_offsets[n_profiles] - row_offsets[0];
   const size_t src_bytes = rows_total * kAlpha * 4;
-  ST_TRY(dev_alloc(&c->mt, blk->mem, bytes32 + bytes8 + src_bytes + 64));
+  const size_t desc_bytes = up16(n_profiles * sizeof(ProfBuildDesc));
+  auto blk = std::make_unique<ProfileBlock>();
+  ST_TRY(dev_alloc(&c->mt, blk->mem, bytes32 + bytes8));
+  DevMem tmp;  // uploaded rows and descriptors, freed once the layouts are built
+  ST_TRY(dev_alloc(&c->mt, tmp, src_bytes + desc_bytes + 16));
   char* base = blk->mem.as<char>();
-  int32_t* d_src = reinterpret_cast<int32_t*>(base + bytes32 + bytes8);
+  int32_t* d_src = tmp.as<int32_t>();
+  ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + up16(src_bytes));
   if (src_bytes)
     ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->own));
-  for (uint32_t k = 0; k < n_profiles; ++k) {
-    const Item& x = it[k];
-    int32_t* p32 = reinterpret_cast<int32_t*>(base + x.o32);
-    int8_t* p8 = reinterpret_cast<int8_t*>(base + bytes32 + x.o8);
-    const uint32_t total = kProfRows * x.stride32;
-    const int grid = std::min<uint32_t>((total + 255) / 256, 1024);
-    build_profile_kernel<<<grid, 256, 0, c->own>>>(d_src + x.orows * kAlpha, x.m, p8, x.stride8, p32, x.stride32,
-                                                    x.fits8 ? 1 : 0);
-    ++c->launches;
-  }
+  ST_CUDA(cudaMemcpyAsync(d_desc, desc.data(), n_profiles * sizeof(ProfBuildDesc), cudaMemcpyHostToDevice, c->own));
+  build_profiles_kernel<<<n_profiles, 256, 0, c->own>>>(d_src, d_desc, base);
+  ++c->launches;
   ST_CUDA(cudaGetLastError());
   ST_CUDA(cudaStreamSynchronize(c->own));
   const int bi = static_cast<int>(c->blocks.size());
   for (uint32_t k = 0; k < n_profiles; ++k) {
-    const Item& x = it[k];
+    const ProfBuildDesc& x = desc[k];
     ProfileMeta pm;
     pm.m = x.m;
-    pm.max_score = x.mx;
-    pm.fits8 = x.fits8;
+    pm.max_score = mx[k];
+    pm.fits8 = x.fits8 != 0;
     pm.live = true;
     pm.block = bi;
     pm.p32 = reinterpret_cast<const int32_t*>(base + x.o32);
-    pm.p8 = reinterpret_cast<const int8_t*>(base + bytes32 + x.o8);
+    pm.p8 = reinterpret_cast<const int8_t*>(base + x.o8);
     pm.stride8 = x.stride8;
     pm.stride32 = x.stride32;
     ids[k] = static_cast<uint32_t>(c->profs.size());
@@ -540,15 +577,55 @@ static inline bool gaps16_ok(int32_t open, int32_t ext) {
   return open >= 0 && ext >= 0 && static_cast<int64_t>(open) + ext <= 16384;
 }
 
-static uint64_t band_cells(uint32_t m, uint32_t n, int64_t center, int64_t radius) {
-  // cells (i, j), 1-based, with |j - i - center| <= radius
-  uint64_t cells = 0;
-  for (uint32_t i = 1; i <= m; ++i) {
-    const int64_t lo = std::max<int64_t>(1, i + center - radius);
-    const int64_t hi = std::min<int64_t>(n, i + center + radius);
-    if (hi >= lo) cells += static_cast<uint64_t>(hi - lo + 1);
+static int64_t linear_pos_sum(int64_t s, int64_t e, int64_t a, int b) {
+  // sum over i in [s, e] of max(0, a + b*i), b in {-1, 0, 1}
+  if (e < s) return 0;
+  if (b == 0) return a > 0 ? (e - s + 1) * a : 0;
+  if (b == 1) {
+    const int64_t i0 = std::max(s, 1 - a);
+    if (i0 > e) return 0;
+    const int64_t k = e - i0 + 1;
+    return k * a + (i0 + e) * k / 2;
   }
-  return cells;
+  const int64_t i1 = std::min(e, a - 1);
+  if (i1 < s) return 0;
+  const int64_t k = i1 - s + 1;
+  return k * a - (s + i1) * k / 2;
+}
+
+static uint64_t band_cells(uint32_t m, uint32_t n, int64_t c, int64_t r) {
+  // cells (i, j), 1-based, with |j - i - c| <= r: row i spans [max(1, i+c-r), min(n, i+c+r)]
+  if (m == 0 || n == 0 || r < 0) return 0;
+  int64_t p1 = 2 - c + r;                   // from here on the left end is i + c - r
+  int64_t p2 = static_cast<int64_t>(n) - c - r + 1;  // from here on the right end is n
+  const int64_t lo = 1, hi = static_cast<int64_t>(m) + 1;
+  p1 = std::min(std::max(p1, lo), hi);
+  p2 = std::min(std::max(p2, lo), hi);
+  const int64_t cuts[4] = {lo, std::min(p1, p2), std::max(p1, p2), hi};
+  int64_t total = 0;
+  for (int g = 0; g < 3; ++g) {
+    const int64_t s = cuts[g], e = cuts[g + 1] - 1;
+    if (e < s) continue;
+    const bool left1 = s + c - r <= 1;
+    const bool rightA = s + c + r <= static_cast<int64_t>(n);
+    int64_t a;
+    int b;
+    if (left1 && rightA) {
+      a = c + r;
+      b = 1;
+    } else if (left1) {
+      a = n;
+      b = 0;
+    } else if (rightA) {
+      a = 2 * r + 1;
+      b = 0;
+    } else {
+      a = static_cast<int64_t>(n) - c + r + 1;
+      b = -1;
+    }
+    total += linear_pos_sum(s, e, a, b);
+  }
+  return static_cast<uint64_t>(total);
 }
 
 struct ClassPlan {
@@ -556,10 +633,12 @@ struct ClassPlan {
   std::vector<Sw16CtaTask> cta;
   std::vector<Sw16WarpTask> wt;
   std::vector<uint32_t> slots;
-  DevMem d_cta, d_wt, d_slots, d_scratch;
+  size_t o_cta = 0, o_wt = 0, o_slots = 0, o_scratch = 0;  // offsets in the plan's device arena
   uint32_t grid = 0;
   uint32_t smem = 0;
   uint32_t scratch_stride = 0;
+  uint64_t cells = 0;  // sum of m*n over this class's pairs
+  Sw16Params prm;
 };
 
 struct st_plan {
@@ -569,12 +648,15 @@ struct st_plan {
   int32_t* d_scores = nullptr;
   uint32_t* d_kernels = nullptr;
   std::vector<ClassPlan> classes;
-  DevMem d_pair_q, d_pair_t, d_pair_c, d_pair_r;
-  DevMem d_list, d_counters, d_counters_init, d_scratch32;
+  DevMem arena;  // every device buffer of the plan (from the context's pool)
+  uint32_t* counters = nullptr;
+  const uint32_t* counters_init = nullptr;
   uint32_t n_static32 = 0;
   uint32_t grid32 = 0, scratch32_stride = 0;
   uint64_t cells = 0;
+  uint64_t cells32 = 0;  // cells of pairs sent to the 32-bit kernel at plan time (band cells for bands)
   uint32_t kernels_per_run = 0;
+  Sw32Params p32;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -624,8 +706,24 @@ static void emit_query(ClassPlan& cp, const Sw16Class& k, uint32_t q, uint32_t m
   }
 }
 
+// The launches of one run, in stream order: clear outputs, reset counters,
+// every 16-bit class, then the 32-bit kernel over the static list plus the
+// pairs the 16-bit classes flagged.
+static int plan_enqueue(st_plan* p, cudaStream_t st) {
+  if (p->n) {
+    if (cudaMemsetAsync(p->d_scores, 0, p->n * 4, st) != cudaSuccess) return ST_ECUDA;
+    if (p->d_kernels && cudaMemsetAsync(p->d_kernels, 0, p->n * 4, st) != cudaSuccess) return ST_ECUDA;
+  }
+  if (cudaMemcpyAsync(p->counters, p->counters_init, (kNumClasses + 2) * 4, cudaMemcpyDeviceToDevice, st) !=
+      cudaSuccess)
+    return ST_ECUDA;
+  for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, st>>>(cp.prm);
+  sw32_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, st>>>(p->p32);
+  return cudaGetLastError() == cudaSuccess ? ST_OK : ST_ECUDA;
+}
+
 static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* d_scores,
-                      uint32_t* d_kernels, st_plan** out) {
+                      uint32_t* d_kernels, st_plan** out, bool capture) {
   if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
   if (n > 0xFFFFFFF0ull) return fail(ST_EINVAL, "too many pairs (%llu)", static_cast<unsigned long long>(n));
   ST_TRY(sync_profiles(c));
@@ -638,63 +736,113 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   plan->d_kernels = d_kernels;
   const bool g16 = gaps16_ok(open, ext);
 
-  std::vector<uint32_t> pq(n), pt(n);
+  std::vector<uint32_t> pq(n), pt(n), tlen(n);
   std::vector<int32_t> pc(n), pr(n);
-  std::vector<uint32_t> list32;
-  // per query: pairs for the 16-bit kernel
-  std::vector<std::vector<uint32_t>> byq(c->profs.size());
+  std::vector<uint8_t> route(n);  // 0: score 0 (empty), 1: 16-bit kernel, 2: 32-bit kernel
+  const uint32_t n_prof = static_cast<uint32_t>(c->profs.size());
+  int64_t bad = -1;
+  uint64_t cells = 0, cells32 = 0;
   uint32_t max_len = 0, max_m32 = 0;
-  for (uint64_t i = 0; i < n; ++i) {
+  // classify every pair (validation, route, cells), in parallel
+#pragma omp parallel for schedule(static) reduction(+ : cells, cells32) reduction(max : max_len, max_m32)
+  for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
     const st_pair& p = pairs[i];
-    if (p.profile >= c->profs.size() || !c->profs[p.profile].live)
-      return fail(ST_EINVAL, "pair %llu: unknown profile id %u", static_cast<unsigned long long>(i), p.profile);
-    if (p.target >= c->n_seqs)
-      return fail(ST_EINVAL, "pair %llu: target %u outside the database (%u sequences)",
-                  static_cast<unsigned long long>(i), p.target, c->n_seqs);
+    if (p.profile >= n_prof || !c->profs[p.profile].live || p.target >= c->n_seqs) {
+#pragma omp critical
+      if (bad < 0 || i < bad) bad = i;
+      continue;
+    }
     pq[i] = p.profile;
     pt[i] = p.target;
     pc[i] = p.band_center;
     pr[i] = p.band_radius;
     const ProfileMeta& pm = c->profs[p.profile];
     const uint32_t tl = c->h_db_len[p.target];
-    if (pm.m == 0 || tl == 0) continue;  // score 0, kernel NONE
+    tlen[i] = tl;
+    if (pm.m == 0 || tl == 0) {
+      route[i] = 0;
+      continue;
+    }
     max_len = std::max(max_len, tl);
+    max_m32 = std::max(max_m32, pm.m);  // every 16-bit pair may be rescored in 32 bits
     if (p.band_radius >= 0) {
-      plan->cells += band_cells(pm.m, tl, p.band_center, p.band_radius);
-      list32.push_back(static_cast<uint32_t>(i));
-      max_m32 = std::max(max_m32, pm.m);
+      const uint64_t bc = band_cells(pm.m, tl, p.band_center, p.band_radius);
+      cells += bc;
+      cells32 += bc;
+      route[i] = 2;
     } else {
-      plan->cells += static_cast<uint64_t>(pm.m) * tl;
-      // every 16-bit pair may be rescored in 32 bits
-      max_m32 = std::max(max_m32, pm.m);
-      if (g16 && pm.fits8)
-        byq[p.profile].push_back(static_cast<uint32_t>(i));
-      else
-        list32.push_back(static_cast<uint32_t>(i));
+      const uint64_t mc = static_cast<uint64_t>(pm.m) * tl;
+      cells += mc;
+      if (g16 && pm.fits8) {
+        route[i] = 1;
+      } else {
+        route[i] = 2;
+        cells32 += mc;
+      }
     }
   }
-
-  // classes: tiles chosen per query length (tuning table)
+  if (bad >= 0) {
+    const st_pair& p = pairs[bad];
+    if (p.profile >= n_prof || !c->profs[p.profile].live)
+      return fail(ST_EINVAL, "pair %lld: unknown profile id %u", static_cast<long long>(bad), p.profile);
+    return fail(ST_EINVAL, "pair %lld: target %u outside the database (%u sequences)", static_cast<long long>(bad),
+                p.target, c->n_seqs);
+  }
+  plan->cells = cells;
+  plan->cells32 = cells32;
+  // 32-bit list in pair order; 16-bit pairs grouped by query (counting sort)
+  std::vector<uint32_t> list32;
+  std::vector<uint64_t> qstart(static_cast<size_t>(n_prof) + 1, 0);
+  for (uint64_t i = 0; i < n; ++i) {
+    if (route[i] == 2) list32.push_back(static_cast<uint32_t>(i));
+    else if (route[i] == 1) ++qstart[pq[i] + 1];
+  }
+  for (uint32_t q = 0; q < n_prof; ++q) qstart[q + 1] += qstart[q];
+  std::vector<uint32_t> byq(qstart[n_prof]);
+  {
+    std::vector<uint64_t> fill(qstart.begin(), qstart.end() - 1);
+    for (uint64_t i = 0; i < n; ++i)
+      if (route[i] == 1) byq[fill[pq[i]]++] = static_cast<uint32_t>(i);
+  }
+  // per query (in parallel): targets longest first, then the tile class
+  std::vector<uint32_t> qlist;
+  for (uint32_t q = 0; q < n_prof; ++q)
+    if (qstart[q + 1] > qstart[q]) qlist.push_back(q);
+  std::vector<int> qclass(qlist.size());
+  std::vector<uint64_t> qsum(qlist.size());
+  int toolong = -1;
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int64_t k = 0; k < static_cast<int64_t>(qlist.size()); ++k) {
+    const uint32_t q = qlist[k];
+    uint32_t* v0 = byq.data() + qstart[q];
+    uint32_t* v1 = byq.data() + qstart[q + 1];
+    std::stable_sort(v0, v1, [&](uint32_t a, uint32_t b) { return tlen[a] > tlen[b]; });
+    uint64_t sum_n = 0;
+    for (uint32_t* it = v0; it != v1; ++it) sum_n += tlen[*it];
+    const uint32_t m = c->profs[q].m;
+    const int cls = tuning_pick(&c->tuning, m, static_cast<uint32_t>(sum_n / (v1 - v0)));
+    const uint32_t rows = kClasses[cls].G * kClasses[cls].R;
+    const uint32_t P = (m + rows - 1) / rows;
+    if (static_cast<uint64_t>(kProfRows) * P * rows > kMaxSmem) {
+#pragma omp critical
+      toolong = static_cast<int>(m);
+    }
+    qclass[k] = cls;
+    qsum[k] = sum_n;
+  }
+  if (toolong >= 0) return fail(ST_EINVAL, "query of %d rows does not fit the shared-memory profile", toolong);
   std::vector<ClassPlan> cps(kNumClasses);
   for (int k = 0; k < kNumClasses; ++k) cps[k].cls = k;
   std::vector<uint32_t> tl;
-  for (uint32_t q = 0; q < byq.size(); ++q) {
-    auto& v = byq[q];
-    if (v.empty()) continue;
-    std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) { return c->h_db_len[pt[a]] > c->h_db_len[pt[b]]; });
+  for (size_t k = 0; k < qlist.size(); ++k) {
+    const uint32_t q = qlist[k];
+    const int cls = qclass[k];
+    const uint64_t a0 = qstart[q], a1 = qstart[q + 1];
+    std::vector<uint32_t> v(byq.begin() + a0, byq.begin() + a1);
     tl.resize(v.size());
-    uint64_t sum_n = 0;
-    for (size_t j = 0; j < v.size(); ++j) {
-      tl[j] = c->h_db_len[pt[v[j]]];
-      sum_n += tl[j];
-    }
-    const uint32_t m = c->profs[q].m;
-    const int k = tuning_pick(&c->tuning, m, static_cast<uint32_t>(sum_n / v.size()));
-    const uint32_t rows = kClasses[k].G * kClasses[k].R;
-    const uint32_t P = (m + rows - 1) / rows;
-    if (static_cast<uint64_t>(kProfRows) * P * rows > kMaxSmem)
-      return fail(ST_EINVAL, "query of %u rows does not fit the shared-memory profile", m);
-    emit_query(cps[k], kClasses[k], q, m, v, tl, 64);
+    for (size_t j = 0; j < v.size(); ++j) tl[j] = tlen[v[j]];
+    emit_query(cps[cls], kClasses[cls], q, c->profs[q].m, v, tl, 64);
+    cps[cls].cells += static_cast<uint64_t>(c->profs[q].m) * qsum[k];
   }
 
   // order CTA tasks by estimated cost, longest first
@@ -715,32 +863,11 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     cp.cta.swap(sorted);
   }
 
-  // device buffers
-  auto upload = [&](DevMem& d, const void* src, size_t bytes) -> int {
-    ST_TRY(dev_alloc(&c->mt, d, bytes));
-    if (bytes) ST_CUDA(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, c->own));
-    return ST_OK;
-  };
-  ST_TRY(upload(plan->d_pair_q, pq.data(), n * 4));
-  ST_TRY(upload(plan->d_pair_t, pt.data(), n * 4));
-  ST_TRY(upload(plan->d_pair_c, pc.data(), n * 4));
-  ST_TRY(upload(plan->d_pair_r, pr.data(), n * 4));
-  // 32-bit list: static entries first, then room for every 16-bit pair
-  plan->n_static32 = static_cast<uint32_t>(list32.size());
-  ST_TRY(dev_alloc(&c->mt, plan->d_list, std::max<size_t>(n, 1) * 4));
-  if (!list32.empty())
-    ST_CUDA(cudaMemcpyAsync(plan->d_list.p, list32.data(), list32.size() * 4, cudaMemcpyHostToDevice, c->own));
-  // counters: [0, kNumClasses) class work, [kNumClasses] 32-bit work, [kNumClasses+1] list count
-  std::vector<uint32_t> cinit(kNumClasses + 2, 0);
-  cinit[kNumClasses + 1] = plan->n_static32;
-  ST_TRY(upload(plan->d_counters_init, cinit.data(), cinit.size() * 4));
-  ST_TRY(dev_alloc(&c->mt, plan->d_counters, cinit.size() * 4));
-
-  const DeviceDb db = db_view(c);
-  const DeviceProfiles pv = prof_view(c);
-  uint32_t* counters = plan->d_counters.as<uint32_t>();
+  // launch shapes and scratch needs
+  uint32_t nonempty = 0;
   for (auto& cp : cps) {
     if (cp.cta.empty()) continue;
+    ++nonempty;
     const Sw16Class& k = kClasses[cp.cls];
     uint32_t max_mpad = 0, max_cols = 0;
     bool multi = false;
@@ -752,91 +879,148 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     cp.smem = kProfRows * max_mpad;
     ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(k.fn), kWarps16 * 32, cp.smem,
                           static_cast<uint32_t>(cp.cta.size()), &cp.grid));
-    ST_TRY(upload(cp.d_cta, cp.cta.data(), cp.cta.size() * sizeof(Sw16CtaTask)));
-    ST_TRY(upload(cp.d_wt, cp.wt.data(), cp.wt.size() * sizeof(Sw16WarpTask)));
-    ST_TRY(upload(cp.d_slots, cp.slots.data(), cp.slots.size() * 4));
     cp.scratch_stride = multi ? max_cols : 0;
-    const size_t groups = static_cast<size_t>(cp.grid) * kWarps16 * (32 / k.G);
-    ST_TRY(dev_alloc(&c->mt, cp.d_scratch, multi ? groups * max_cols * sizeof(uint2) : 16));
   }
-  for (auto& cp : cps)
-    if (!cp.cta.empty()) plan->classes.push_back(std::move(cp));
-
   // 32-bit kernel: a few persistent CTAs (rescoring is rare)
   ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0,
                         2 * c->sms, &plan->grid32));
   plan->grid32 = std::min<uint32_t>(plan->grid32, 2 * c->sms);
   plan->scratch32_stride = max_m32 > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
-  ST_TRY(dev_alloc(&c->mt, plan->d_scratch32,
-                   plan->scratch32_stride
-                       ? static_cast<size_t>(plan->grid32) * kWarps32 * plan->scratch32_stride * sizeof(int2)
-                       : 16));
-  ST_CUDA(cudaStreamSynchronize(c->own));
+  plan->n_static32 = static_cast<uint32_t>(list32.size());
 
-  // capture the run into a CUDA graph (on the context's own stream)
-  ST_CUDA(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-  int cap_err = ST_OK;
-  do {
-    if (n) {
-      if (cudaMemsetAsync(d_scores, 0, n * 4, c->own) != cudaSuccess) { cap_err = ST_ECUDA; break; }
-      if (d_kernels && cudaMemsetAsync(d_kernels, 0, n * 4, c->own) != cudaSuccess) { cap_err = ST_ECUDA; break; }
-    }
-    if (cudaMemcpyAsync(counters, plan->d_counters_init.p, (kNumClasses + 2) * 4, cudaMemcpyDeviceToDevice,
-                        c->own) != cudaSuccess) { cap_err = ST_ECUDA; break; }
-    uint32_t nk = 0;
-    for (auto& cp : plan->classes) {
-      const Sw16Class& k = kClasses[cp.cls];
-      Sw16Params prm;
-      prm.db = db;
-      prm.prof = pv;
-      prm.cta_tasks = cp.d_cta.as<Sw16CtaTask>();
-      prm.n_cta_tasks = static_cast<uint32_t>(cp.cta.size());
-      prm.warp_tasks = cp.d_wt.as<Sw16WarpTask>();
-      prm.slot_pair = cp.d_slots.as<uint32_t>();
-      prm.pair_target = plan->d_pair_t.as<uint32_t>();
-      prm.scores = d_scores;
-      prm.kernels = d_kernels;
-      prm.ovf_count = counters + kNumClasses + 1;
-      prm.ovf_pairs = plan->d_list.as<uint32_t>();
-      prm.work_counter = counters + cp.cls;
-      prm.scratch = cp.d_scratch.as<uint2>();
-      prm.scratch_stride = cp.scratch_stride;
-      prm.open = open;
-      prm.ext = ext;
-      k.fn<<<cp.grid, kWarps16 * 32, cp.smem, c->own>>>(prm);
-      ++nk;
-    }
-    Sw32Params p32;
+  // one device arena: [initialised data (one upload)] [scratch]
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~static_cast<size_t>(255);
+    return o;
+  };
+  const size_t o_pq = carve(n * 4), o_pt = carve(n * 4), o_pc = carve(n * 4), o_pr = carve(n * 4);
+  const size_t o_list = carve(std::max<uint64_t>(n, 1) * 4);
+  const size_t o_cinit = carve((kNumClasses + 2) * 4);
+  for (auto& cp : cps) {
+    if (cp.cta.empty()) continue;
+    cp.o_cta = carve(cp.cta.size() * sizeof(Sw16CtaTask));
+    cp.o_wt = carve(cp.wt.size() * sizeof(Sw16WarpTask));
+    cp.o_slots = carve(cp.slots.size() * 4);
+  }
+  const size_t data_bytes = off;
+  const size_t o_cnt = carve((kNumClasses + 2) * 4);
+  for (auto& cp : cps) {
+    if (cp.cta.empty() || !cp.scratch_stride) continue;
+    const size_t groups = static_cast<size_t>(cp.grid) * kWarps16 * (32 / kClasses[cp.cls].G);
+    cp.o_scratch = carve(groups * cp.scratch_stride * sizeof(uint2));
+  }
+  const size_t o_s32 = carve(plan->scratch32_stride
+                                 ? static_cast<size_t>(plan->grid32) * kWarps32 * plan->scratch32_stride * sizeof(int2)
+                                 : 16);
+  const size_t total_bytes = off;
+  ST_TRY(pool_get(c, total_bytes, plan->arena));
+  char* dbase = plan->arena.as<char>();
+  // stage the data region in pinned memory and upload it at once
+  ST_TRY(c->pin.reserve(data_bytes));
+  ST_CUDA(cudaStreamSynchronize(c->stream));  // the pinned block may still feed an earlier copy
+  char* h = c->pin.as<char>();
+#pragma omp parallel sections
+  {
+#pragma omp section
+    memcpy(h + o_pq, pq.data(), n * 4);
+#pragma omp section
+    memcpy(h + o_pt, pt.data(), n * 4);
+#pragma omp section
+    memcpy(h + o_pc, pc.data(), n * 4);
+#pragma omp section
+    memcpy(h + o_pr, pr.data(), n * 4);
+  }
+  if (!list32.empty()) memcpy(h + o_list, list32.data(), list32.size() * 4);
+  {
+    // counters: [0, kNumClasses) class work, [kNumClasses] 32-bit work, [kNumClasses+1] list count
+    uint32_t* ci = reinterpret_cast<uint32_t*>(h + o_cinit);
+    for (int k = 0; k < kNumClasses + 2; ++k) ci[k] = 0;
+    ci[kNumClasses + 1] = plan->n_static32;
+  }
+  for (auto& cp : cps) {
+    if (cp.cta.empty()) continue;
+    memcpy(h + cp.o_cta, cp.cta.data(), cp.cta.size() * sizeof(Sw16CtaTask));
+    memcpy(h + cp.o_wt, cp.wt.data(), cp.wt.size() * sizeof(Sw16WarpTask));
+    memcpy(h + cp.o_slots, cp.slots.data(), cp.slots.size() * 4);
+  }
+  ST_CUDA(cudaMemcpyAsync(dbase, h, data_bytes, cudaMemcpyHostToDevice, c->stream));
+  plan->counters = reinterpret_cast<uint32_t*>(dbase + o_cnt);
+  plan->counters_init = reinterpret_cast<const uint32_t*>(dbase + o_cinit);
+  for (auto& cp : cps)
+    if (!cp.cta.empty()) plan->classes.push_back(std::move(cp));
+
+  const DeviceDb db = db_view(c);
+  const DeviceProfiles pv = prof_view(c);
+  uint32_t* counters = plan->counters;
+  const uint32_t* d_pair_q = reinterpret_cast<const uint32_t*>(dbase + o_pq);
+  const uint32_t* d_pair_t = reinterpret_cast<const uint32_t*>(dbase + o_pt);
+  const int32_t* d_pair_c = reinterpret_cast<const int32_t*>(dbase + o_pc);
+  const int32_t* d_pair_r = reinterpret_cast<const int32_t*>(dbase + o_pr);
+  uint32_t* d_list = reinterpret_cast<uint32_t*>(dbase + o_list);
+
+  // kernel parameters (kept on the plan: the graph and the per-class profiler launch the same)
+  for (auto& cp : plan->classes) {
+    Sw16Params& prm = cp.prm;
+    prm.db = db;
+    prm.prof = pv;
+    prm.cta_tasks = reinterpret_cast<const Sw16CtaTask*>(dbase + cp.o_cta);
+    prm.n_cta_tasks = static_cast<uint32_t>(cp.cta.size());
+    prm.warp_tasks = reinterpret_cast<const Sw16WarpTask*>(dbase + cp.o_wt);
+    prm.slot_pair = reinterpret_cast<const uint32_t*>(dbase + cp.o_slots);
+    prm.pair_target = d_pair_t;
+    prm.scores = d_scores;
+    prm.kernels = d_kernels;
+    prm.ovf_count = counters + kNumClasses + 1;
+    prm.ovf_pairs = d_list;
+    prm.work_counter = counters + cp.cls;
+    prm.scratch = reinterpret_cast<uint2*>(dbase + cp.o_scratch);
+    prm.scratch_stride = cp.scratch_stride;
+    prm.open = open;
+    prm.ext = ext;
+  }
+  {
+    Sw32Params& p32 = plan->p32;
     p32.db = db;
     p32.prof = pv;
-    p32.list = plan->d_list.as<uint32_t>();
+    p32.list = d_list;
     p32.list_count = counters + kNumClasses + 1;
-    p32.pair_query = plan->d_pair_q.as<uint32_t>();
-    p32.pair_target = plan->d_pair_t.as<uint32_t>();
-    p32.pair_center = plan->d_pair_c.as<int32_t>();
-    p32.pair_radius = plan->d_pair_r.as<int32_t>();
+    p32.pair_query = d_pair_q;
+    p32.pair_target = d_pair_t;
+    p32.pair_center = d_pair_c;
+    p32.pair_radius = d_pair_r;
     p32.scores = d_scores;
     p32.kernels = d_kernels;
     p32.work_counter = counters + kNumClasses;
-    p32.scratch = plan->d_scratch32.as<int2>();
+    p32.scratch = reinterpret_cast<int2*>(dbase + o_s32);
     p32.scratch_stride = plan->scratch32_stride;
     p32.open = open;
     p32.ext = ext;
-    sw32_kernel<kWarps32><<<plan->grid32, kWarps32 * 32, 0, c->own>>>(p32);
-    ++nk;
-    plan->kernels_per_run = nk;
-  } while (0);
-  cudaError_t ce = cudaStreamEndCapture(c->own, &plan->graph);
-  if (cap_err != ST_OK || ce != cudaSuccess)
-    return fail(ST_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce != cudaSuccess ? ce : cudaGetLastError()));
-  ST_CUDA(cudaGraphInstantiate(&plan->exec, plan->graph, 0));
+  }
+
+  plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1;
+  if (capture) {
+    // capture a run into a CUDA graph on the context's own stream (ordered after the upload)
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    ST_CUDA(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
+    const int rc = plan_enqueue(plan.get(), c->own);
+    cudaError_t ce = cudaStreamEndCapture(c->own, &plan->graph);
+    if (rc != ST_OK || ce != cudaSuccess)
+      return fail(ST_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce != cudaSuccess ? ce : cudaGetLastError()));
+    ST_CUDA(cudaGraphInstantiate(&plan->exec, plan->graph, 0));
+  }
   *out = plan.release();
   return ST_OK;
 }
 
 static int plan_run(st_plan* p) {
   st_ctx* c = p->ctx;
-  ST_CUDA(cudaGraphLaunch(p->exec, c->stream));
+  if (p->exec) {
+    ST_CUDA(cudaGraphLaunch(p->exec, c->stream));
+  } else if (plan_enqueue(p, c->stream) != ST_OK) {
+    return fail(ST_ECUDA, "plan launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
   c->launches += p->kernels_per_run;
   return ST_OK;
 }
@@ -845,6 +1029,7 @@ static void plan_free(st_plan* p) {
   if (!p) return;
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
+  pool_put(p->ctx, std::move(p->arena));
   delete p;
 }
 
@@ -852,7 +1037,7 @@ extern "C" int st_plan_create(st_ctx* c, const st_pair* pairs, uint64_t n, int32
                               int32_t* d_scores, uint32_t* d_kernels, st_plan** plan) {
   CTX_GUARD(c);
   if (!plan || (n && (!pairs || !d_scores))) return fail(ST_EINVAL, "st_plan_create: null argument");
-  return plan_build(c, pairs, n, open, ext, d_scores, d_kernels, plan);
+  return plan_build(c, pairs, n, open, ext, d_scores, d_kernels, plan, true);
 }
 
 extern "C" int st_plan_run(st_plan* p) {
@@ -871,9 +1056,46 @@ extern "C" int st_plan_stats(st_plan* p, uint64_t* cells, uint64_t* rescored, ui
   if (rescored) {
     uint32_t cnt = 0;
     ST_CUDA(cudaStreamSynchronize(c->stream));
-    ST_CUDA(cudaMemcpy(&cnt, p->d_counters.as<uint32_t>() + kNumClasses + 1, 4, cudaMemcpyDeviceToHost));
+    ST_CUDA(cudaMemcpy(&cnt, p->counters + kNumClasses + 1, 4, cudaMemcpyDeviceToHost));
     *rescored = cnt >= p->n_static32 ? cnt - p->n_static32 : 0;
   }
+  return ST_OK;
+}
+
+extern "C" int st_plan_profile(st_plan* p, uint32_t cap, int32_t* classes, uint64_t* cells, float* ms,
+                               uint32_t* n_out) {
+  if (!p) return fail(ST_EINVAL, "null plan");
+  st_ctx* c = p->ctx;
+  CTX_GUARD(c);
+  if (!n_out || (cap && (!classes || !cells || !ms))) return fail(ST_EINVAL, "st_plan_profile: null output");
+  const uint32_t n = static_cast<uint32_t>(p->classes.size()) + 1;
+  *n_out = n;
+  if (cap < n) return fail(ST_EINVAL, "st_plan_profile: room for %u entries needed", n);
+  cudaEvent_t e0, e1;
+  ST_CUDA(cudaEventCreate(&e0));
+  ST_CUDA(cudaEventCreate(&e1));
+  ST_CUDA(cudaMemcpyAsync(p->counters, p->counters_init, (kNumClasses + 2) * 4, cudaMemcpyDeviceToDevice,
+                          c->stream));
+  for (uint32_t i = 0; i < n; ++i) {
+    ST_CUDA(cudaEventRecord(e0, c->stream));
+    if (i + 1 < n) {
+      const ClassPlan& cp = p->classes[i];
+      kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, c->stream>>>(cp.prm);
+      classes[i] = cp.cls;
+      cells[i] = cp.cells;
+    } else {
+      // every 16-bit class has run: the list holds the static and the rescored pairs
+      sw32_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, c->stream>>>(p->p32);
+      classes[i] = -1;
+      cells[i] = p->cells32;
+    }
+    ST_CUDA(cudaEventRecord(e1, c->stream));
+    ST_CUDA(cudaEventSynchronize(e1));
+    ST_CUDA(cudaEventElapsedTime(&ms[i], e0, e1));
+    ++c->launches;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   return ST_OK;
 }
 
@@ -892,11 +1114,16 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
   if (n && (!pairs || !scores)) return fail(ST_EINVAL, "st_sw_score_pairs: null argument");
   if (n == 0) return ST_OK;
   DevMem d_out;
-  ST_TRY(dev_alloc(&c->mt, d_out, n * 8));
+  ST_TRY(pool_get(c, n * 8, d_out));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() { pool_put(c, std::move(*m)); }
+  } back{c, &d_out};
   int32_t* d_scores = d_out.as<int32_t>();
   uint32_t* d_kern = reinterpret_cast<uint32_t*>(d_scores + n);
   st_plan* p = nullptr;
-  ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p));
+  ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p, false));
   std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
   ST_TRY(plan_run(p));
   ST_CUDA(cudaMemcpyAsync(scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1309,7 +1536,7 @@ extern "C" int st_autotune(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t 
       if (tune_cost(&c->tuning, k, max_m, 64, false) >= 1e300) continue;
       c->tuning.table[mb][nb] = k;
       st_plan* p = nullptr;
-      ST_TRY(plan_build(c, v.data(), v.size(), open, ext, out.as<int32_t>(), nullptr, &p));
+      ST_TRY(plan_build(c, v.data(), v.size(), open, ext, out.as<int32_t>(), nullptr, &p, true));
       std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
       cudaStream_t saved = c->stream;
       c->stream = c->own;
