@@ -279,7 +279,7 @@ def main():
         total_cells = float(cells)
     gcups = total_cells / (ms * 1e-3) / 1e9
     stats = plan.stats()
-    launch_profile = [{"tile": (f"G{sh[0]}xR{sh[1]}" if sh else "sw32"), "cells": c, "ms": round(t, 3),
+    launch_profile = [{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if sh else "sw32"), "cells": c, "ms": round(t, 3),
                        "gcups": round(c / (t * 1e-3) / 1e9, 1) if t > 0 else None}
                       for sh, c, t in plan.profile()] if rank == 0 else None
     scores = d_scores.cpu().numpy()
@@ -330,17 +330,24 @@ def main():
         local_q = w.pair_q.astype(np.int64)
         h2d = int(rows_pin.nbytes + pairs_pin.nbytes)
         d2h = int(w.n_pairs * 8)
-        e2e_times, e2e_ok = [], True
+        e2e_times, e2e_ok, parts = [], True, []
         for _ in range(args.e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             eids = ctx.create_profiles_arena(rows_pin, row_offs)
+            t1 = time.perf_counter()
             pairs_pin["profile"] = eids[local_q]
+            t2 = time.perf_counter()
             es, ek = ctx.sw_score_pairs(pairs_pin, gaps, with_kernels=True)
+            t3 = time.perf_counter()
             for i in eids:
                 ctx.free_profile(i)
-            e2e_times.append(time.perf_counter() - t0)
+            t4 = time.perf_counter()
+            e2e_times.append(t4 - t0)
+            parts.append([t1 - t0, t2 - t1, t3 - t2, t4 - t3])
             e2e_ok &= bool(np.array_equal(es, scores))
+        e2e_parts = {k: [round(1e3 * float(p[i]), 2) for p in parts]
+                     for i, k in enumerate(["profiles", "pair_ids", "score_pairs", "free"])}
         e2e_gcups = cells / float(np.median(e2e_times)) / 1e9
 
         cb = cpu_baseline(w, scores, args.cpu_seconds)
@@ -357,7 +364,7 @@ def main():
             "cpu_baseline": cb,
             "e2e": {"value": round(e2e_gcups, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": args.e2e_steps, "matches_device_run": bool(e2e_ok),
-                    "ms_per_step": round(1e3 * float(np.median(e2e_times)), 2),
+                    "ms_per_step": round(1e3 * float(np.median(e2e_times)), 2), "ms_parts": e2e_parts,
                     "includes": "per step: profile build from int32 rows (pinned), pair upload, plan, kernel "
                                 "launches, scores + kernel tags download, profile free; target database resident"},
             "plain": {"value": round(plain_gcups, 3), "unit": UNIT, "pairs": int(len(sample)),

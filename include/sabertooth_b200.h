@@ -151,13 +151,13 @@ int st_ungapped_hits_device(st_ctx* ctx, const st_hit* d_hits, uint64_t n, int32
 
 /* ---- tile classes and autotuning ----------------------------------------- */
 /* The packed 16-bit kernel runs in tile classes: G lanes per alignment x R
- * query rows per lane.  A per-context table maps (query-length bin, mean
+ * query rows per lane x C target columns per wavefront step.  A per-context table maps (query-length bin, mean
  * target-length bin) to a class; -1 entries use the built-in cost model.
  * Query bins: <=32, <=64, ..., <=8192, >8192 (10); target bins: <=64, <=128,
  * ..., <=4096, >4096 (8); the table is row-major [10][8].  (No reference
  * counterpart: the reference picks SIMD widths at run time, src/simd.rs:59-124.) */
 int st_tune_num_classes(void);
-int st_tune_class_shape(int cls, int* lanes_per_alignment, int* rows_per_lane);
+int st_tune_class_shape(int cls, int* lanes_per_alignment, int* rows_per_lane, int* cols_per_step);
 int st_tune_get(st_ctx* ctx, int32_t* table);
 int st_tune_set(st_ctx* ctx, const int32_t* table);
 /* Times every feasible class on samples (whole queries, up to max_pairs_per_bin

@@ -67,7 +67,7 @@ SIGNATURES = {
     "st_ungapped_hits": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
     "st_ungapped_hits_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
     "st_tune_num_classes": (C.c_int, []),
-    "st_tune_class_shape": (C.c_int, [C.c_int, _P, _P]),
+    "st_tune_class_shape": (C.c_int, [C.c_int, _P, _P, _P]),
     "st_tune_get": (C.c_int, [_P, _P]),
     "st_tune_set": (C.c_int, [_P, _P]),
     "st_autotune": (C.c_int, [_P, _P, _u64, _i32, _i32, _u32, _P]),

@@ -208,11 +208,12 @@ def _vp(x):
 
 
 def tile_classes():
+    """(lanes per alignment G, query rows per lane R, target columns per step C) of every tile class."""
     out = []
     for c in range(lib.st_tune_num_classes()):
-        g, r = C.c_int(), C.c_int()
-        check(lib.st_tune_class_shape(c, C.byref(g), C.byref(r)))
-        out.append((g.value, r.value))
+        g, r, k = C.c_int(), C.c_int(), C.c_int()
+        check(lib.st_tune_class_shape(c, C.byref(g), C.byref(r), C.byref(k)))
+        out.append((g.value, r.value, k.value))
     return out
 
 

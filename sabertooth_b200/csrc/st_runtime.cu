@@ -53,6 +53,27 @@ static int fail(int code, const char* fmt, ...) {
 
 extern "C" const char* st_last_error(void) { return g_last_error.c_str(); }
 
+// Host phase tracing (ST_TRACE=1 in the environment): one line per phase on stderr.
+#include <chrono>
+static bool trace_on() {
+  static const bool on = [] {
+    const char* v = getenv("ST_TRACE");
+    return v && v[0] && v[0] != '0';
+  }();
+  return on;
+}
+struct TraceClock {
+  const char* what;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit TraceClock(const char* w) : what(w) {}
+  void lap(const char* phase) {
+    if (!trace_on()) return;
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[st] %s %s %.3f ms\n", what, phase, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
+
 // Lets other translation units of the library report through st_last_error().
 __attribute__((visibility("hidden"))) void st_internal_set_error(const char* msg) { g_last_error = msg; }
 
@@ -144,29 +165,31 @@ static inline size_t up256(size_t x) { return (x + 255) & ~static_cast<size_t>(2
 // ---------------------------------------------------------------------------
 // kernel classes
 // ---------------------------------------------------------------------------
-constexpr int kWarps16 = 8;
+constexpr int kWarps16 = 4;
 constexpr int kWarps32 = 4;
 constexpr int kMaxSmem = 226 * 1024;  // dynamic shared memory per CTA (the 227 KB opt-in less room for static shared)
 
 using Sw16Fn = void (*)(const Sw16Params);
 
 struct Sw16Class {
-  int G, R;
+  int G, R, C;
   Sw16Fn fn;
 };
 
-#define ST_CLASS(g, r) {g, r, sw16_kernel<g, r, kWarps16>}
+#define ST_CLASS(g, r, c) {g, r, c, sw16_kernel<g, r, c, kWarps16>}
 static const Sw16Class kClasses[] = {
-    ST_CLASS(4, 8),  ST_CLASS(8, 8),  ST_CLASS(16, 8),  ST_CLASS(32, 8),  ST_CLASS(4, 16), ST_CLASS(8, 16),
-    ST_CLASS(16, 16), ST_CLASS(32, 16), ST_CLASS(4, 32), ST_CLASS(8, 32), ST_CLASS(16, 32), ST_CLASS(32, 32),
+    ST_CLASS(4, 8, 4),   ST_CLASS(8, 8, 4),   ST_CLASS(16, 8, 4),  ST_CLASS(32, 8, 4),
+    ST_CLASS(8, 16, 2),  ST_CLASS(16, 8, 2),  ST_CLASS(16, 16, 2), ST_CLASS(32, 8, 2),
+    ST_CLASS(32, 12, 2), ST_CLASS(32, 16, 2), ST_CLASS(32, 20, 2), ST_CLASS(32, 24, 2),
 };
 #undef ST_CLASS
 constexpr int kNumClasses = sizeof(kClasses) / sizeof(kClasses[0]);
 
 int st_tuning_num_classes() { return kNumClasses; }
-void st_tuning_class_shape(int c, int* G, int* R) {
+void st_tuning_class_shape(int c, int* G, int* R, int* C) {
   *G = kClasses[c].G;
   *R = kClasses[c].R;
+  *C = kClasses[c].C;
 }
 
 // ---------------------------------------------------------------------------
@@ -199,6 +222,7 @@ struct st_ctx {
   // database
   DevMem db_arena, db_off, db_len;
   std::vector<uint32_t> h_db_len;
+  std::vector<uint64_t> h_db_off;  // arena offset of each sequence (multiple of 16)
   uint32_t n_seqs = 0;
   uint64_t n_res = 0;
   bool has_db = false;
@@ -299,9 +323,17 @@ static DeviceProfiles prof_view(st_ctx* c) {
   return p;
 }
 
-static int set_smem_limits() {
-  for (int i = 0; i < kNumClasses; ++i)
-    ST_CUDA(cudaFuncSetAttribute(kClasses[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+static int g_class_smem[kNumClasses];  // dynamic shared memory each 16-bit class may use
+
+static int set_smem_limits(int device) {
+  int optin = 0;
+  ST_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  for (int i = 0; i < kNumClasses; ++i) {
+    cudaFuncAttributes fa;
+    ST_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kClasses[i].fn)));
+    g_class_smem[i] = std::min<int>(kMaxSmem, optin - static_cast<int>(fa.sharedSizeBytes));
+    ST_CUDA(cudaFuncSetAttribute(kClasses[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, g_class_smem[i]));
+  }
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
   return ST_OK;
@@ -338,7 +370,7 @@ extern "C" st_ctx* st_init(int device, size_t hbm_budget_bytes) {
     return nullptr;
   }
   c->stream = c->own;
-  if (set_smem_limits() != ST_OK) return nullptr;
+  if (set_smem_limits(device) != ST_OK) return nullptr;
   tuning_defaults(&c->tuning);
   return c.release();
 }
@@ -425,6 +457,7 @@ extern "C" int st_db_upload(st_ctx* c, const uint8_t* residues, const uint64_t* 
   if (n_seqs) ST_CUDA(cudaMemcpyAsync(c->db_len.p, len.data(), len.size() * 4, cudaMemcpyHostToDevice, c->own));
   ST_CUDA(cudaStreamSynchronize(c->own));
   c->h_db_len = std::move(len);
+  c->h_db_off.assign(off.begin(), off.end() - 1);
   c->n_seqs = n_seqs;
   c->n_res = offsets[n_seqs] - offsets[0];
   c->has_db = true;
@@ -471,6 +504,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   if (!row_offsets || !ids || (!rows && n_profiles && row_offsets[n_profiles] > row_offsets[0]))
     return fail(ST_EINVAL, "st_profiles_create: null input");
   if (n_profiles == 0) return ST_OK;
+  TraceClock tc("profiles");
   std::vector<ProfBuildDesc> desc(n_profiles);
   std::vector<int32_t> mx(n_profiles);
   for (uint32_t k = 0; k < n_profiles; ++k) {
@@ -506,6 +540,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
     desc[k].o8 = bytes32 + bytes8;
     bytes8 += up16(static_cast<size_t>(kProfRows) * desc[k].stride8);
   }
+  tc.lap("range");
   const size_t rows_total = row_offsets[n_profiles] - row_offsets[0];
   const size_t src_bytes = rows_total * kAlpha * 4;
   const size_t desc_bytes = up16(n_profiles * sizeof(ProfBuildDesc));
@@ -513,6 +548,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   ST_TRY(dev_alloc(&c->mt, blk->mem, bytes32 + bytes8));
   DevMem tmp;  // uploaded rows and descriptors, freed once the layouts are built
   ST_TRY(dev_alloc(&c->mt, tmp, src_bytes + desc_bytes + 16));
+  tc.lap("alloc");
   char* base = blk->mem.as<char>();
   int32_t* d_src = tmp.as<int32_t>();
   ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + up16(src_bytes));
@@ -523,6 +559,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   ++c->launches;
   ST_CUDA(cudaGetLastError());
   ST_CUDA(cudaStreamSynchronize(c->own));
+  tc.lap("upload+build");
   const int bi = static_cast<int>(c->blocks.size());
   for (uint32_t k = 0; k < n_profiles; ++k) {
     const ProfBuildDesc& x = desc[k];
@@ -632,7 +669,7 @@ struct ClassPlan {
   int cls = -1;
   std::vector<Sw16CtaTask> cta;
   std::vector<Sw16WarpTask> wt;
-  std::vector<uint32_t> slots;
+  std::vector<Sw16Slot> slots;
   size_t o_cta = 0, o_wt = 0, o_slots = 0, o_scratch = 0;  // offsets in the plan's device arena
   uint32_t grid = 0;
   uint32_t smem = 0;
@@ -669,43 +706,6 @@ static int occupancy_grid(st_ctx* c, const void* fn, int threads, size_t smem, u
   return ST_OK;
 }
 
-// Shape of the work for one query in one class: warp tasks of S = 64/G targets
-// (two per lane group), targets in descending length.
-static void emit_query(ClassPlan& cp, const Sw16Class& k, uint32_t q, uint32_t m, const std::vector<uint32_t>& pairs,
-                       const std::vector<uint32_t>& tlen, uint32_t max_wt_per_cta) {
-  const uint32_t S = 64 / k.G;
-  const uint32_t rows = static_cast<uint32_t>(k.G * k.R);
-  const uint32_t P = std::max<uint32_t>(1, (m + rows - 1) / rows);
-  const uint32_t m_pad = P * rows;
-  uint32_t first_wt = static_cast<uint32_t>(cp.wt.size());
-  for (size_t i = 0; i < pairs.size(); i += S) {
-    Sw16WarpTask w;
-    w.slot_begin = static_cast<uint32_t>(cp.slots.size());
-    uint32_t ncols = 32;
-    for (uint32_t s = 0; s < S; ++s) {
-      const size_t j = i + s;
-      if (j < pairs.size()) {
-        cp.slots.push_back(pairs[j]);
-        ncols = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(tlen[j])));
-      } else {
-        cp.slots.push_back(kNoPair);
-      }
-    }
-    w.ncols = ncols;
-    cp.wt.push_back(w);
-    const uint32_t done = static_cast<uint32_t>(cp.wt.size()) - first_wt;
-    if (done == max_wt_per_cta || i + S >= pairs.size()) {
-      Sw16CtaTask t;
-      t.query = q;
-      t.wt_begin = first_wt;
-      t.wt_end = static_cast<uint32_t>(cp.wt.size());
-      t.m_pad = m_pad;
-      cp.cta.push_back(t);
-      first_wt = static_cast<uint32_t>(cp.wt.size());
-    }
-  }
-}
-
 // The launches of one run, in stream order: clear outputs, reset counters,
 // every 16-bit class, then the 32-bit kernel over the static list plus the
 // pairs the 16-bit classes flagged.
@@ -735,6 +735,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   plan->d_scores = d_scores;
   plan->d_kernels = d_kernels;
   const bool g16 = gaps16_ok(open, ext);
+  TraceClock tc("plan");
 
   std::vector<uint32_t> pq(n), pt(n), tlen(n);
   std::vector<int32_t> pc(n), pr(n);
@@ -790,6 +791,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   }
   plan->cells = cells;
   plan->cells32 = cells32;
+  tc.lap("classify");
   // 32-bit list in pair order; 16-bit pairs grouped by query (counting sort)
   std::vector<uint32_t> list32;
   std::vector<uint64_t> qstart(static_cast<size_t>(n_prof) + 1, 0);
@@ -820,10 +822,11 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     uint64_t sum_n = 0;
     for (uint32_t* it = v0; it != v1; ++it) sum_n += tlen[*it];
     const uint32_t m = c->profs[q].m;
-    const int cls = tuning_pick(&c->tuning, m, static_cast<uint32_t>(sum_n / (v1 - v0)));
+    const uint32_t mean_n = static_cast<uint32_t>(sum_n / (v1 - v0));
+    const int cls = tuning_refine(&c->tuning, tuning_pick(&c->tuning, m, mean_n), m, mean_n);
     const uint32_t rows = kClasses[cls].G * kClasses[cls].R;
     const uint32_t P = (m + rows - 1) / rows;
-    if (static_cast<uint64_t>(kProfRows) * P * rows > kMaxSmem) {
+    if (static_cast<uint64_t>(kProfRows) * P * rows > static_cast<uint64_t>(g_class_smem[cls])) {
 #pragma omp critical
       toolong = static_cast<int>(m);
     }
@@ -831,38 +834,96 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     qsum[k] = sum_n;
   }
   if (toolong >= 0) return fail(ST_EINVAL, "query of %d rows does not fit the shared-memory profile", toolong);
+  tc.lap("group+sort");
   std::vector<ClassPlan> cps(kNumClasses);
   for (int k = 0; k < kNumClasses; ++k) cps[k].cls = k;
-  std::vector<uint32_t> tl;
+  // emission, two passes: sizes and offsets per query (in query order within each class), then a parallel fill
+  struct QEmit {
+    uint32_t n_wt, n_cta;
+    size_t wt_off, slot_off, cta_off;
+  };
+  std::vector<QEmit> qe(qlist.size());
+  std::vector<size_t> n_wt_cls(kNumClasses, 0), n_slot_cls(kNumClasses, 0), n_cta_cls(kNumClasses, 0);
+  constexpr uint32_t kMaxWtPerCta = 64;
   for (size_t k = 0; k < qlist.size(); ++k) {
     const uint32_t q = qlist[k];
     const int cls = qclass[k];
-    const uint64_t a0 = qstart[q], a1 = qstart[q + 1];
-    std::vector<uint32_t> v(byq.begin() + a0, byq.begin() + a1);
-    tl.resize(v.size());
-    for (size_t j = 0; j < v.size(); ++j) tl[j] = tlen[v[j]];
-    emit_query(cps[cls], kClasses[cls], q, c->profs[q].m, v, tl, 64);
+    const uint32_t S = 64 / kClasses[cls].G;
+    const uint64_t np = qstart[q + 1] - qstart[q];
+    QEmit& e = qe[k];
+    e.n_wt = static_cast<uint32_t>((np + S - 1) / S);
+    e.n_cta = (e.n_wt + kMaxWtPerCta - 1) / kMaxWtPerCta;
+    e.wt_off = n_wt_cls[cls];
+    e.slot_off = n_slot_cls[cls];
+    e.cta_off = n_cta_cls[cls];
+    n_wt_cls[cls] += e.n_wt;
+    n_slot_cls[cls] += static_cast<size_t>(e.n_wt) * S;
+    n_cta_cls[cls] += e.n_cta;
     cps[cls].cells += static_cast<uint64_t>(c->profs[q].m) * qsum[k];
   }
-
+  std::vector<std::vector<uint64_t>> cta_cost(kNumClasses);
+  for (int k = 0; k < kNumClasses; ++k) {
+    cps[k].wt.resize(n_wt_cls[k]);
+    cps[k].slots.resize(n_slot_cls[k]);
+    cps[k].cta.resize(n_cta_cls[k]);
+    cta_cost[k].resize(n_cta_cls[k]);
+  }
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < static_cast<int64_t>(qlist.size()); ++k) {
+    const uint32_t q = qlist[k];
+    const int cls = qclass[k];
+    const Sw16Class& kc = kClasses[cls];
+    ClassPlan& cp = cps[cls];
+    const QEmit& e = qe[k];
+    const uint32_t S = 64 / kc.G;
+    const uint32_t m = c->profs[q].m;
+    const uint32_t rows = static_cast<uint32_t>(kc.G * kc.R);
+    const uint32_t P = std::max<uint32_t>(1, (m + rows - 1) / rows);
+    const uint32_t min_cols = P > 1 ? static_cast<uint32_t>(up16(std::max(32, kc.C * kc.G))) : 32u;
+    const uint32_t* v = byq.data() + qstart[q];
+    const size_t np = qstart[q + 1] - qstart[q];
+    for (uint32_t w = 0; w < e.n_wt; ++w) {
+      const size_t sb = e.slot_off + static_cast<size_t>(w) * S;
+      uint32_t ncols = min_cols;
+      for (uint32_t sidx = 0; sidx < S; ++sidx) {
+        const size_t j = static_cast<size_t>(w) * S + sidx;
+        Sw16Slot sl{kNoPair, 0, 0, 0};
+        if (j < np) {
+          const uint32_t pi = v[j];
+          sl.pair = pi;
+          sl.toff16 = static_cast<uint32_t>(c->h_db_off[pt[pi]] / 16);
+          sl.tlen16 = static_cast<uint32_t>(up16(tlen[pi]));
+          sl.tlen = tlen[pi];
+          ncols = std::max<uint32_t>(ncols, sl.tlen16);
+        }
+        cp.slots[sb + sidx] = sl;
+      }
+      cp.wt[e.wt_off + w] = Sw16WarpTask{static_cast<uint32_t>(sb), ncols};
+    }
+    for (uint32_t t = 0; t < e.n_cta; ++t) {
+      const uint32_t w0 = t * kMaxWtPerCta, w1 = std::min(e.n_wt, w0 + kMaxWtPerCta);
+      cp.cta[e.cta_off + t] = Sw16CtaTask{q, static_cast<uint32_t>(e.wt_off + w0), static_cast<uint32_t>(e.wt_off + w1),
+                                          P * rows};
+      uint64_t cst = 0;
+      for (uint32_t w = w0; w < w1; ++w)
+        cst += static_cast<uint64_t>(P * cp.wt[e.wt_off + w].ncols / kc.C) * (kc.R * kc.C + 8);
+      cta_cost[cls][e.cta_off + t] = cst;
+    }
+  }
+  tc.lap("emit");
   // order CTA tasks by estimated cost, longest first
   for (auto& cp : cps) {
     if (cp.cta.empty()) continue;
-    const Sw16Class& k = kClasses[cp.cls];
-    std::vector<std::pair<uint64_t, uint32_t>> cost(cp.cta.size());
-    for (size_t i = 0; i < cp.cta.size(); ++i) {
-      uint64_t cst = 0;
-      const uint32_t P = cp.cta[i].m_pad / (k.G * k.R);
-      for (uint32_t w = cp.cta[i].wt_begin; w < cp.cta[i].wt_end; ++w)
-        cst += static_cast<uint64_t>(P * cp.wt[w].ncols + k.G) * (k.R + 6);
-      cost[i] = {cst, static_cast<uint32_t>(i)};
-    }
-    std::stable_sort(cost.begin(), cost.end(), [](auto& a, auto& b) { return a.first > b.first; });
+    const auto& cost0 = cta_cost[cp.cls];
+    std::vector<uint32_t> idx(cp.cta.size());
+    std::iota(idx.begin(), idx.end(), 0u);
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return cost0[a] > cost0[b]; });
     std::vector<Sw16CtaTask> sorted(cp.cta.size());
-    for (size_t i = 0; i < cost.size(); ++i) sorted[i] = cp.cta[cost[i].second];
+    for (size_t i = 0; i < idx.size(); ++i) sorted[i] = cp.cta[idx[i]];
     cp.cta.swap(sorted);
   }
 
+  tc.lap("lpt");
   // launch shapes and scratch needs
   uint32_t nonempty = 0;
   for (auto& cp : cps) {
@@ -902,8 +963,12 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     if (cp.cta.empty()) continue;
     cp.o_cta = carve(cp.cta.size() * sizeof(Sw16CtaTask));
     cp.o_wt = carve(cp.wt.size() * sizeof(Sw16WarpTask));
-    cp.o_slots = carve(cp.slots.size() * 4);
+    cp.o_slots = carve(cp.slots.size() * sizeof(Sw16Slot));
   }
+  uint32_t zcols = 64;
+  for (auto& cp : cps)
+    for (auto& w : cp.wt) zcols = std::max(zcols, w.ncols + 8);
+  const size_t o_zline = carve(static_cast<size_t>(zcols) * sizeof(uint2));
   const size_t data_bytes = off;
   const size_t o_cnt = carve((kNumClasses + 2) * 4);
   for (auto& cp : cps) {
@@ -915,7 +980,9 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
                                  ? static_cast<size_t>(plan->grid32) * kWarps32 * plan->scratch32_stride * sizeof(int2)
                                  : 16);
   const size_t total_bytes = off;
+  tc.lap("shapes");
   ST_TRY(pool_get(c, total_bytes, plan->arena));
+  tc.lap("arena");
   char* dbase = plan->arena.as<char>();
   // stage the data region in pinned memory and upload it at once
   ST_TRY(c->pin.reserve(data_bytes));
@@ -934,6 +1001,12 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   }
   if (!list32.empty()) memcpy(h + o_list, list32.data(), list32.size() * 4);
   {
+    // input of a first pass: H = 0 above the query, F = first-row F
+    uint2* z = reinterpret_cast<uint2*>(h + o_zline);
+    const uint2 v = make_uint2(0u, pk_splat(-open));
+    for (uint32_t i = 0; i < zcols; ++i) z[i] = v;
+  }
+  {
     // counters: [0, kNumClasses) class work, [kNumClasses] 32-bit work, [kNumClasses+1] list count
     uint32_t* ci = reinterpret_cast<uint32_t*>(h + o_cinit);
     for (int k = 0; k < kNumClasses + 2; ++k) ci[k] = 0;
@@ -943,9 +1016,10 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     if (cp.cta.empty()) continue;
     memcpy(h + cp.o_cta, cp.cta.data(), cp.cta.size() * sizeof(Sw16CtaTask));
     memcpy(h + cp.o_wt, cp.wt.data(), cp.wt.size() * sizeof(Sw16WarpTask));
-    memcpy(h + cp.o_slots, cp.slots.data(), cp.slots.size() * 4);
+    memcpy(h + cp.o_slots, cp.slots.data(), cp.slots.size() * sizeof(Sw16Slot));
   }
   ST_CUDA(cudaMemcpyAsync(dbase, h, data_bytes, cudaMemcpyHostToDevice, c->stream));
+  tc.lap("stage+upload");
   plan->counters = reinterpret_cast<uint32_t*>(dbase + o_cnt);
   plan->counters_init = reinterpret_cast<const uint32_t*>(dbase + o_cinit);
   for (auto& cp : cps)
@@ -963,19 +1037,19 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   // kernel parameters (kept on the plan: the graph and the per-class profiler launch the same)
   for (auto& cp : plan->classes) {
     Sw16Params& prm = cp.prm;
-    prm.db = db;
+    prm.arena = db.arena;
     prm.prof = pv;
     prm.cta_tasks = reinterpret_cast<const Sw16CtaTask*>(dbase + cp.o_cta);
     prm.n_cta_tasks = static_cast<uint32_t>(cp.cta.size());
     prm.warp_tasks = reinterpret_cast<const Sw16WarpTask*>(dbase + cp.o_wt);
-    prm.slot_pair = reinterpret_cast<const uint32_t*>(dbase + cp.o_slots);
-    prm.pair_target = d_pair_t;
+    prm.slots = reinterpret_cast<const Sw16Slot*>(dbase + cp.o_slots);
     prm.scores = d_scores;
     prm.kernels = d_kernels;
     prm.ovf_count = counters + kNumClasses + 1;
     prm.ovf_pairs = d_list;
     prm.work_counter = counters + cp.cls;
     prm.scratch = reinterpret_cast<uint2*>(dbase + cp.o_scratch);
+    prm.zline = reinterpret_cast<const uint2*>(dbase + o_zline);
     prm.scratch_stride = cp.scratch_stride;
     prm.open = open;
     prm.ext = ext;
@@ -1123,12 +1197,15 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
   int32_t* d_scores = d_out.as<int32_t>();
   uint32_t* d_kern = reinterpret_cast<uint32_t*>(d_scores + n);
   st_plan* p = nullptr;
+  TraceClock tc("pairs");
   ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p, false));
   std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
+  tc.lap("plan");
   ST_TRY(plan_run(p));
   ST_CUDA(cudaMemcpyAsync(scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
   if (kernels) ST_CUDA(cudaMemcpyAsync(kernels, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
   ST_CUDA(cudaStreamSynchronize(c->stream));
+  tc.lap("run+download");
   return ST_OK;
 }
 
@@ -1161,10 +1238,14 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
   o = up16(o);
   const size_t o_cta = o; o += sizeof(Sw16CtaTask);
   const size_t o_wt = o; o += sizeof(Sw16WarpTask);
-  const size_t o_slots = o; o += 64 * 4;
+  o = up16(o);  // slot records are read as 16-byte vectors
+  const size_t o_slots = o; o += 64 * sizeof(Sw16Slot);
   const size_t o_cnt = o; o += (kNumClasses + 2) * 4;
   const size_t o_list = o; o += 4;
   const size_t o_res = o; o += 8;
+  o = up16(o);
+  const size_t o_zline = o; o += (static_cast<size_t>(std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)))) + 
+                                  static_cast<size_t>(32 * 4 + 16)) * sizeof(uint2);
   const size_t total = up16(o);
   const bool use16 = pm.fits8 && gaps16_ok(open, ext);
   int k = 0;
@@ -1173,10 +1254,14 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
     k = tuning_pick_single(&c->tuning, pm.m, n);
     rows = kClasses[k].G * kClasses[k].R;
     P = (pm.m + rows - 1) / rows;
-    if (static_cast<size_t>(kProfRows) * P * rows > kMaxSmem) return fail(ST_EINVAL, "query too long");
+    if (static_cast<size_t>(kProfRows) * P * rows > static_cast<size_t>(g_class_smem[k]))
+      return fail(ST_EINVAL, "query of %u rows too long for the shared-memory profile", pm.m);
   }
+  uint32_t ncols = std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)));
+  if (use16 && P > 1) ncols = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(kClasses[k].C * kClasses[k].G)));
+  const uint32_t sstride = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(n) + 32));
   // any warp of the CTA may take the task: room for every group of the CTA
-  const size_t scratch_need = static_cast<size_t>(kWarps16) * 8 * (up16(n) + 32) * sizeof(uint2);
+  const size_t scratch_need = static_cast<size_t>(kWarps16) * 8 * sstride * sizeof(uint2);
   ST_TRY(c->pin.reserve(total));
   if (c->stage.bytes < total) ST_TRY(dev_alloc(&c->mt, c->stage, total * 2));
   if (c->scratch_small.bytes < scratch_need) ST_TRY(dev_alloc(&c->mt, c->scratch_small, scratch_need * 2));
@@ -1192,15 +1277,20 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
   *reinterpret_cast<int32_t*>(h + o_pc) = 0;
   *reinterpret_cast<int32_t*>(h + o_pr) = -1;  // no band
   Sw16CtaTask ct{profile, 0, 1, P * std::max<uint32_t>(rows, 1)};
-  Sw16WarpTask wt{0, std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)))};
+  Sw16WarpTask wt{0, ncols};
   memcpy(h + o_cta, &ct, sizeof(ct));
   memcpy(h + o_wt, &wt, sizeof(wt));
-  uint32_t* slots = reinterpret_cast<uint32_t*>(h + o_slots);
-  for (int s = 0; s < 64; ++s) slots[s] = kNoPair;
-  slots[0] = 0;
+  Sw16Slot* slots = reinterpret_cast<Sw16Slot*>(h + o_slots);
+  for (int s = 0; s < 64; ++s) slots[s] = Sw16Slot{kNoPair, 0, 0, 0};
+  slots[0] = Sw16Slot{0, 0, static_cast<uint32_t>(up16(n)), n};  // the staged target sits at offset 0
   uint32_t* cnt = reinterpret_cast<uint32_t*>(h + o_cnt);
   if (!use16) cnt[kNumClasses + 1] = 1;  // the pair goes straight to the 32-bit list
   *reinterpret_cast<uint32_t*>(h + o_list) = 0;
+  {
+    uint2* z = reinterpret_cast<uint2*>(h + o_zline);
+    const size_t nz = (total - o_zline) / sizeof(uint2);
+    for (size_t i = 0; i < nz; ++i) z[i] = make_uint2(0u, pk_splat(-open));
+  }
   char* d = c->stage.as<char>();
   ST_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, c->stream));
   DeviceDb db;
@@ -1215,20 +1305,20 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
   uint32_t* d_list = reinterpret_cast<uint32_t*>(d + o_list);
   if (use16) {
     Sw16Params prm;
-    prm.db = db;
+    prm.arena = reinterpret_cast<const uint8_t*>(d);
     prm.prof = pv;
     prm.cta_tasks = reinterpret_cast<const Sw16CtaTask*>(d + o_cta);
     prm.n_cta_tasks = 1;
     prm.warp_tasks = reinterpret_cast<const Sw16WarpTask*>(d + o_wt);
-    prm.slot_pair = reinterpret_cast<const uint32_t*>(d + o_slots);
-    prm.pair_target = reinterpret_cast<const uint32_t*>(d + o_pt);
+    prm.slots = reinterpret_cast<const Sw16Slot*>(d + o_slots);
     prm.scores = d_score;
     prm.kernels = d_kern;
     prm.ovf_count = d_cnt + kNumClasses + 1;
     prm.ovf_pairs = d_list;
     prm.work_counter = d_cnt + k;
     prm.scratch = c->scratch_small.as<uint2>();
-    prm.scratch_stride = static_cast<uint32_t>(up16(n) + 32);
+    prm.zline = reinterpret_cast<const uint2*>(d + o_zline);
+    prm.scratch_stride = sstride;
     prm.open = open;
     prm.ext = ext;
     kClasses[k].fn<<<1, kWarps16 * 32, kProfRows * P * rows, c->stream>>>(prm);
@@ -1465,10 +1555,11 @@ extern "C" int st_probe_dpx(st_ctx* c, double* ops_per_s) {
 // ---------------------------------------------------------------------------
 extern "C" int st_tune_num_classes(void) { return kNumClasses; }
 
-extern "C" int st_tune_class_shape(int cls, int* lanes, int* rows) {
+extern "C" int st_tune_class_shape(int cls, int* lanes, int* rows, int* cols) {
   if (cls < 0 || cls >= kNumClasses || !lanes || !rows) return fail(ST_EINVAL, "bad tile class %d", cls);
   *lanes = kClasses[cls].G;
   *rows = kClasses[cls].R;
+  if (cols) *cols = kClasses[cls].C;
   return ST_OK;
 }
 

@@ -50,6 +50,6 @@ def test_errors_are_reported_not_raised_in_c():
 def test_tile_classes_are_listed():
     from sabertooth_b200 import tile_classes
     cls = tile_classes()
-    assert (32, 32) in cls and (4, 8) in cls
-    for g, r in cls:
-        assert g in (4, 8, 16, 32) and r in (8, 16, 32)
+    assert (32, 16, 2) in cls and (4, 8, 4) in cls
+    for g, r, c in cls:
+        assert g in (4, 8, 16, 32) and r % 4 == 0 and 8 <= r <= 32 and c in (1, 2, 4)
