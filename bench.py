@@ -340,8 +340,7 @@ def main():
             t2 = time.perf_counter()
             es, ek = ctx.sw_score_pairs(pairs_pin, gaps, with_kernels=True)
             t3 = time.perf_counter()
-            for i in eids:
-                ctx.free_profile(i)
+            ctx.free_profiles(eids)
             t4 = time.perf_counter()
             e2e_times.append(t4 - t0)
             parts.append([t1 - t0, t2 - t1, t3 - t2, t4 - t3])

@@ -69,6 +69,10 @@ int st_db_info(st_ctx* ctx, uint32_t* n_seqs, uint64_t* n_residues);
  * rows = int32 [m][21].  m = 0 is allowed (every score is then 0). */
 int st_profile_create(st_ctx* ctx, const int32_t* rows, uint32_t m, uint32_t* id);
 int st_profile_free(st_ctx* ctx, uint32_t id);
+/* Batch form of st_profile_free (no reference counterpart: the reference drops
+ * each QueryProfile on its own). Stops at the first unknown id, with the ids
+ * before it freed. A freed id may be handed out again by a later create. */
+int st_profiles_free(st_ctx* ctx, const uint32_t* ids, uint32_t n);
 /* Batch form: n_profiles profiles from one rows arena; row_offsets[k]..row_offsets[k+1]
  * are the rows of profile k; ids written to ids[0..n_profiles). */
 int st_profiles_create(st_ctx* ctx, const int32_t* rows, const uint64_t* row_offsets, uint32_t n_profiles,

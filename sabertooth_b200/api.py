@@ -141,6 +141,11 @@ class Context:
     def free_profile(self, pid):
         check(lib.st_profile_free(self._h, int(pid)))
 
+    def free_profiles(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        if len(ids):
+            check(lib.st_profiles_free(self._h, ptr(ids), len(ids)))
+
     # -- (G) batched -------------------------------------------------------
     def sw_score_pairs(self, pairs, gaps: GapCosts, with_kernels=False):
         """Scores of many (profile, db target[, band]) pairs; host buffers in and out."""

@@ -165,7 +165,7 @@ static inline size_t up256(size_t x) { return (x + 255) & ~static_cast<size_t>(2
 // ---------------------------------------------------------------------------
 // kernel classes
 // ---------------------------------------------------------------------------
-constexpr int kWarps16 = 4;
+constexpr int kWarps16 = 8;
 constexpr int kWarps32 = 4;
 constexpr int kMaxSmem = 226 * 1024;  // dynamic shared memory per CTA (the 227 KB opt-in less room for static shared)
 
@@ -232,12 +232,41 @@ struct st_ctx {
   DevMem d_p8, d_p32, d_stride8, d_stride32, d_qlen, d_maxs, d_fits8;
   bool prof_dirty = true;
   uint32_t max_m = 0;
+  std::vector<uint32_t> free_ids;  // ids of freed profiles, handed out again
+  std::vector<int> free_blocks;    // blocks whose profiles are all freed
   // staging for the per-call paths
   Pinned pin;
   DevMem stage;
   DevMem scratch_small;
   Tuning tuning;
   std::vector<DevMem> pool;  // device arenas of finished plans, reused by later plans
+  // pipelined batches: pinned staging ring (one block per plan in flight) and two side streams
+  static constexpr int kStageRing = 6;
+  Pinned plan_pin[kStageRing];
+  cudaEvent_t plan_pin_ev[kStageRing] = {};
+  bool plan_pin_used[kStageRing] = {};
+  static constexpr int kMaxSide = 4;
+  cudaStream_t side[kMaxSide] = {};
+  Pinned out_pin;  // scores and kernel tags on their way to pageable caller buffers
+  cudaEvent_t side_ev[1 + kMaxSide] = {};  // [0] start of a batch, [1 + i] end of side stream i's work
+  // fork streams of a plan's launches: the 16-bit classes run side by side, the 32-bit kernel after them.
+  // Set 0 serves the context's own / caller's stream, set 1 + i side stream i.
+  struct ForkSet {
+    static constexpr int kForks = 3;
+    cudaStream_t s[kForks] = {};
+    cudaEvent_t ev[kForks + 1] = {};
+  };
+  ForkSet forks[1 + kMaxSide];
+  // host buffers of the planner, kept between plans so their pages stay mapped
+  struct PlanScratch {
+    std::vector<uint32_t> pq, pt, tlen, byq, list32;
+    std::vector<int32_t> pc, pr;
+    std::vector<uint8_t> route;
+    std::vector<uint64_t> qstart;
+    std::vector<Sw16Slot> slots[32];
+    std::vector<Sw16WarpTask> wt[32];
+    std::vector<Sw16CtaTask> cta[32];
+  } ps;
 };
 
 // A device buffer of at least `bytes` from the context's pool (or a new allocation).
@@ -258,7 +287,7 @@ static int pool_get(st_ctx* c, size_t bytes, DevMem& out) {
 static void pool_put(st_ctx* c, DevMem&& m) {
   if (!m.p) return;
   c->pool.push_back(std::move(m));
-  while (c->pool.size() > 4) {  // keep the four most recent arenas
+  while (c->pool.size() > 96) {  // keep the most recent arenas (one per chunk of a pipelined batch)
     c->pool.erase(c->pool.begin());
   }
 }
@@ -380,6 +409,23 @@ extern "C" void st_shutdown(st_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaStreamSynchronize(c->own);
+  for (auto s : c->side)
+    if (s) cudaStreamSynchronize(s);
+  for (auto s : c->side)
+    if (s) cudaStreamDestroy(s);
+  for (auto e : c->side_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto e : c->plan_pin_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& f : c->forks) {
+    for (auto s : f.s)
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    for (auto e : f.ev)
+      if (e) cudaEventDestroy(e);
+  }
   cudaStream_t own = c->own;
   delete c;
   cudaStreamDestroy(own);
@@ -513,23 +559,11 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
       return fail(ST_EINVAL, "st_profiles_create: query of %llu rows exceeds 2^20",
                   static_cast<unsigned long long>(row_offsets[k + 1] - row_offsets[k]));
   }
-  // score range per profile (residues >= 21 score 0), in parallel over profiles
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) {
-    const uint64_t m = row_offsets[k + 1] - row_offsets[k];
-    int32_t lo = 0, hi = 0;
-    const int32_t* r = rows + row_offsets[k] * kAlpha;
-    for (size_t i = 0; i < m * kAlpha; ++i) {
-      lo = std::min(lo, r[i]);
-      hi = std::max(hi, r[i]);
-    }
-    mx[k] = hi;
-    desc[k].m = static_cast<uint32_t>(m);
-    desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
-  }
+  // layouts depend on the lengths only
   size_t bytes8 = 0, bytes32 = 0;
   for (uint32_t k = 0; k < n_profiles; ++k) {
     ProfBuildDesc& x = desc[k];
+    x.m = static_cast<uint32_t>(row_offsets[k + 1] - row_offsets[k]);
     x.src_row = row_offsets[k] - row_offsets[0];
     x.stride8 = static_cast<uint32_t>(std::max<size_t>(up16(x.m), 16));
     x.stride32 = static_cast<uint32_t>(std::max<size_t>(up256(x.m), kSw32Rows));
@@ -540,27 +574,60 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
     desc[k].o8 = bytes32 + bytes8;
     bytes8 += up16(static_cast<size_t>(kProfRows) * desc[k].stride8);
   }
-  tc.lap("range");
   const size_t rows_total = row_offsets[n_profiles] - row_offsets[0];
   const size_t src_bytes = rows_total * kAlpha * 4;
   const size_t desc_bytes = up16(n_profiles * sizeof(ProfBuildDesc));
-  auto blk = std::make_unique<ProfileBlock>();
-  ST_TRY(dev_alloc(&c->mt, blk->mem, bytes32 + bytes8));
-  DevMem tmp;  // uploaded rows and descriptors, freed once the layouts are built
-  ST_TRY(dev_alloc(&c->mt, tmp, src_bytes + desc_bytes + 16));
+  DevMem blk_mem, tmp;  // tmp: uploaded rows and descriptors, back to the pool once the layouts are built
+  ST_TRY(pool_get(c, bytes32 + bytes8, blk_mem));
+  ST_TRY(pool_get(c, src_bytes + desc_bytes + 16, tmp));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() {
+      cudaStreamSynchronize(c->own);
+      pool_put(c, std::move(*m));
+    }
+  } back_tmp{c, &tmp};
   tc.lap("alloc");
-  char* base = blk->mem.as<char>();
+  char* base = blk_mem.as<char>();
   int32_t* d_src = tmp.as<int32_t>();
   ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + up16(src_bytes));
+  // the rows travel while the host computes their score ranges
   if (src_bytes)
     ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->own));
+  // score range per profile (residues >= 21 score 0), in parallel over profiles
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) {
+    const uint64_t m = desc[k].m;
+    int32_t lo = 0, hi = 0;
+    const int32_t* r = rows + row_offsets[k] * kAlpha;
+    for (size_t i = 0; i < m * kAlpha; ++i) {
+      lo = std::min(lo, r[i]);
+      hi = std::max(hi, r[i]);
+    }
+    mx[k] = hi;
+    desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
+  }
+  tc.lap("range");
   ST_CUDA(cudaMemcpyAsync(d_desc, desc.data(), n_profiles * sizeof(ProfBuildDesc), cudaMemcpyHostToDevice, c->own));
   build_profiles_kernel<<<n_profiles, 256, 0, c->own>>>(d_src, d_desc, base);
   ++c->launches;
   ST_CUDA(cudaGetLastError());
   ST_CUDA(cudaStreamSynchronize(c->own));
   tc.lap("upload+build");
-  const int bi = static_cast<int>(c->blocks.size());
+  int bi;
+  if (!c->free_blocks.empty()) {
+    bi = c->free_blocks.back();
+    c->free_blocks.pop_back();
+  } else {
+    bi = static_cast<int>(c->blocks.size());
+    c->blocks.push_back(std::make_unique<ProfileBlock>());
+  }
+  ProfileBlock* blk = c->blocks[bi].get();
+  blk->mem = std::move(blk_mem);
+  blk->live = n_profiles;
+  // freed ids first (in increasing order), then new ones
+  if (c->free_ids.size() > 1) std::sort(c->free_ids.begin(), c->free_ids.end(), std::greater<uint32_t>());
   for (uint32_t k = 0; k < n_profiles; ++k) {
     const ProfBuildDesc& x = desc[k];
     ProfileMeta pm;
@@ -573,11 +640,15 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
     pm.p8 = reinterpret_cast<const int8_t*>(base + x.o8);
     pm.stride8 = x.stride8;
     pm.stride32 = x.stride32;
-    ids[k] = static_cast<uint32_t>(c->profs.size());
-    c->profs.push_back(pm);
+    if (!c->free_ids.empty()) {
+      ids[k] = c->free_ids.back();
+      c->free_ids.pop_back();
+      c->profs[ids[k]] = pm;
+    } else {
+      ids[k] = static_cast<uint32_t>(c->profs.size());
+      c->profs.push_back(pm);
+    }
   }
-  blk->live = n_profiles;
-  c->blocks.push_back(std::move(blk));
   c->prof_dirty = true;
   return ST_OK;
 }
@@ -587,17 +658,34 @@ extern "C" int st_profile_create(st_ctx* c, const int32_t* rows, uint32_t m, uin
   return st_profiles_create(c, rows, off, 1, id);
 }
 
-extern "C" int st_profile_free(st_ctx* c, uint32_t id) {
-  CTX_GUARD(c);
+// Releases one profile; its id is handed out again by a later create. The
+// block's device memory goes back to the context's pool when its last
+// profile is freed (after work already queued on the stream has finished).
+static int profile_free(st_ctx* c, uint32_t id) {
   if (id >= c->profs.size() || !c->profs[id].live) return fail(ST_EINVAL, "unknown profile id %u", id);
   ProfileMeta& p = c->profs[id];
   p.live = false;
   ProfileBlock* b = c->blocks[p.block].get();
   if (--b->live == 0) {
     ST_CUDA(cudaStreamSynchronize(c->stream));
-    b->mem.release();
+    pool_put(c, std::move(b->mem));
+    c->free_blocks.push_back(p.block);
   }
+  p.block = -1;
+  c->free_ids.push_back(id);
   c->prof_dirty = true;
+  return ST_OK;
+}
+
+extern "C" int st_profile_free(st_ctx* c, uint32_t id) {
+  CTX_GUARD(c);
+  return profile_free(c, id);
+}
+
+extern "C" int st_profiles_free(st_ctx* c, const uint32_t* ids, uint32_t n) {
+  CTX_GUARD(c);
+  if (n && !ids) return fail(ST_EINVAL, "st_profiles_free: null ids");
+  for (uint32_t k = 0; k < n; ++k) ST_TRY(profile_free(c, ids[k]));
   return ST_OK;
 }
 
@@ -709,7 +797,10 @@ static int occupancy_grid(st_ctx* c, const void* fn, int threads, size_t smem, u
 // The launches of one run, in stream order: clear outputs, reset counters,
 // every 16-bit class, then the 32-bit kernel over the static list plus the
 // pairs the 16-bit classes flagged.
-static int plan_enqueue(st_plan* p, cudaStream_t st) {
+// With a fork set, the largest class runs on `st` and the others on fork
+// streams (forked and joined through events, which graph capture records as
+// parallel branches), so the tail of one class overlaps the others.
+static int plan_enqueue(st_plan* p, cudaStream_t st, st_ctx::ForkSet* fs) {
   if (p->n) {
     if (cudaMemsetAsync(p->d_scores, 0, p->n * 4, st) != cudaSuccess) return ST_ECUDA;
     if (p->d_kernels && cudaMemsetAsync(p->d_kernels, 0, p->n * 4, st) != cudaSuccess) return ST_ECUDA;
@@ -717,13 +808,51 @@ static int plan_enqueue(st_plan* p, cudaStream_t st) {
   if (cudaMemcpyAsync(p->counters, p->counters_init, (kNumClasses + 2) * 4, cudaMemcpyDeviceToDevice, st) !=
       cudaSuccess)
     return ST_ECUDA;
-  for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, st>>>(cp.prm);
+  const size_t nc = p->classes.size();
+  if (!fs || nc <= 1) {
+    for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, st>>>(cp.prm);
+  } else {
+    size_t big = 0;
+    for (size_t i = 1; i < nc; ++i)
+      if (p->classes[i].cells > p->classes[big].cells) big = i;
+    if (cudaEventRecord(fs->ev[0], st) != cudaSuccess) return ST_ECUDA;
+    bool used[st_ctx::ForkSet::kForks] = {};
+    int next = 0;
+    for (size_t i = 0; i < nc; ++i) {
+      if (i == big) continue;
+      const int j = next++ % st_ctx::ForkSet::kForks;
+      if (!used[j] && cudaStreamWaitEvent(fs->s[j], fs->ev[0], 0) != cudaSuccess) return ST_ECUDA;
+      used[j] = true;
+      const ClassPlan& cp = p->classes[i];
+      kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, fs->s[j]>>>(cp.prm);
+    }
+    const ClassPlan& cb = p->classes[big];
+    kClasses[cb.cls].fn<<<cb.grid, kWarps16 * 32, cb.smem, st>>>(cb.prm);
+    for (int j = 0; j < st_ctx::ForkSet::kForks; ++j) {
+      if (!used[j]) continue;
+      if (cudaEventRecord(fs->ev[1 + j], fs->s[j]) != cudaSuccess) return ST_ECUDA;
+      if (cudaStreamWaitEvent(st, fs->ev[1 + j], 0) != cudaSuccess) return ST_ECUDA;
+    }
+  }
   sw32_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, st>>>(p->p32);
   return cudaGetLastError() == cudaSuccess ? ST_OK : ST_ECUDA;
 }
 
+static int fork_set(st_ctx* c, int i, st_ctx::ForkSet** out) {
+  st_ctx::ForkSet& f = c->forks[i];
+  for (auto& s : f.s)
+    if (!s) ST_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  for (auto& e : f.ev)
+    if (!e) ST_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  *out = &f;
+  return ST_OK;
+}
+
+// Builds a plan for `n` pairs. Its initialised data is staged in pinned block
+// `slot` of the context's ring and uploaded on `up`; the block is reused only
+// after that copy has finished (an event per block).
 static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* d_scores,
-                      uint32_t* d_kernels, st_plan** out, bool capture) {
+                      uint32_t* d_kernels, st_plan** out, bool capture, cudaStream_t up, int slot) {
   if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
   if (n > 0xFFFFFFF0ull) return fail(ST_EINVAL, "too many pairs (%llu)", static_cast<unsigned long long>(n));
   ST_TRY(sync_profiles(c));
@@ -737,9 +866,19 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   const bool g16 = gaps16_ok(open, ext);
   TraceClock tc("plan");
 
-  std::vector<uint32_t> pq(n), pt(n), tlen(n);
-  std::vector<int32_t> pc(n), pr(n);
-  std::vector<uint8_t> route(n);  // 0: score 0 (empty), 1: 16-bit kernel, 2: 32-bit kernel
+  auto& ps = c->ps;
+  std::vector<uint32_t>& pq = ps.pq;
+  std::vector<uint32_t>& pt = ps.pt;
+  std::vector<uint32_t>& tlen = ps.tlen;
+  std::vector<int32_t>& pc = ps.pc;
+  std::vector<int32_t>& pr = ps.pr;
+  std::vector<uint8_t>& route = ps.route;  // 0: score 0 (empty), 1: 16-bit kernel, 2: 32-bit kernel
+  pq.resize(n);
+  pt.resize(n);
+  tlen.resize(n);
+  pc.resize(n);
+  pr.resize(n);
+  route.resize(n);
   const uint32_t n_prof = static_cast<uint32_t>(c->profs.size());
   int64_t bad = -1;
   uint64_t cells = 0, cells32 = 0;
@@ -793,14 +932,17 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   plan->cells32 = cells32;
   tc.lap("classify");
   // 32-bit list in pair order; 16-bit pairs grouped by query (counting sort)
-  std::vector<uint32_t> list32;
-  std::vector<uint64_t> qstart(static_cast<size_t>(n_prof) + 1, 0);
+  std::vector<uint32_t>& list32 = ps.list32;
+  list32.clear();
+  std::vector<uint64_t>& qstart = ps.qstart;
+  qstart.assign(static_cast<size_t>(n_prof) + 1, 0);
   for (uint64_t i = 0; i < n; ++i) {
     if (route[i] == 2) list32.push_back(static_cast<uint32_t>(i));
     else if (route[i] == 1) ++qstart[pq[i] + 1];
   }
   for (uint32_t q = 0; q < n_prof; ++q) qstart[q + 1] += qstart[q];
-  std::vector<uint32_t> byq(qstart[n_prof]);
+  std::vector<uint32_t>& byq = ps.byq;
+  byq.resize(qstart[n_prof]);
   {
     std::vector<uint64_t> fill(qstart.begin(), qstart.end() - 1);
     for (uint64_t i = 0; i < n; ++i)
@@ -836,23 +978,92 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   if (toolong >= 0) return fail(ST_EINVAL, "query of %d rows does not fit the shared-memory profile", toolong);
   tc.lap("group+sort");
   std::vector<ClassPlan> cps(kNumClasses);
-  for (int k = 0; k < kNumClasses; ++k) cps[k].cls = k;
-  // emission, two passes: sizes and offsets per query (in query order within each class), then a parallel fill
+  for (int k = 0; k < kNumClasses; ++k) {
+    cps[k].cls = k;
+    cps[k].slots.swap(ps.slots[k]);  // borrow the kept buffers (returned below)
+    cps[k].wt.swap(ps.wt[k]);
+    cps[k].cta.swap(ps.cta[k]);
+  }
+  // Emission. A query's pairs (sorted by target length, longest first) form
+  // warp tasks of S = 64/G pairs; consecutive warp tasks form CTA tasks. A CTA
+  // task ends at 64 warp tasks, or (once it holds a warp task for each warp)
+  // when its estimated cost would pass the class's cap: the class's total cost
+  // over kWaves waves of a grid of two CTAs per SM. Small caps keep the
+  // longest CTA task of a long query a small part of the launch, so short
+  // launches (pipelined chunks) end without a long tail.
+  // Passes: warp-task counts and costs, CTA-task counts, offsets, parallel fill.
   struct QEmit {
     uint32_t n_wt, n_cta;
     size_t wt_off, slot_off, cta_off;
+    uint64_t cost;
   };
   std::vector<QEmit> qe(qlist.size());
-  std::vector<size_t> n_wt_cls(kNumClasses, 0), n_slot_cls(kNumClasses, 0), n_cta_cls(kNumClasses, 0);
   constexpr uint32_t kMaxWtPerCta = 64;
+  constexpr uint64_t kWaves = 8;
+  struct QShape {
+    uint32_t S, P, rows, min_cols, step_cost, C;
+  };
+  auto shape_of = [&](int64_t k) {
+    const Sw16Class& kc = kClasses[qclass[k]];
+    QShape sh;
+    sh.S = 64 / kc.G;
+    sh.rows = static_cast<uint32_t>(kc.G * kc.R);
+    sh.P = std::max<uint32_t>(1, (c->profs[qlist[k]].m + sh.rows - 1) / sh.rows);
+    sh.min_cols = sh.P > 1 ? static_cast<uint32_t>(up16(std::max(32, kc.C * kc.G))) : 32u;
+    sh.step_cost = static_cast<uint32_t>(kc.R * kc.C + 8);
+    sh.C = static_cast<uint32_t>(kc.C);
+    return sh;
+  };
+  // columns of warp task w of query k: its first pair has the longest target
+  auto wt_cols = [&](int64_t k, const QShape& sh, uint32_t w) {
+    const uint32_t* v = byq.data() + qstart[qlist[k]];
+    return std::max<uint32_t>(sh.min_cols, static_cast<uint32_t>(up16(tlen[v[static_cast<size_t>(w) * sh.S]])));
+  };
+  auto wt_cost = [&](const QShape& sh, uint32_t ncols) {
+    return static_cast<uint64_t>(sh.P) * (ncols / sh.C) * sh.step_cost;
+  };
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < static_cast<int64_t>(qlist.size()); ++k) {
+    const QShape sh = shape_of(k);
+    const uint64_t np = qstart[qlist[k] + 1] - qstart[qlist[k]];
+    QEmit& e = qe[k];
+    e.n_wt = static_cast<uint32_t>((np + sh.S - 1) / sh.S);
+    e.cost = 0;
+    for (uint32_t w = 0; w < e.n_wt; ++w) e.cost += wt_cost(sh, wt_cols(k, sh, w));
+  }
+  std::vector<uint64_t> cap(kNumClasses, 0);
+  for (size_t k = 0; k < qlist.size(); ++k) cap[qclass[k]] += qe[k].cost;
+  for (int k = 0; k < kNumClasses; ++k) cap[k] = std::max<uint64_t>(1, cap[k] / (kWaves * 2 * c->sms));
+  // calls f(w0, w1, cost) for each CTA task of query k, in order
+  auto for_each_cta = [&](int64_t k, const QShape& sh, auto&& f) {
+    const uint32_t n_wt = qe[k].n_wt;
+    const uint64_t cp = cap[qclass[k]];
+    uint32_t w0 = 0;
+    uint64_t acc = 0;
+    for (uint32_t w = 0; w < n_wt; ++w) {
+      const uint64_t cw = wt_cost(sh, wt_cols(k, sh, w));
+      const uint32_t cnt = w - w0;
+      if (cnt == kMaxWtPerCta || (cnt >= static_cast<uint32_t>(kWarps16) && acc + cw > cp)) {
+        f(w0, w, acc);
+        w0 = w;
+        acc = 0;
+      }
+      acc += cw;
+    }
+    if (n_wt > w0) f(w0, n_wt, acc);
+  };
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < static_cast<int64_t>(qlist.size()); ++k) {
+    uint32_t n = 0;
+    for_each_cta(k, shape_of(k), [&](uint32_t, uint32_t, uint64_t) { ++n; });
+    qe[k].n_cta = n;
+  }
+  std::vector<size_t> n_wt_cls(kNumClasses, 0), n_slot_cls(kNumClasses, 0), n_cta_cls(kNumClasses, 0);
   for (size_t k = 0; k < qlist.size(); ++k) {
     const uint32_t q = qlist[k];
     const int cls = qclass[k];
     const uint32_t S = 64 / kClasses[cls].G;
-    const uint64_t np = qstart[q + 1] - qstart[q];
     QEmit& e = qe[k];
-    e.n_wt = static_cast<uint32_t>((np + S - 1) / S);
-    e.n_cta = (e.n_wt + kMaxWtPerCta - 1) / kMaxWtPerCta;
     e.wt_off = n_wt_cls[cls];
     e.slot_off = n_slot_cls[cls];
     e.cta_off = n_cta_cls[cls];
@@ -872,21 +1083,16 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   for (int64_t k = 0; k < static_cast<int64_t>(qlist.size()); ++k) {
     const uint32_t q = qlist[k];
     const int cls = qclass[k];
-    const Sw16Class& kc = kClasses[cls];
     ClassPlan& cp = cps[cls];
     const QEmit& e = qe[k];
-    const uint32_t S = 64 / kc.G;
-    const uint32_t m = c->profs[q].m;
-    const uint32_t rows = static_cast<uint32_t>(kc.G * kc.R);
-    const uint32_t P = std::max<uint32_t>(1, (m + rows - 1) / rows);
-    const uint32_t min_cols = P > 1 ? static_cast<uint32_t>(up16(std::max(32, kc.C * kc.G))) : 32u;
+    const QShape sh = shape_of(k);
     const uint32_t* v = byq.data() + qstart[q];
     const size_t np = qstart[q + 1] - qstart[q];
     for (uint32_t w = 0; w < e.n_wt; ++w) {
-      const size_t sb = e.slot_off + static_cast<size_t>(w) * S;
-      uint32_t ncols = min_cols;
-      for (uint32_t sidx = 0; sidx < S; ++sidx) {
-        const size_t j = static_cast<size_t>(w) * S + sidx;
+      const size_t sb = e.slot_off + static_cast<size_t>(w) * sh.S;
+      uint32_t ncols = sh.min_cols;
+      for (uint32_t sidx = 0; sidx < sh.S; ++sidx) {
+        const size_t j = static_cast<size_t>(w) * sh.S + sidx;
         Sw16Slot sl{kNoPair, 0, 0, 0};
         if (j < np) {
           const uint32_t pi = v[j];
@@ -900,15 +1106,13 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
       }
       cp.wt[e.wt_off + w] = Sw16WarpTask{static_cast<uint32_t>(sb), ncols};
     }
-    for (uint32_t t = 0; t < e.n_cta; ++t) {
-      const uint32_t w0 = t * kMaxWtPerCta, w1 = std::min(e.n_wt, w0 + kMaxWtPerCta);
-      cp.cta[e.cta_off + t] = Sw16CtaTask{q, static_cast<uint32_t>(e.wt_off + w0), static_cast<uint32_t>(e.wt_off + w1),
-                                          P * rows};
-      uint64_t cst = 0;
-      for (uint32_t w = w0; w < w1; ++w)
-        cst += static_cast<uint64_t>(P * cp.wt[e.wt_off + w].ncols / kc.C) * (kc.R * kc.C + 8);
-      cta_cost[cls][e.cta_off + t] = cst;
-    }
+    size_t t = e.cta_off;
+    for_each_cta(k, sh, [&](uint32_t w0, uint32_t w1, uint64_t cost) {
+      cp.cta[t] = Sw16CtaTask{q, static_cast<uint32_t>(e.wt_off + w0), static_cast<uint32_t>(e.wt_off + w1),
+                              sh.P * sh.rows};
+      cta_cost[cls][t] = cost;
+      ++t;
+    });
   }
   tc.lap("emit");
   // order CTA tasks by estimated cost, longest first
@@ -985,9 +1189,12 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   tc.lap("arena");
   char* dbase = plan->arena.as<char>();
   // stage the data region in pinned memory and upload it at once
-  ST_TRY(c->pin.reserve(data_bytes));
-  ST_CUDA(cudaStreamSynchronize(c->stream));  // the pinned block may still feed an earlier copy
-  char* h = c->pin.as<char>();
+  Pinned& pin = c->plan_pin[slot];
+  if (!c->plan_pin_ev[slot]) ST_CUDA(cudaEventCreateWithFlags(&c->plan_pin_ev[slot], cudaEventDisableTiming));
+  if (c->plan_pin_used[slot]) ST_CUDA(cudaEventSynchronize(c->plan_pin_ev[slot]));  // may still feed a copy
+  c->plan_pin_used[slot] = false;
+  ST_TRY(pin.reserve(data_bytes));
+  char* h = pin.as<char>();
 #pragma omp parallel sections
   {
 #pragma omp section
@@ -1016,14 +1223,40 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     if (cp.cta.empty()) continue;
     memcpy(h + cp.o_cta, cp.cta.data(), cp.cta.size() * sizeof(Sw16CtaTask));
     memcpy(h + cp.o_wt, cp.wt.data(), cp.wt.size() * sizeof(Sw16WarpTask));
-    memcpy(h + cp.o_slots, cp.slots.data(), cp.slots.size() * sizeof(Sw16Slot));
+    const size_t ns = cp.slots.size();
+    const Sw16Slot* src = cp.slots.data();
+    Sw16Slot* dst = reinterpret_cast<Sw16Slot*>(h + cp.o_slots);
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < static_cast<int64_t>((ns + 65535) / 65536); ++b) {
+      const size_t a0 = static_cast<size_t>(b) * 65536, a1 = std::min(ns, a0 + 65536);
+      memcpy(dst + a0, src + a0, (a1 - a0) * sizeof(Sw16Slot));
+    }
   }
-  ST_CUDA(cudaMemcpyAsync(dbase, h, data_bytes, cudaMemcpyHostToDevice, c->stream));
+  ST_CUDA(cudaMemcpyAsync(dbase, h, data_bytes, cudaMemcpyHostToDevice, up));
+  ST_CUDA(cudaEventRecord(c->plan_pin_ev[slot], up));
+  c->plan_pin_used[slot] = true;
   tc.lap("stage+upload");
   plan->counters = reinterpret_cast<uint32_t*>(dbase + o_cnt);
   plan->counters_init = reinterpret_cast<const uint32_t*>(dbase + o_cinit);
-  for (auto& cp : cps)
-    if (!cp.cta.empty()) plan->classes.push_back(std::move(cp));
+  for (auto& cp : cps) {
+    if (!cp.cta.empty()) {
+      ClassPlan kept;
+      kept.cls = cp.cls;
+      kept.cta.assign(cp.cta.begin(), cp.cta.end());  // small: one entry per query and class
+      kept.grid = cp.grid;
+      kept.smem = cp.smem;
+      kept.scratch_stride = cp.scratch_stride;
+      kept.cells = cp.cells;
+      kept.o_cta = cp.o_cta;
+      kept.o_wt = cp.o_wt;
+      kept.o_slots = cp.o_slots;
+      kept.o_scratch = cp.o_scratch;
+      plan->classes.push_back(std::move(kept));
+    }
+    ps.slots[cp.cls].swap(cp.slots);
+    ps.wt[cp.cls].swap(cp.wt);
+    ps.cta[cp.cls].swap(cp.cta);
+  }
 
   const DeviceDb db = db_view(c);
   const DeviceProfiles pv = prof_view(c);
@@ -1076,9 +1309,11 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1;
   if (capture) {
     // capture a run into a CUDA graph on the context's own stream (ordered after the upload)
-    ST_CUDA(cudaStreamSynchronize(c->stream));
+    ST_CUDA(cudaStreamSynchronize(up));
     ST_CUDA(cudaStreamBeginCapture(c->own, cudaStreamCaptureModeThreadLocal));
-    const int rc = plan_enqueue(plan.get(), c->own);
+    st_ctx::ForkSet* fs = nullptr;
+    ST_TRY(fork_set(c, 0, &fs));
+    const int rc = plan_enqueue(plan.get(), c->own, fs);
     cudaError_t ce = cudaStreamEndCapture(c->own, &plan->graph);
     if (rc != ST_OK || ce != cudaSuccess)
       return fail(ST_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce != cudaSuccess ? ce : cudaGetLastError()));
@@ -1092,8 +1327,11 @@ static int plan_run(st_plan* p) {
   st_ctx* c = p->ctx;
   if (p->exec) {
     ST_CUDA(cudaGraphLaunch(p->exec, c->stream));
-  } else if (plan_enqueue(p, c->stream) != ST_OK) {
-    return fail(ST_ECUDA, "plan launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  } else {
+    st_ctx::ForkSet* fs = nullptr;
+    ST_TRY(fork_set(c, 0, &fs));
+    if (plan_enqueue(p, c->stream, fs) != ST_OK)
+      return fail(ST_ECUDA, "plan launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   c->launches += p->kernels_per_run;
   return ST_OK;
@@ -1111,7 +1349,7 @@ extern "C" int st_plan_create(st_ctx* c, const st_pair* pairs, uint64_t n, int32
                               int32_t* d_scores, uint32_t* d_kernels, st_plan** plan) {
   CTX_GUARD(c);
   if (!plan || (n && (!pairs || !d_scores))) return fail(ST_EINVAL, "st_plan_create: null argument");
-  return plan_build(c, pairs, n, open, ext, d_scores, d_kernels, plan, true);
+  return plan_build(c, pairs, n, open, ext, d_scores, d_kernels, plan, true, c->stream, 0);
 }
 
 extern "C" int st_plan_run(st_plan* p) {
@@ -1182,6 +1420,34 @@ extern "C" void st_plan_destroy(st_plan* p) {
   plan_free(p);
 }
 
+static bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // not a CUDA-known pointer: pageable
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Pipelining of large batches: pairs per chunk (ST_PIPELINE_PAIRS overrides;
+// 0 turns pipelining off) and side streams the chunks rotate over
+// (ST_PIPELINE_STREAMS, 1 to 4).
+static uint64_t env_u64(const char* name, uint64_t dflt) {
+  const char* v = getenv(name);
+  if (!v || !*v) return dflt;
+  return strtoull(v, nullptr, 10);
+}
+
+static uint64_t pipeline_chunks(uint64_t n) {
+  const uint64_t chunk = env_u64("ST_PIPELINE_PAIRS", 160 * 1024);
+  if (chunk == 0 || n < chunk + chunk / 2) return 1;
+  return std::min<uint64_t>(64, (n + chunk - 1) / chunk);
+}
+
+static int pipeline_streams() {
+  return static_cast<int>(std::min<uint64_t>(st_ctx::kMaxSide, std::max<uint64_t>(1, env_u64("ST_PIPELINE_STREAMS", 4))));
+}
+
 extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
                                  int32_t* scores, uint32_t* kernels) {
   CTX_GUARD(c);
@@ -1196,15 +1462,133 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
   } back{c, &d_out};
   int32_t* d_scores = d_out.as<int32_t>();
   uint32_t* d_kern = reinterpret_cast<uint32_t*>(d_scores + n);
-  st_plan* p = nullptr;
   TraceClock tc("pairs");
-  ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p, false));
-  std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
-  tc.lap("plan");
-  ST_TRY(plan_run(p));
-  ST_CUDA(cudaMemcpyAsync(scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
-  if (kernels) ST_CUDA(cudaMemcpyAsync(kernels, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  // Results come back through pinned memory unless the caller's buffers are
+  // pinned already: a copy into pageable memory would block the host until
+  // the kernels before it finish, which serialises planning with the GPU.
+  const bool direct = host_pinned(scores) && (!kernels || host_pinned(kernels));
+  int32_t* h_scores = scores;
+  uint32_t* h_kern = kernels;
+  if (!direct) {
+    ST_TRY(c->out_pin.reserve(n * 8));
+    h_scores = c->out_pin.as<int32_t>();
+    h_kern = kernels ? c->out_pin.as<uint32_t>(n * 4) : nullptr;
+  }
+  auto copy_out = [&]() {
+    if (direct) return;
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < static_cast<int64_t>((n + 262143) / 262144); ++b) {
+      const uint64_t a0 = static_cast<uint64_t>(b) * 262144, a1 = std::min<uint64_t>(n, a0 + 262144);
+      memcpy(scores + a0, h_scores + a0, (a1 - a0) * 4);
+      if (kernels) memcpy(kernels + a0, h_kern + a0, (a1 - a0) * 4);
+    }
+  };
+  const uint64_t chunks = pipeline_chunks(n);
+  if (chunks <= 1) {
+    st_plan* p = nullptr;
+    ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p, false, c->stream, 0));
+    std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
+    tc.lap("plan");
+    ST_TRY(plan_run(p));
+    ST_CUDA(cudaMemcpyAsync(h_scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (kernels) ST_CUDA(cudaMemcpyAsync(h_kern, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    copy_out();
+    tc.lap("run+download");
+    return ST_OK;
+  }
+  // Pipelined: the pairs are cut into contiguous chunks, each planned on the
+  // host while the chunks before it run. Chunks alternate between two side
+  // streams, so the tail of one chunk's persistent grid overlaps the start of
+  // the next; each chunk downloads its own scores on its stream.
+  ST_TRY(sync_profiles(c));
+  {
+    // every pair is checked before the first chunk launches, so an error leaves no partial work
+    const uint32_t n_prof = static_cast<uint32_t>(c->profs.size());
+    int64_t bad = INT64_MAX;
+#pragma omp parallel for schedule(static) reduction(min : bad)
+    for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+      const st_pair& p = pairs[i];
+      if (p.profile >= n_prof || !c->profs[p.profile].live || p.target >= c->n_seqs) bad = std::min<int64_t>(bad, i);
+    }
+    if (bad != INT64_MAX) {
+      const st_pair& p = pairs[bad];
+      if (p.profile >= n_prof || !c->profs[p.profile].live)
+        return fail(ST_EINVAL, "pair %lld: unknown profile id %u", static_cast<long long>(bad), p.profile);
+      return fail(ST_EINVAL, "pair %lld: target %u outside the database (%u sequences)", static_cast<long long>(bad),
+                  p.target, c->n_seqs);
+    }
+  }
+  const int n_side = pipeline_streams();
+  for (int i = 0; i < n_side; ++i)
+    if (!c->side[i]) ST_CUDA(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
+  for (auto& e : c->side_ev)
+    if (!e) ST_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  ST_CUDA(cudaEventRecord(c->side_ev[0], c->stream));  // after earlier work on the caller's stream
+  for (int i = 0; i < n_side; ++i) ST_CUDA(cudaStreamWaitEvent(c->side[i], c->side_ev[0], 0));
+  std::vector<std::unique_ptr<st_plan, void (*)(st_plan*)>> plans;
+  plans.reserve(chunks);
+  // with ST_TRACE: device time of each chunk's launches, relative to the batch start
+  std::vector<cudaEvent_t> tev;
+  if (trace_on()) {
+    tev.assign(2 * chunks + 1, nullptr);
+    for (auto& e : tev) cudaEventCreate(&e);
+    cudaEventRecord(tev[0], c->stream);
+  }
+  struct Drain {  // on every exit: the side streams finish before any plan (and its arena) is released
+    st_ctx* c;
+    ~Drain() {
+      for (auto s : c->side)
+        if (s) cudaStreamSynchronize(s);
+    }
+  };
+  int rc = ST_OK;
+  {
+    Drain drain{c};
+    for (uint64_t k = 0; k < chunks && rc == ST_OK; ++k) {
+      const uint64_t b = n * k / chunks, e = n * (k + 1) / chunks;
+      cudaStream_t s = c->side[k % n_side];
+      st_plan* p = nullptr;
+      rc = plan_build(c, pairs + b, e - b, open, ext, d_scores + b, d_kern + b, &p, false, s,
+                      static_cast<int>(k % st_ctx::kStageRing));
+      if (rc != ST_OK) break;
+      plans.emplace_back(p, plan_free);
+      if (!tev.empty()) cudaEventRecord(tev[1 + 2 * k], s);
+      st_ctx::ForkSet* fs = nullptr;
+      rc = fork_set(c, 1 + static_cast<int>(k % n_side), &fs);
+      if (rc != ST_OK) break;
+      if (plan_enqueue(p, s, fs) != ST_OK) {
+        rc = fail(ST_ECUDA, "plan launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        break;
+      }
+      c->launches += p->kernels_per_run;
+      if (!tev.empty()) cudaEventRecord(tev[2 + 2 * k], s);
+      if (cudaMemcpyAsync(h_scores + b, d_scores + b, (e - b) * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          (kernels && cudaMemcpyAsync(h_kern + b, d_kern + b, (e - b) * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess))
+        rc = fail(ST_ECUDA, "score download failed: %s", cudaGetErrorString(cudaGetLastError()));
+      tc.lap("chunk");
+    }
+    if (rc == ST_OK) {
+      // the caller's stream is ordered after the batch
+      for (int i = 0; i < n_side && rc == ST_OK; ++i)
+        if (cudaEventRecord(c->side_ev[1 + i], c->side[i]) != cudaSuccess ||
+            cudaStreamWaitEvent(c->stream, c->side_ev[1 + i], 0) != cudaSuccess)
+          rc = fail(ST_ECUDA, "stream ordering failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+  }
+  if (!tev.empty()) {
+    cudaStreamSynchronize(c->stream);
+    for (uint64_t k = 0; k < plans.size(); ++k) {
+      float a = 0, b = 0;
+      cudaEventElapsedTime(&a, tev[0], tev[1 + 2 * k]);
+      cudaEventElapsedTime(&b, tev[0], tev[2 + 2 * k]);
+      fprintf(stderr, "[st] chunk %llu device %.3f .. %.3f ms (%.3f)\n", static_cast<unsigned long long>(k), a, b, b - a);
+    }
+    for (auto e : tev) cudaEventDestroy(e);
+  }
+  if (rc != ST_OK) return rc;
   ST_CUDA(cudaStreamSynchronize(c->stream));
+  copy_out();
   tc.lap("run+download");
   return ST_OK;
 }
@@ -1627,7 +2011,7 @@ extern "C" int st_autotune(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t 
       if (tune_cost(&c->tuning, k, max_m, 64, false) >= 1e300) continue;
       c->tuning.table[mb][nb] = k;
       st_plan* p = nullptr;
-      ST_TRY(plan_build(c, v.data(), v.size(), open, ext, out.as<int32_t>(), nullptr, &p, true));
+      ST_TRY(plan_build(c, v.data(), v.size(), open, ext, out.as<int32_t>(), nullptr, &p, true, c->stream, 0));
       std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
       cudaStream_t saved = c->stream;
       c->stream = c->own;

@@ -98,3 +98,96 @@ def test_memory_budget_is_enforced():
             c.create_profiles([np.zeros((20000, 21), dtype=np.int32)])
     finally:
         c.close()
+
+
+def _big_batch(seed, n_pairs, n_q=700, n_t=4000):
+    """Many short pairs: enough for the pipelined (chunked, two-stream) form, cheap for the oracle."""
+    from sabertooth_b200 import blosum62
+    rng = np.random.default_rng(seed)
+    m = blosum62()
+    queries = [rng.integers(0, 21, int(L)).astype(np.uint8) for L in rng.integers(0, 70, n_q)]
+    targets = [rng.integers(0, 22, int(L)).astype(np.uint8) for L in rng.integers(0, 90, n_t)]
+    for k in range(0, n_t, 7):  # near-identical targets so that some scores are high
+        q = queries[k % n_q]
+        targets[k] = np.concatenate([targets[k][:5], q, targets[k][5:]]).astype(np.uint8)
+    rows = [m.sequence_rows(q) for q in queries]
+    pq = rng.integers(0, n_q, n_pairs).astype(np.uint32)
+    pt = rng.integers(0, n_t, n_pairs).astype(np.uint32)
+    return rows, targets, pq, pt
+
+
+def test_pipelined_batch_matches_oracle_and_single_plan(ctx):
+    import torch
+    rows, targets, pq, pt = _big_batch(11, 420_000)
+    n = len(pq)
+    center = np.zeros(n, dtype=np.int32)
+    radius = np.full(n, -1, dtype=np.int32)
+    banded = np.arange(0, n, 997)  # banded pairs in every chunk take the 32-bit kernel
+    radius[banded] = 3
+    center[banded] = (np.arange(len(banded)) % 9) - 4
+    ctx.upload_db_list(targets)
+    ids = ctx.create_profiles(rows)
+    try:
+        pairs = np.zeros(n, dtype=PAIR_DTYPE)
+        pairs["profile"] = ids[pq]
+        pairs["target"] = pt
+        pairs["band_center"] = center
+        pairs["band_radius"] = radius
+        for gaps in [GapCosts(11, 1), GapCosts(300, 1)]:  # the second routes every pair to the 32-bit kernel
+            got, kinds = ctx.sw_score_pairs(pairs, gaps, with_kernels=True)
+            want = O.sw_pairs(O.Arena(rows, targets), pq, pt, gaps.open, gaps.extend, center.astype(np.int64),
+                              radius.astype(np.int64))
+            assert np.array_equal(got, want), gaps
+            # the single captured plan (no chunking) gives the same scores and kernel tags
+            d_s = torch.empty(n, dtype=torch.int32, device="cuda")
+            d_k = torch.empty(n, dtype=torch.int32, device="cuda")
+            plan = ctx.plan(pairs, gaps, d_s.data_ptr(), d_k.data_ptr())
+            plan.run()
+            ctx.synchronize()
+            assert np.array_equal(d_s.cpu().numpy(), got)
+            assert np.array_equal(d_k.cpu().numpy().view(np.uint32), kinds)
+            plan.close()
+        # twice in a row: pooled arenas and the staging ring give the same result
+        assert np.array_equal(ctx.sw_score_pairs(pairs, GapCosts(11, 1)), ctx.sw_score_pairs(pairs, GapCosts(11, 1)))
+    finally:
+        for i in ids:
+            ctx.free_profile(i)
+
+
+def test_pipelined_batch_error_in_a_late_chunk_leaves_context_usable(ctx):
+    from sabertooth_b200._lib import StError
+    rows, targets, pq, pt = _big_batch(12, 400_000)
+    ctx.upload_db_list(targets)
+    ids = ctx.create_profiles(rows)
+    try:
+        pairs = np.zeros(len(pq), dtype=PAIR_DTYPE)
+        pairs["profile"] = ids[pq]
+        pairs["target"] = pt
+        pairs["band_radius"] = -1
+        bad = pairs.copy()
+        bad["target"][len(pq) - 5] = 10_000_000  # in the last chunk, after earlier chunks were launched
+        with pytest.raises(StError, match="outside the database"):
+            ctx.sw_score_pairs(bad, GapCosts(11, 1))
+        got = ctx.sw_score_pairs(pairs, GapCosts(11, 1))
+        assert np.array_equal(got, O.sw_pairs(O.Arena(rows, targets), pq, pt, 11, 1))
+    finally:
+        for i in ids:
+            ctx.free_profile(i)
+
+
+def test_profile_ids_are_reused_and_batch_free_checks_ids(ctx):
+    from sabertooth_b200._lib import StError
+    w = W.config3(seed=4, n_queries=6, db_residues=20_000, per_query=10)
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    first = ctx.sw_score_pairs(_pairs(ids, w), GapCosts(44, 4))
+    ctx.free_profiles(ids)
+    with pytest.raises(StError, match="unknown profile"):
+        ctx.free_profiles(ids[:1])
+    again = ctx.create_profiles(w.rows[::-1])  # the same ids come back, now for other rows
+    assert sorted(again.tolist()) == sorted(ids.tolist())
+    rev = again[::-1]
+    assert np.array_equal(ctx.sw_score_pairs(_pairs(rev, w), GapCosts(44, 4)), first)
+    want = O.sw_pairs(O.Arena(w.rows, w.targets()), w.pair_q, w.pair_t, 44, 4)
+    assert np.array_equal(first, want)
+    ctx.free_profiles(again)
