@@ -40,9 +40,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="fraction of the 4,000 queries (quick runs)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--tuning-in", default=None, help="load a saved tile-class table (JSON) before planning")
-    ap.add_argument("--tuning-out", default=None, help="save the tile-class table used (JSON)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure the tile-class rates on this workload instead of the built-in B200 rates")
+    ap.add_argument("--no-autotune", action="store_true", help="(default) use the built-in or loaded rates")
+    ap.add_argument("--tuning-in", default=None, help="load a saved tile-class table and rates (JSON) before planning")
+    ap.add_argument("--tuning-out", default=None, help="save the tile-class table and rates used (JSON)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--plain-pairs", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -231,12 +233,15 @@ def main():
 
     t_tune = time.perf_counter()
     if args.tuning_in:
-        ctx.set_tuning_table(np.array(json.load(open(args.tuning_in))["table"], dtype=np.int32))
-    tuned = 0 if args.no_autotune else ctx.autotune(pairs, gaps, max_pairs_per_bin=6000)
+        saved_tuning = json.load(open(args.tuning_in))
+        ctx.set_tuning_table(np.array(saved_tuning["table"], dtype=np.int32))
+        if "rates" in saved_tuning:
+            ctx.set_tuning_rates(np.array(saved_tuning["rates"], dtype=np.float32))
+    tuned = ctx.autotune(pairs, gaps, max_pairs=400_000) if args.autotune and not args.no_autotune else 0
     t_tune = time.perf_counter() - t_tune
     if args.tuning_out and rank == 0:
         with open(args.tuning_out, "w") as f:
-            json.dump({"table": ctx.tuning_table().tolist()}, f)
+            json.dump({"table": ctx.tuning_table().tolist(), "rates": ctx.tuning_rates().tolist()}, f)
 
     d_scores = torch.empty(w.n_pairs, dtype=torch.int32, device="cuda")
     d_kern = torch.empty(w.n_pairs, dtype=torch.int32, device="cuda")
@@ -377,7 +382,8 @@ def main():
             "gpu32_pairs": int((kern == 2).sum()),
             "launch_classes": int(stats["launch_classes"]),
             "launch_profile": launch_profile,
-            "autotuned_bins": int(tuned),
+            "autotuned_classes": int(tuned),
+            "class_rates_tcells_per_s": [round(float(r), 3) for r in ctx.tuning_rates()],
             "setup_s": {"generate": round(t_gen, 1), "autotune": round(t_tune, 1), "plan": round(t_plan, 2)},
             "step_ms_min_max": [round(min(step_ms), 3), round(max(step_ms), 3)],
         }

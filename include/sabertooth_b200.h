@@ -155,19 +155,28 @@ int st_ungapped_hits_device(st_ctx* ctx, const st_hit* d_hits, uint64_t n, int32
 
 /* ---- tile classes and autotuning ----------------------------------------- */
 /* The packed 16-bit kernel runs in tile classes: G lanes per alignment x R
- * query rows per lane x C target columns per wavefront step.  A per-context table maps (query-length bin, mean
- * target-length bin) to a class; -1 entries use the built-in cost model.
- * Query bins: <=32, <=64, ..., <=8192, >8192 (10); target bins: <=64, <=128,
- * ..., <=4096, >4096 (8); the table is row-major [10][8].  (No reference
- * counterpart: the reference picks SIMD widths at run time, src/simd.rs:59-124.) */
+ * query rows per lane x C target columns per wavefront step.  In a batch each
+ * query takes the class with the least estimated time: its streamed cells
+ * (padded rows x padded columns) over the class's rate (streamed cells per
+ * second / 1e12; built-in B200 figures until st_autotune measures them; a rate
+ * of 0 leaves the class out).  A per-context table maps (query-length bin,
+ * mean target-length bin) to a class that is then forced; -1 entries (the
+ * default) use the rates.  Query bins: <=32, <=64, ..., <=8192, >8192 (10);
+ * target bins: <=64, <=128, ..., <=4096, >4096 (8); the table is row-major
+ * [10][8].  (No reference counterpart: the reference picks SIMD widths at run
+ * time, src/simd.rs:59-124.) */
 int st_tune_num_classes(void);
 int st_tune_class_shape(int cls, int* lanes_per_alignment, int* rows_per_lane, int* cols_per_step);
 int st_tune_get(st_ctx* ctx, int32_t* table);
 int st_tune_set(st_ctx* ctx, const int32_t* table);
-/* Times every feasible class on samples (whole queries, up to max_pairs_per_bin
- * pairs) of each length bin present in the pairs and stores the fastest. */
+/* Per-class rates: rates[k] for k < min(cap, st_tune_num_classes()). */
+int st_tune_get_rates(st_ctx* ctx, float* rates, uint32_t cap);
+int st_tune_set_rates(st_ctx* ctx, const float* rates, uint32_t n);
+/* Measures every class's rate on a sample of the pairs (whole queries, spread
+ * over the batch, up to max_pairs pairs) by planning it with all queries forced
+ * into that class; the forcing table is left as it was. */
 int st_autotune(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
-                uint32_t max_pairs_per_bin, uint32_t* bins_tuned);
+                uint32_t max_pairs, uint32_t* classes_calibrated);
 
 /* ---- allocation-free scoring ----------------------------------------------- */
 /* Exact SW-Gotoh score of ONE pair over caller-owned device buffers, with no

@@ -71,6 +71,8 @@ SIGNATURES = {
     "st_tune_class_shape": (C.c_int, [C.c_int, _P, _P, _P]),
     "st_tune_get": (C.c_int, [_P, _P]),
     "st_tune_set": (C.c_int, [_P, _P]),
+    "st_tune_get_rates": (C.c_int, [_P, _P, _u32]),
+    "st_tune_set_rates": (C.c_int, [_P, _P, _u32]),
     "st_autotune": (C.c_int, [_P, _P, _u64, _i32, _i32, _u32, _P]),
     "st_sw_score_noalloc": (C.c_int, [_P, _u32, _P, _u32, _i32, _i32, _P, _P]),
     "st_probe_dpx": (C.c_int, [_P, _P]),

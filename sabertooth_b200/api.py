@@ -186,11 +186,11 @@ class Context:
                                           _vp(d_n_pairs)))
 
     # -- tuning / measurement ---------------------------------------------------
-    def autotune(self, pairs, gaps: GapCosts, max_pairs_per_bin=4096):
+    def autotune(self, pairs, gaps: GapCosts, max_pairs=200_000):
+        """Measures every tile class's rate on a sample of `pairs`; returns the number of classes measured."""
         pairs = as_pairs(pairs)
         nb = C.c_uint32()
-        check(lib.st_autotune(self._h, ptr(pairs), len(pairs), gaps.open, gaps.extend, max_pairs_per_bin,
-                              C.byref(nb)))
+        check(lib.st_autotune(self._h, ptr(pairs), len(pairs), gaps.open, gaps.extend, max_pairs, C.byref(nb)))
         return nb.value
 
     def tuning_table(self):
@@ -201,6 +201,15 @@ class Context:
     def set_tuning_table(self, table):
         t = np.ascontiguousarray(table, dtype=np.int32).reshape(10, 8)
         check(lib.st_tune_set(self._h, ptr(t)))
+
+    def tuning_rates(self):
+        r = np.zeros(lib.st_tune_num_classes(), dtype=np.float32)
+        check(lib.st_tune_get_rates(self._h, ptr(r), len(r)))
+        return r
+
+    def set_tuning_rates(self, rates):
+        r = np.ascontiguousarray(rates, dtype=np.float32)
+        check(lib.st_tune_set_rates(self._h, ptr(r), len(r)))
 
     def probe_dpx(self):
         v = C.c_double()

@@ -160,6 +160,7 @@ struct Pinned {
 };
 
 static inline size_t up16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+static inline size_t up4(size_t x) { return (x + 3) & ~static_cast<size_t>(3); }
 static inline size_t up256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
 // ---------------------------------------------------------------------------
@@ -172,18 +173,24 @@ constexpr int kMaxSmem = 226 * 1024;  // dynamic shared memory per CTA (the 227 
 using Sw16Fn = void (*)(const Sw16Params);
 
 struct Sw16Class {
-  int G, R, C;
+  int G, R, C, W;  // lanes per alignment, rows per lane, columns per step, warps per CTA
   Sw16Fn fn;
 };
 
-#define ST_CLASS(g, r, c) {g, r, c, sw16_kernel<g, r, c, kWarps16>}
+#define ST_CLASS(g, r, c) {g, r, c, kWarps16, sw16_kernel<g, r, c, kWarps16>}
+#define ST_CLASS_W(g, r, c, w) {g, r, c, w, sw16_kernel<g, r, c, w>}
 static const Sw16Class kClasses[] = {
     ST_CLASS(4, 8, 4),   ST_CLASS(8, 8, 4),   ST_CLASS(16, 8, 4),  ST_CLASS(32, 8, 4),
-    ST_CLASS(8, 16, 2),  ST_CLASS(16, 8, 2),  ST_CLASS(16, 16, 2), ST_CLASS(32, 8, 2),
-    ST_CLASS(32, 12, 2), ST_CLASS(32, 16, 2), ST_CLASS(32, 20, 2), ST_CLASS(32, 24, 2),
+    ST_CLASS(4, 12, 4),  ST_CLASS(8, 12, 4),  ST_CLASS(16, 12, 4), ST_CLASS(32, 12, 4),
+    ST_CLASS(4, 16, 4),  ST_CLASS(8, 16, 4),  ST_CLASS(16, 16, 4), ST_CLASS(32, 16, 4),
+    ST_CLASS(4, 24, 4),  ST_CLASS(8, 24, 4),  ST_CLASS(16, 24, 4), ST_CLASS(32, 24, 4),
+    ST_CLASS_W(4, 32, 4, 4), ST_CLASS_W(8, 32, 4, 4), ST_CLASS_W(16, 32, 4, 4),
+    ST_CLASS(32, 16, 2),
 };
 #undef ST_CLASS
+#undef ST_CLASS_W
 constexpr int kNumClasses = sizeof(kClasses) / sizeof(kClasses[0]);
+static_assert(kNumClasses <= kMaxTileClasses, "tile classes exceed the tuning arrays");
 
 int st_tuning_num_classes() { return kNumClasses; }
 void st_tuning_class_shape(int c, int* G, int* R, int* C) {
@@ -762,7 +769,8 @@ struct ClassPlan {
   uint32_t grid = 0;
   uint32_t smem = 0;
   uint32_t scratch_stride = 0;
-  uint64_t cells = 0;  // sum of m*n over this class's pairs
+  uint64_t cells = 0;     // sum of m*n over this class's pairs
+  uint64_t streamed = 0;  // cells the wavefront streams (padded rows x padded columns x slots)
   Sw16Params prm;
 };
 
@@ -780,6 +788,7 @@ struct st_plan {
   uint32_t grid32 = 0, scratch32_stride = 0;
   uint64_t cells = 0;
   uint64_t cells32 = 0;  // cells of pairs sent to the 32-bit kernel at plan time (band cells for bands)
+  uint64_t streamed = 0;  // cells streamed by the 16-bit classes
   uint32_t kernels_per_run = 0;
   Sw32Params p32;
   cudaGraph_t graph = nullptr;
@@ -810,7 +819,7 @@ static int plan_enqueue(st_plan* p, cudaStream_t st, st_ctx::ForkSet* fs) {
     return ST_ECUDA;
   const size_t nc = p->classes.size();
   if (!fs || nc <= 1) {
-    for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, st>>>(cp.prm);
+    for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, st>>>(cp.prm);
   } else {
     size_t big = 0;
     for (size_t i = 1; i < nc; ++i)
@@ -824,10 +833,10 @@ static int plan_enqueue(st_plan* p, cudaStream_t st, st_ctx::ForkSet* fs) {
       if (!used[j] && cudaStreamWaitEvent(fs->s[j], fs->ev[0], 0) != cudaSuccess) return ST_ECUDA;
       used[j] = true;
       const ClassPlan& cp = p->classes[i];
-      kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, fs->s[j]>>>(cp.prm);
+      kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, fs->s[j]>>>(cp.prm);
     }
     const ClassPlan& cb = p->classes[big];
-    kClasses[cb.cls].fn<<<cb.grid, kWarps16 * 32, cb.smem, st>>>(cb.prm);
+    kClasses[cb.cls].fn<<<cb.grid, kClasses[cb.cls].W * 32, cb.smem, st>>>(cb.prm);
     for (int j = 0; j < st_ctx::ForkSet::kForks; ++j) {
       if (!used[j]) continue;
       if (cudaEventRecord(fs->ev[1 + j], fs->s[j]) != cudaSuccess) return ST_ECUDA;
@@ -864,6 +873,14 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   plan->d_scores = d_scores;
   plan->d_kernels = d_kernels;
   const bool g16 = gaps16_ok(open, ext);
+  // the longest query whose int8 profile fits the shared memory of some 16-bit class;
+  // longer ones take the 32-bit kernel
+  uint32_t max_m16 = 0;
+  for (int k = 0; k < kNumClasses; ++k) {
+    const uint32_t rows = static_cast<uint32_t>(kClasses[k].G * kClasses[k].R);
+    const uint32_t smem = static_cast<uint32_t>(std::min<int>(g_class_smem[k], 216 * 1024));  // the models' limit
+    max_m16 = std::max(max_m16, smem / kProfRows / rows * rows);
+  }
   TraceClock tc("plan");
 
   auto& ps = c->ps;
@@ -913,7 +930,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     } else {
       const uint64_t mc = static_cast<uint64_t>(pm.m) * tl;
       cells += mc;
-      if (g16 && pm.fits8) {
+      if (g16 && pm.fits8 && pm.m <= max_m16) {
         route[i] = 1;
       } else {
         route[i] = 2;
@@ -961,11 +978,17 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     uint32_t* v0 = byq.data() + qstart[q];
     uint32_t* v1 = byq.data() + qstart[q + 1];
     std::stable_sort(v0, v1, [&](uint32_t a, uint32_t b) { return tlen[a] > tlen[b]; });
+    thread_local std::vector<uint32_t> tl_desc;
+    tl_desc.resize(v1 - v0);
     uint64_t sum_n = 0;
-    for (uint32_t* it = v0; it != v1; ++it) sum_n += tlen[*it];
+    for (uint32_t* it = v0; it != v1; ++it) {
+      tl_desc[it - v0] = tlen[*it];
+      sum_n += tlen[*it];
+    }
     const uint32_t m = c->profs[q].m;
     const uint32_t mean_n = static_cast<uint32_t>(sum_n / (v1 - v0));
-    const int cls = tuning_refine(&c->tuning, tuning_pick(&c->tuning, m, mean_n), m, mean_n);
+    int cls = tuning_pick_batch(&c->tuning, m, tl_desc.data(), tl_desc.size(), mean_n);
+    if (cls < 0) cls = tuning_pick_single(&c->tuning, m, mean_n);  // no class has a rate: the wavefront model
     const uint32_t rows = kClasses[cls].G * kClasses[cls].R;
     const uint32_t P = (m + rows - 1) / rows;
     if (static_cast<uint64_t>(kProfRows) * P * rows > static_cast<uint64_t>(g_class_smem[cls])) {
@@ -995,7 +1018,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   struct QEmit {
     uint32_t n_wt, n_cta;
     size_t wt_off, slot_off, cta_off;
-    uint64_t cost;
+    uint64_t cost, streamed;
   };
   std::vector<QEmit> qe(qlist.size());
   constexpr uint32_t kMaxWtPerCta = 64;
@@ -1017,7 +1040,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   // columns of warp task w of query k: its first pair has the longest target
   auto wt_cols = [&](int64_t k, const QShape& sh, uint32_t w) {
     const uint32_t* v = byq.data() + qstart[qlist[k]];
-    return std::max<uint32_t>(sh.min_cols, static_cast<uint32_t>(up16(tlen[v[static_cast<size_t>(w) * sh.S]])));
+    return std::max<uint32_t>(sh.min_cols, static_cast<uint32_t>(up4(tlen[v[static_cast<size_t>(w) * sh.S]])));
   };
   auto wt_cost = [&](const QShape& sh, uint32_t ncols) {
     return static_cast<uint64_t>(sh.P) * (ncols / sh.C) * sh.step_cost;
@@ -1029,7 +1052,12 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     QEmit& e = qe[k];
     e.n_wt = static_cast<uint32_t>((np + sh.S - 1) / sh.S);
     e.cost = 0;
-    for (uint32_t w = 0; w < e.n_wt; ++w) e.cost += wt_cost(sh, wt_cols(k, sh, w));
+    e.streamed = 0;
+    for (uint32_t w = 0; w < e.n_wt; ++w) {
+      const uint32_t nc = wt_cols(k, sh, w);
+      e.cost += wt_cost(sh, nc);
+      e.streamed += static_cast<uint64_t>(sh.P) * sh.rows * nc * sh.S;
+    }
   }
   std::vector<uint64_t> cap(kNumClasses, 0);
   for (size_t k = 0; k < qlist.size(); ++k) cap[qclass[k]] += qe[k].cost;
@@ -1043,7 +1071,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     for (uint32_t w = 0; w < n_wt; ++w) {
       const uint64_t cw = wt_cost(sh, wt_cols(k, sh, w));
       const uint32_t cnt = w - w0;
-      if (cnt == kMaxWtPerCta || (cnt >= static_cast<uint32_t>(kWarps16) && acc + cw > cp)) {
+      if (cnt == kMaxWtPerCta || (cnt >= static_cast<uint32_t>(kClasses[qclass[k]].W) && acc + cw > cp)) {
         f(w0, w, acc);
         w0 = w;
         acc = 0;
@@ -1071,6 +1099,8 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     n_slot_cls[cls] += static_cast<size_t>(e.n_wt) * S;
     n_cta_cls[cls] += e.n_cta;
     cps[cls].cells += static_cast<uint64_t>(c->profs[q].m) * qsum[k];
+    cps[cls].streamed += e.streamed;
+    plan->streamed += e.streamed;
   }
   std::vector<std::vector<uint64_t>> cta_cost(kNumClasses);
   for (int k = 0; k < kNumClasses; ++k) {
@@ -1100,7 +1130,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
           sl.toff16 = static_cast<uint32_t>(c->h_db_off[pt[pi]] / 16);
           sl.tlen16 = static_cast<uint32_t>(up16(tlen[pi]));
           sl.tlen = tlen[pi];
-          ncols = std::max<uint32_t>(ncols, sl.tlen16);
+          ncols = std::max<uint32_t>(ncols, static_cast<uint32_t>(up4(tlen[pi])));
         }
         cp.slots[sb + sidx] = sl;
       }
@@ -1142,7 +1172,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     }
     for (auto& w : cp.wt) max_cols = std::max(max_cols, w.ncols);
     cp.smem = kProfRows * max_mpad;
-    ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(k.fn), kWarps16 * 32, cp.smem,
+    ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(k.fn), k.W * 32, cp.smem,
                           static_cast<uint32_t>(cp.cta.size()), &cp.grid));
     cp.scratch_stride = multi ? max_cols : 0;
   }
@@ -1177,7 +1207,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   const size_t o_cnt = carve((kNumClasses + 2) * 4);
   for (auto& cp : cps) {
     if (cp.cta.empty() || !cp.scratch_stride) continue;
-    const size_t groups = static_cast<size_t>(cp.grid) * kWarps16 * (32 / kClasses[cp.cls].G);
+    const size_t groups = static_cast<size_t>(cp.grid) * kClasses[cp.cls].W * (32 / kClasses[cp.cls].G);
     cp.o_scratch = carve(groups * cp.scratch_stride * sizeof(uint2));
   }
   const size_t o_s32 = carve(plan->scratch32_stride
@@ -1247,6 +1277,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
       kept.smem = cp.smem;
       kept.scratch_stride = cp.scratch_stride;
       kept.cells = cp.cells;
+      kept.streamed = cp.streamed;
       kept.o_cta = cp.o_cta;
       kept.o_wt = cp.o_wt;
       kept.o_slots = cp.o_slots;
@@ -1392,7 +1423,7 @@ extern "C" int st_plan_profile(st_plan* p, uint32_t cap, int32_t* classes, uint6
     ST_CUDA(cudaEventRecord(e0, c->stream));
     if (i + 1 < n) {
       const ClassPlan& cp = p->classes[i];
-      kClasses[cp.cls].fn<<<cp.grid, kWarps16 * 32, cp.smem, c->stream>>>(cp.prm);
+      kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, c->stream>>>(cp.prm);
       classes[i] = cp.cls;
       cells[i] = cp.cells;
     } else {
@@ -1641,11 +1672,11 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
     if (static_cast<size_t>(kProfRows) * P * rows > static_cast<size_t>(g_class_smem[k]))
       return fail(ST_EINVAL, "query of %u rows too long for the shared-memory profile", pm.m);
   }
-  uint32_t ncols = std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)));
+  uint32_t ncols = std::max<uint32_t>(32, static_cast<uint32_t>(up4(n)));
   if (use16 && P > 1) ncols = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(kClasses[k].C * kClasses[k].G)));
   const uint32_t sstride = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(n) + 32));
   // any warp of the CTA may take the task: room for every group of the CTA
-  const size_t scratch_need = static_cast<size_t>(kWarps16) * 8 * sstride * sizeof(uint2);
+  const size_t scratch_need = static_cast<size_t>(kClasses[k].W) * 8 * sstride * sizeof(uint2);
   ST_TRY(c->pin.reserve(total));
   if (c->stage.bytes < total) ST_TRY(dev_alloc(&c->mt, c->stage, total * 2));
   if (c->scratch_small.bytes < scratch_need) ST_TRY(dev_alloc(&c->mt, c->scratch_small, scratch_need * 2));
@@ -1705,7 +1736,7 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
     prm.scratch_stride = sstride;
     prm.open = open;
     prm.ext = ext;
-    kClasses[k].fn<<<1, kWarps16 * 32, kProfRows * P * rows, c->stream>>>(prm);
+    kClasses[k].fn<<<1, kClasses[k].W * 32, kProfRows * P * rows, c->stream>>>(prm);
     ++c->launches;
   }
   // the 32-bit kernel scores the pair only when it is in the list (headroom reached, or not 16-bit eligible)
@@ -1965,75 +1996,107 @@ extern "C" int st_tune_set(st_ctx* c, const int32_t* table) {
   return ST_OK;
 }
 
+// Calibrates the rate of every 16-bit tile class on a sample of the batch:
+// whole queries, spread over the batch, up to max_pairs pairs. The sample is
+// planned with every query forced into one class at a time, timed (one
+// warm-up run, then three), and the class's rate set to the streamed cells
+// per second. The forcing table is restored afterwards.
 extern "C" int st_autotune(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
-                           uint32_t max_pairs_per_bin, uint32_t* bins_tuned) {
+                           uint32_t max_pairs, uint32_t* classes_calibrated) {
   CTX_GUARD(c);
   if (n && !pairs) return fail(ST_EINVAL, "st_autotune: null pairs");
   if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
   ST_TRY(sync_profiles(c));
-  if (bins_tuned) *bins_tuned = 0;
+  if (classes_calibrated) *classes_calibrated = 0;
   if (!gaps16_ok(open, ext)) return ST_OK;  // nothing runs on the 16-bit kernel
-  // pairs of the 16-bit kernel, grouped by query
+  // queries that every class can stage (the models' shared-memory limit)
+  uint32_t max_m = UINT32_MAX;
+  for (int k = 0; k < kNumClasses; ++k) {
+    const uint32_t rows = static_cast<uint32_t>(kClasses[k].G * kClasses[k].R);
+    max_m = std::min(max_m, static_cast<uint32_t>(216 * 1024) / kProfRows / rows * rows);
+  }
   std::vector<std::vector<uint32_t>> byq(c->profs.size());
   for (uint64_t i = 0; i < n; ++i) {
     const st_pair& p = pairs[i];
     if (p.profile >= c->profs.size() || !c->profs[p.profile].live || p.target >= c->n_seqs)
       return fail(ST_EINVAL, "st_autotune: bad pair %llu", static_cast<unsigned long long>(i));
     const ProfileMeta& pm = c->profs[p.profile];
-    if (p.band_radius >= 0 || !pm.fits8 || pm.m == 0 || c->h_db_len[p.target] == 0) continue;
+    if (p.band_radius >= 0 || !pm.fits8 || pm.m == 0 || pm.m > max_m || c->h_db_len[p.target] == 0) continue;
     byq[p.profile].push_back(static_cast<uint32_t>(i));
   }
-  std::vector<std::vector<st_pair>> bins(kTuneMBins * kTuneNBins);
-  for (uint32_t q = 0; q < byq.size(); ++q) {
-    if (byq[q].empty()) continue;
-    uint64_t sum = 0;
-    for (uint32_t i : byq[q]) sum += c->h_db_len[pairs[i].target];
-    const int b = tune_mbin(c->profs[q].m) * kTuneNBins + tune_nbin(static_cast<uint32_t>(sum / byq[q].size()));
-    auto& v = bins[b];
-    if (v.size() >= max_pairs_per_bin) continue;
-    for (uint32_t i : byq[q]) v.push_back(pairs[i]);
-  }
+  std::vector<uint32_t> qs;
+  for (uint32_t q = 0; q < byq.size(); ++q)
+    if (!byq[q].empty()) qs.push_back(q);
+  if (qs.empty()) return ST_OK;
+  // whole queries in a fixed scattered order (a multiplicative hash of the id) until the sample is full
+  std::sort(qs.begin(), qs.end(), [](uint32_t a, uint32_t b) { return a * 2654435761u < b * 2654435761u; });
+  std::vector<st_pair> sample;
+  for (size_t k = 0; k < qs.size() && sample.size() < max_pairs; ++k)
+    for (uint32_t i : byq[qs[k]]) sample.push_back(pairs[i]);
   DevMem out;
+  ST_TRY(dev_alloc(&c->mt, out, sample.size() * 8));
   cudaEvent_t e0, e1;
   ST_CUDA(cudaEventCreate(&e0));
   ST_CUDA(cudaEventCreate(&e1));
-  uint32_t tuned = 0;
-  for (int b = 0; b < kTuneMBins * kTuneNBins; ++b) {
-    auto& v = bins[b];
-    if (v.empty()) continue;
-    if (out.bytes < v.size() * 8) ST_TRY(dev_alloc(&c->mt, out, v.size() * 8));
-    const int mb = b / kTuneNBins, nb = b % kTuneNBins;
-    uint32_t max_m = 0;
-    for (auto& p : v) max_m = std::max(max_m, c->profs[p.profile].m);
-    int best_c = -1;
-    float best_ms = 1e30f;
-    for (int k = 0; k < kNumClasses; ++k) {
-      if (tune_cost(&c->tuning, k, max_m, 64, false) >= 1e300) continue;
-      c->tuning.table[mb][nb] = k;
-      st_plan* p = nullptr;
-      ST_TRY(plan_build(c, v.data(), v.size(), open, ext, out.as<int32_t>(), nullptr, &p, true, c->stream, 0));
-      std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
-      cudaStream_t saved = c->stream;
-      c->stream = c->own;
-      ST_TRY(plan_run(p));  // warm-up
-      ST_CUDA(cudaEventRecord(e0, c->own));
-      const int reps = 3;
-      for (int r = 0; r < reps; ++r) ST_TRY(plan_run(p));
-      ST_CUDA(cudaEventRecord(e1, c->own));
-      ST_CUDA(cudaEventSynchronize(e1));
-      c->stream = saved;
-      float ms = 0;
-      ST_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best_ms) {
-        best_ms = ms;
-        best_c = k;
-      }
+  struct Events {
+    cudaEvent_t a, b;
+    ~Events() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
     }
-    c->tuning.table[mb][nb] = best_c;
-    ++tuned;
+  } evs{e0, e1};
+  Tuning saved = c->tuning;
+  struct Restore {
+    st_ctx* c;
+    Tuning* t;
+    bool armed = true;
+    ~Restore() {
+      if (armed) c->tuning = *t;
+    }
+  } restore{c, &saved};
+  float rates[kMaxTileClasses] = {};
+  uint32_t done = 0;
+  for (int k = 0; k < kNumClasses; ++k) {
+    for (int i = 0; i < kTuneMBins; ++i)
+      for (int j = 0; j < kTuneNBins; ++j) c->tuning.table[i][j] = k;
+    st_plan* p = nullptr;
+    ST_TRY(plan_build(c, sample.data(), sample.size(), open, ext, out.as<int32_t>(), nullptr, &p, true, c->own, 0));
+    std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
+    cudaStream_t prev = c->stream;
+    c->stream = c->own;
+    int rc = plan_run(p);  // warm-up
+    if (rc == ST_OK && cudaEventRecord(e0, c->own) != cudaSuccess) rc = fail(ST_ECUDA, "event record failed");
+    for (int r = 0; r < 3 && rc == ST_OK; ++r) rc = plan_run(p);
+    if (rc == ST_OK && cudaEventRecord(e1, c->own) != cudaSuccess) rc = fail(ST_ECUDA, "event record failed");
+    c->stream = prev;
+    ST_TRY(rc);
+    ST_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    ST_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms > 0 && p->streamed > 0) {
+      rates[k] = static_cast<float>(static_cast<double>(p->streamed) * 3 / (ms * 1e-3) / 1e12);
+      ++done;
+    }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (bins_tuned) *bins_tuned = tuned;
+  for (int k = 0; k < kNumClasses; ++k) saved.rate[k] = rates[k];
+  if (classes_calibrated) *classes_calibrated = done;
+  return ST_OK;
+}
+
+extern "C" int st_tune_get_rates(st_ctx* c, float* rates, uint32_t cap) {
+  CTX_GUARD(c);
+  if (cap && !rates) return fail(ST_EINVAL, "st_tune_get_rates: null output");
+  for (uint32_t k = 0; k < cap && k < static_cast<uint32_t>(kNumClasses); ++k) rates[k] = c->tuning.rate[k];
+  return ST_OK;
+}
+
+extern "C" int st_tune_set_rates(st_ctx* c, const float* rates, uint32_t n) {
+  CTX_GUARD(c);
+  if (n && !rates) return fail(ST_EINVAL, "st_tune_set_rates: null input");
+  if (n > static_cast<uint32_t>(kNumClasses)) return fail(ST_EINVAL, "st_tune_set_rates: %u rates for %d classes", n, kNumClasses);
+  for (uint32_t k = 0; k < n; ++k) {
+    if (!(rates[k] >= 0.0f) || rates[k] > 1e6f) return fail(ST_EINVAL, "st_tune_set_rates: bad rate %g", rates[k]);
+    c->tuning.rate[k] = rates[k];
+  }
   return ST_OK;
 }

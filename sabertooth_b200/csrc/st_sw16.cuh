@@ -53,7 +53,7 @@ struct Sw16CtaTask {
 
 struct Sw16WarpTask {
   uint32_t slot_begin;  // 64/G consecutive slot records, two per group
-  uint32_t ncols;       // columns streamed per pass: multiple of 16, >= 32 (>= C*G with several passes)
+  uint32_t ncols;       // columns streamed per pass: multiple of 4, >= 32 (>= C*G with several passes)
 };
 
 // One target of a warp task: everything lane 0 needs, in one 16-byte load.

@@ -1,18 +1,28 @@
-// Tile-class selection for the packed 16-bit kernel: lanes per alignment (G)
-// and query rows per lane (R) per length bin.  A table filled by the autotuner
-// (st_autotune) takes precedence; empty entries fall back to a cost model of
-// the wavefront: a warp task streams P * ncols + G - 1 steps, each costing
-// about R row-updates plus a fixed per-step overhead, for 64 / G targets.
+// Tile-class selection for the packed 16-bit kernel: lanes per alignment (G),
+// query rows per lane (R) and columns per step (C).
+//
+// Batches: each query takes the class with the least estimated time, its
+// streamed cells (padded rows x padded columns x slots, from its own target
+// lengths) divided by the class's measured rate (streamed cells per second,
+// calibrated by st_autotune; built-in B200 figures by default, 0 = class not
+// considered).  A table entry per (query length, mean target length) bin, set
+// by the caller, forces a class for that bin.
+//
+// Single alignments (the per-call path) use a model of the wavefront: a task
+// streams P * ncols / C + G - 1 steps, each costing about R * C row updates
+// plus a fixed per-step overhead.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 
 constexpr int kTuneMBins = 10;  // query length: <=32, <=64, ..., <=8192, >8192
 constexpr int kTuneNBins = 8;   // mean target length: <=64, <=128, ..., <=4096, >4096
-constexpr int kMaxTileClasses = 16;
+constexpr int kMaxTileClasses = 32;
 
 struct Tuning {
-  int table[kTuneMBins][kTuneNBins];  // class index, -1 = cost model
-  double step_overhead;               // per-step overhead in row-update units
+  int table[kTuneMBins][kTuneNBins];  // class index, -1 = rate model
+  double step_overhead;               // per-step overhead in row-update units (single alignments)
+  float rate[kMaxTileClasses];        // streamed cells per second / 1e12, per class; 0 = not used
 };
 
 int st_tuning_num_classes();
@@ -38,10 +48,70 @@ inline int tune_nbin(uint32_t n) {
   return b;
 }
 
+// Rates measured on B200 (148 SMs, 1965 MHz), streamed cells per second / 1e12,
+// with every query of the PSSM workload (4,000 queries of 50-2,000 rows, 1.2 M
+// pairs, targets of 160 residues on average) forced into one class.
+inline float tuning_default_rate(int G, int R, int C) {
+  if (C != 4) return 0.0f;
+  static const struct {
+    int G, R;
+    float rate;
+  } kRates[] = {
+      {4, 8, 3.545f},   {8, 8, 4.288f},   {16, 8, 4.434f},  {32, 8, 4.345f},  {4, 12, 3.638f},
+      {8, 12, 4.429f},  {16, 12, 4.630f}, {32, 12, 4.448f}, {4, 16, 3.801f},  {8, 16, 4.644f},
+      {16, 16, 4.813f}, {32, 16, 4.650f}, {4, 24, 4.439f},  {8, 24, 5.160f},  {16, 24, 5.247f},
+      {32, 24, 5.030f}, {4, 32, 4.923f},  {8, 32, 5.306f},  {16, 32, 5.244f},
+  };
+  for (const auto& r : kRates)
+    if (r.G == G && r.R == R) return r.rate;
+  return 0.0f;
+}
+
 inline void tuning_defaults(Tuning* t) {
   for (int i = 0; i < kTuneMBins; ++i)
     for (int j = 0; j < kTuneNBins; ++j) t->table[i][j] = -1;
   t->step_overhead = 8.0;
+  for (int c = 0; c < kMaxTileClasses; ++c) t->rate[c] = 0.0f;
+  for (int c = 0; c < st_tuning_num_classes() && c < kMaxTileClasses; ++c) {
+    int G, R, C;
+    st_tuning_class_shape(c, &G, &R, &C);
+    t->rate[c] = tuning_default_rate(G, R, C);
+  }
+}
+
+// Streamed cells of one query (m rows) in class c over its targets' lengths,
+// sorted longest first: warp tasks of 64/G targets stream the longest one's
+// length rounded up to 4 columns (at least C*G columns when the query takes
+// several passes).
+inline double tune_streamed(int c, uint32_t m, const uint32_t* tlen_desc, size_t n) {
+  int G, R, C;
+  st_tuning_class_shape(c, &G, &R, &C);
+  const uint32_t rows = static_cast<uint32_t>(G * R);
+  const uint32_t P = (m + rows - 1) / rows;
+  if (22.0 * P * rows > 216.0 * 1024) return 1e300;  // profile does not fit shared memory
+  const uint32_t S = static_cast<uint32_t>(64 / G);
+  uint32_t minc = 32;
+  if (P > 1) minc = std::max<uint32_t>(minc, (static_cast<uint32_t>(C * G) + 15) & ~15u);
+  double cols = 0;
+  for (size_t w = 0; w < n; w += S) cols += std::max<uint32_t>(minc, (tlen_desc[w] + 3) & ~3u);
+  return cols * S * P * rows;
+}
+
+// The class with the least estimated time for one query of a batch.
+inline int tuning_pick_batch(const Tuning* t, uint32_t m, const uint32_t* tlen_desc, size_t n, uint32_t mean_n) {
+  const int forced = t->table[tune_mbin(m)][tune_nbin(mean_n)];
+  if (forced >= 0 && forced < st_tuning_num_classes() && tune_streamed(forced, m, tlen_desc, n) < 1e300) return forced;
+  int best = -1;
+  double bt = 1e301;
+  for (int c = 0; c < st_tuning_num_classes() && c < kMaxTileClasses; ++c) {
+    if (!(t->rate[c] > 0.0f)) continue;
+    const double v = tune_streamed(c, m, tlen_desc, n) / t->rate[c];
+    if (v < bt) {
+      bt = v;
+      best = c;
+    }
+  }
+  return best;
 }
 
 // Estimated cost of scoring one query (m rows) against targets of mean length n in class c:
@@ -69,32 +139,6 @@ inline int tuning_model_pick(const Tuning* t, uint32_t m, uint32_t n, bool singl
     if (v < bc) {
       bc = v;
       best = c;
-    }
-  }
-  return best;
-}
-
-inline int tuning_pick(const Tuning* t, uint32_t m, uint32_t mean_n) {
-  const int c = t->table[tune_mbin(m)][tune_nbin(mean_n)];
-  if (c >= 0 && c < st_tuning_num_classes() && tune_cost(t, c, m, mean_n, false) < 1e300) return c;
-  return tuning_model_pick(t, m, mean_n, false);
-}
-
-// Within the chosen class's family (same lanes per alignment G and columns per
-// step C), the rows per lane R that best fits this query's length.
-inline int tuning_refine(const Tuning* t, int c, uint32_t m, uint32_t n) {
-  int G0, R0, C0;
-  st_tuning_class_shape(c, &G0, &R0, &C0);
-  int best = c;
-  double bc = tune_cost(t, c, m, n, false);
-  for (int k = 0; k < st_tuning_num_classes(); ++k) {
-    int G, R, C;
-    st_tuning_class_shape(k, &G, &R, &C);
-    if (G != G0 || C != C0 || k == c) continue;
-    const double v = tune_cost(t, k, m, n, false);
-    if (v < bc * 0.97) {  // a clear win only: measured classes keep their edge
-      bc = v;
-      best = k;
     }
   }
   return best;

@@ -53,17 +53,24 @@ def test_autotune_keeps_scores_exact(ctx):
     ctx.upload_db(w.db_residues, w.db_offsets)
     ids = ctx.create_profiles(w.rows)
     pairs = _pairs(ids, w)
-    saved = ctx.tuning_table()
+    saved, saved_rates = ctx.tuning_table(), ctx.tuning_rates()
     try:
-        tuned = ctx.autotune(pairs, GapCosts(44, 4), max_pairs_per_bin=2000)
+        tuned = ctx.autotune(pairs, GapCosts(44, 4), max_pairs=2000)
         assert tuned >= 1
-        table = ctx.tuning_table()
-        assert (table >= 0).sum() >= tuned
+        assert np.array_equal(ctx.tuning_table(), saved)  # the forcing table comes back
+        rates = ctx.tuning_rates()
+        assert (rates > 0).sum() == tuned
         got = ctx.sw_score_pairs(pairs, GapCosts(44, 4))
         want = O.sw_pairs(O.Arena(w.rows, w.targets()), w.pair_q, w.pair_t, 44, 4)
         assert np.array_equal(got, want)
+        # a model with one class left gives the same scores
+        only = np.zeros_like(rates)
+        only[1] = 1.0
+        ctx.set_tuning_rates(only)
+        assert np.array_equal(ctx.sw_score_pairs(pairs, GapCosts(44, 4)), want)
     finally:
         ctx.set_tuning_table(saved)
+        ctx.set_tuning_rates(saved_rates)
         for i in ids:
             ctx.free_profile(i)
 
