@@ -62,6 +62,13 @@ static bool trace_on() {
   }();
   return on;
 }
+// A numeric setting from the environment, or the default.
+static uint64_t env_u64(const char* name, uint64_t dflt) {
+  const char* v = getenv(name);
+  if (!v || !*v) return dflt;
+  return strtoull(v, nullptr, 10);
+}
+
 struct TraceClock {
   const char* what;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -1009,11 +1016,12 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   }
   // Emission. A query's pairs (sorted by target length, longest first) form
   // warp tasks of S = 64/G pairs; consecutive warp tasks form CTA tasks. A CTA
-  // task ends at 64 warp tasks, or (once it holds a warp task for each warp)
-  // when its estimated cost would pass the class's cap: the class's total cost
-  // over kWaves waves of a grid of two CTAs per SM. Small caps keep the
-  // longest CTA task of a long query a small part of the launch, so short
-  // launches (pipelined chunks) end without a long tail.
+  // task ends at 128 warp tasks, or (once it holds a warp task for each warp)
+  // when its estimated cost would pass the class's cap: one CTA's share of the
+  // class's total cost on a grid of two CTAs per SM. The cap keeps a long
+  // query from becoming one CTA task longer than the rest of the launch (the
+  // tail); a looser split would pay the ramp, drain and barrier wait of a CTA
+  // task more often.
   // Passes: warp-task counts and costs, CTA-task counts, offsets, parallel fill.
   struct QEmit {
     uint32_t n_wt, n_cta;
@@ -1021,8 +1029,8 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     uint64_t cost, streamed;
   };
   std::vector<QEmit> qe(qlist.size());
-  constexpr uint32_t kMaxWtPerCta = 64;
-  constexpr uint64_t kWaves = 8;
+  constexpr uint32_t kMaxWtPerCta = 128;
+
   struct QShape {
     uint32_t S, P, rows, min_cols, step_cost, C;
   };
@@ -1061,7 +1069,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   }
   std::vector<uint64_t> cap(kNumClasses, 0);
   for (size_t k = 0; k < qlist.size(); ++k) cap[qclass[k]] += qe[k].cost;
-  for (int k = 0; k < kNumClasses; ++k) cap[k] = std::max<uint64_t>(1, cap[k] / (kWaves * 2 * c->sms));
+  for (int k = 0; k < kNumClasses; ++k) cap[k] = std::max<uint64_t>(1, cap[k] / (2 * c->sms));
   // calls f(w0, w1, cost) for each CTA task of query k, in order
   auto for_each_cta = [&](int64_t k, const QShape& sh, auto&& f) {
     const uint32_t n_wt = qe[k].n_wt;
@@ -1460,17 +1468,11 @@ static bool host_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
-// Pipelining of large batches: pairs per chunk (ST_PIPELINE_PAIRS overrides;
+// Pipelining of large batches: 320K pairs per chunk (ST_PIPELINE_PAIRS overrides;
 // 0 turns pipelining off) and side streams the chunks rotate over
 // (ST_PIPELINE_STREAMS, 1 to 4).
-static uint64_t env_u64(const char* name, uint64_t dflt) {
-  const char* v = getenv(name);
-  if (!v || !*v) return dflt;
-  return strtoull(v, nullptr, 10);
-}
-
 static uint64_t pipeline_chunks(uint64_t n) {
-  const uint64_t chunk = env_u64("ST_PIPELINE_PAIRS", 160 * 1024);
+  const uint64_t chunk = env_u64("ST_PIPELINE_PAIRS", 320 * 1024);
   if (chunk == 0 || n < chunk + chunk / 2) return 1;
   return std::min<uint64_t>(64, (n + chunk - 1) / chunk);
 }

@@ -123,8 +123,9 @@ def _big_batch(seed, n_pairs, n_q=700, n_t=4000):
     return rows, targets, pq, pt
 
 
-def test_pipelined_batch_matches_oracle_and_single_plan(ctx):
+def test_pipelined_batch_matches_oracle_and_single_plan(ctx, monkeypatch):
     import torch
+    monkeypatch.setenv("ST_PIPELINE_PAIRS", "65536")  # seven chunks
     rows, targets, pq, pt = _big_batch(11, 420_000)
     n = len(pq)
     center = np.zeros(n, dtype=np.int32)
@@ -161,8 +162,9 @@ def test_pipelined_batch_matches_oracle_and_single_plan(ctx):
             ctx.free_profile(i)
 
 
-def test_pipelined_batch_error_in_a_late_chunk_leaves_context_usable(ctx):
+def test_pipelined_batch_error_in_a_late_chunk_leaves_context_usable(ctx, monkeypatch):
     from sabertooth_b200._lib import StError
+    monkeypatch.setenv("ST_PIPELINE_PAIRS", "65536")
     rows, targets, pq, pt = _big_batch(12, 400_000)
     ctx.upload_db_list(targets)
     ids = ctx.create_profiles(rows)
