@@ -3,6 +3,8 @@
 // classes, persistent-kernel work lists, CUDA-graph capture) and the plain
 // per-call paths that replace the reference's QueryProfile::sw_score_with and
 // ungapped::score_batch.
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -276,7 +278,8 @@ struct st_ctx {
     std::vector<uint32_t> pq, pt, tlen, byq, list32;
     std::vector<int32_t> pc, pr;
     std::vector<uint8_t> route;
-    std::vector<uint64_t> qstart;
+    std::vector<uint64_t> qstart, n32;
+    std::vector<uint32_t> hist;  // per-thread query histograms of the grouping
     std::vector<Sw16Slot> slots[32];
     std::vector<Sw16WarpTask> wt[32];
     std::vector<Sw16CtaTask> cta[32];
@@ -955,23 +958,59 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   plan->cells = cells;
   plan->cells32 = cells32;
   tc.lap("classify");
-  // 32-bit list in pair order; 16-bit pairs grouped by query (counting sort)
+  // 32-bit list in pair order; 16-bit pairs grouped by query, in pair order
+  // within a query: a counting sort with one histogram per thread over
+  // contiguous ranges of pairs, so the result is the serial one.
   std::vector<uint32_t>& list32 = ps.list32;
-  list32.clear();
   std::vector<uint64_t>& qstart = ps.qstart;
   qstart.assign(static_cast<size_t>(n_prof) + 1, 0);
-  for (uint64_t i = 0; i < n; ++i) {
-    if (route[i] == 2) list32.push_back(static_cast<uint32_t>(i));
-    else if (route[i] == 1) ++qstart[pq[i] + 1];
+  const int nt = std::max(1, std::min(omp_get_max_threads(), static_cast<int>((n + 32767) / 32768)));
+  ps.hist.assign(static_cast<size_t>(nt) * n_prof, 0);
+  ps.n32.assign(static_cast<size_t>(nt) + 1, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num();
+    const uint64_t i0 = n * t / nt, i1 = n * (t + 1) / nt;
+    uint32_t* h = ps.hist.data() + static_cast<size_t>(t) * n_prof;
+    uint64_t k32 = 0;
+    for (uint64_t i = i0; i < i1; ++i) {
+      if (route[i] == 1) ++h[pq[i]];
+      else if (route[i] == 2) ++k32;
+    }
+    ps.n32[t + 1] = k32;
   }
-  for (uint32_t q = 0; q < n_prof; ++q) qstart[q + 1] += qstart[q];
+  // per query: start of the query, then each thread's start inside it
+  for (uint32_t q = 0; q < n_prof; ++q) {
+    uint64_t sum = 0;
+    for (int t = 0; t < nt; ++t) sum += ps.hist[static_cast<size_t>(t) * n_prof + q];
+    qstart[q + 1] = qstart[q] + sum;
+  }
+  for (int t = 0; t < nt; ++t) ps.n32[t + 1] += ps.n32[t];
+  list32.resize(ps.n32[nt]);
   std::vector<uint32_t>& byq = ps.byq;
   byq.resize(qstart[n_prof]);
-  {
-    std::vector<uint64_t> fill(qstart.begin(), qstart.end() - 1);
-    for (uint64_t i = 0; i < n; ++i)
-      if (route[i] == 1) byq[fill[pq[i]]++] = static_cast<uint32_t>(i);
+#pragma omp parallel for schedule(static)
+  for (int64_t q = 0; q < static_cast<int64_t>(n_prof); ++q) {
+    uint64_t o = qstart[q];
+    for (int t = 0; t < nt; ++t) {
+      uint32_t& h = ps.hist[static_cast<size_t>(t) * n_prof + q];
+      const uint32_t cnt = h;
+      h = static_cast<uint32_t>(o - qstart[q]);  // becomes the thread's offset inside the query
+      o += cnt;
+    }
   }
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num();
+    const uint64_t i0 = n * t / nt, i1 = n * (t + 1) / nt;
+    uint32_t* h = ps.hist.data() + static_cast<size_t>(t) * n_prof;
+    uint64_t k32 = ps.n32[t];
+    for (uint64_t i = i0; i < i1; ++i) {
+      if (route[i] == 1) byq[qstart[pq[i]] + h[pq[i]]++] = static_cast<uint32_t>(i);
+      else if (route[i] == 2) list32[k32++] = static_cast<uint32_t>(i);
+    }
+  }
+  tc.lap("group");
   // per query (in parallel): targets longest first, then the tile class
   std::vector<uint32_t> qlist;
   for (uint32_t q = 0; q < n_prof; ++q)
@@ -1006,7 +1045,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     qsum[k] = sum_n;
   }
   if (toolong >= 0) return fail(ST_EINVAL, "query of %d rows does not fit the shared-memory profile", toolong);
-  tc.lap("group+sort");
+  tc.lap("sort+pick");
   std::vector<ClassPlan> cps(kNumClasses);
   for (int k = 0; k < kNumClasses; ++k) {
     cps[k].cls = k;
@@ -1468,13 +1507,25 @@ static bool host_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
-// Pipelining of large batches: 320K pairs per chunk (ST_PIPELINE_PAIRS overrides;
-// 0 turns pipelining off) and side streams the chunks rotate over
-// (ST_PIPELINE_STREAMS, 1 to 4).
-static uint64_t pipeline_chunks(uint64_t n) {
+// Pipelining of large batches: chunks of about 320K pairs (ST_PIPELINE_PAIRS
+// overrides; 0 turns pipelining off), the first two a quarter and a half of
+// that so the GPU starts early, rotating over side streams
+// (ST_PIPELINE_STREAMS, 1 to 4). Returns the chunk boundaries (one chunk: no
+// pipelining).
+static std::vector<uint64_t> pipeline_bounds(uint64_t n) {
   const uint64_t chunk = env_u64("ST_PIPELINE_PAIRS", 320 * 1024);
-  if (chunk == 0 || n < chunk + chunk / 2) return 1;
-  return std::min<uint64_t>(64, (n + chunk - 1) / chunk);
+  std::vector<uint64_t> b{0};
+  if (chunk == 0 || n < chunk + chunk / 2) {
+    b.push_back(n);
+    return b;
+  }
+  const uint64_t first[2] = {std::max<uint64_t>(1, chunk / 4), std::max<uint64_t>(1, chunk / 2)};
+  uint64_t at = 0;
+  for (int k = 0; k < 2 && n - at > chunk + chunk / 2; ++k) b.push_back(at += first[k]);
+  const uint64_t rest = n - at;
+  const uint64_t m = std::min<uint64_t>(62, std::max<uint64_t>(1, (rest + chunk / 2) / chunk));
+  for (uint64_t k = 1; k <= m; ++k) b.push_back(at + rest * k / m);
+  return b;
 }
 
 static int pipeline_streams() {
@@ -1516,7 +1567,8 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
       if (kernels) memcpy(kernels + a0, h_kern + a0, (a1 - a0) * 4);
     }
   };
-  const uint64_t chunks = pipeline_chunks(n);
+  const std::vector<uint64_t> bounds = pipeline_bounds(n);
+  const uint64_t chunks = bounds.size() - 1;
   if (chunks <= 1) {
     st_plan* p = nullptr;
     ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p, false, c->stream, 0));
@@ -1579,7 +1631,7 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
   {
     Drain drain{c};
     for (uint64_t k = 0; k < chunks && rc == ST_OK; ++k) {
-      const uint64_t b = n * k / chunks, e = n * (k + 1) / chunks;
+      const uint64_t b = bounds[k], e = bounds[k + 1];
       cudaStream_t s = c->side[k % n_side];
       st_plan* p = nullptr;
       rc = plan_build(c, pairs + b, e - b, open, ext, d_scores + b, d_kern + b, &p, false, s,
