@@ -22,6 +22,10 @@
 #include "st_sw32.cuh"
 #include "st_tuning.h"
 #include "st_ungapped.cuh"
+#include "st_dplan.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 using namespace st;
 
@@ -1532,6 +1536,310 @@ static int pipeline_streams() {
   return static_cast<int>(std::min<uint64_t>(st_ctx::kMaxSide, std::max<uint64_t>(1, env_u64("ST_PIPELINE_STREAMS", 4))));
 }
 
+// Checks every pair (profile id live, target in the database) in parallel;
+// reports the first bad one. Also the longest target and query of the batch
+// (the 32-bit kernel's scratch).
+static int validate_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, uint32_t* max_len, uint32_t* max_m) {
+  const uint32_t n_prof = static_cast<uint32_t>(c->profs.size());
+  int64_t bad = INT64_MAX;
+  uint32_t ml = 0, mm = 0;
+#pragma omp parallel for schedule(static) reduction(min : bad) reduction(max : ml, mm)
+  for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+    const st_pair& p = pairs[i];
+    if (p.profile >= n_prof || !c->profs[p.profile].live || p.target >= c->n_seqs) {
+      bad = std::min<int64_t>(bad, i);
+      continue;
+    }
+    const uint32_t tl = c->h_db_len[p.target];
+    const uint32_t m = c->profs[p.profile].m;
+    if (tl && m) {
+      ml = std::max(ml, tl);
+      mm = std::max(mm, m);
+    }
+  }
+  if (bad != INT64_MAX) {
+    const st_pair& p = pairs[bad];
+    if (p.profile >= n_prof || !c->profs[p.profile].live)
+      return fail(ST_EINVAL, "pair %lld: unknown profile id %u", static_cast<long long>(bad), p.profile);
+    return fail(ST_EINVAL, "pair %lld: target %u outside the database (%u sequences)", static_cast<long long>(bad),
+                p.target, c->n_seqs);
+  }
+  if (max_len) *max_len = ml;
+  if (max_m) *max_m = mm;
+  return ST_OK;
+}
+
+static int bits_for(uint64_t x) {
+  int b = 0;
+  while (x) {
+    ++b;
+    x >>= 1;
+  }
+  return std::max(b, 1);
+}
+
+// Builds the plan of pairs[0..n) on the device (st_dplan.cuh), on the
+// context's stream, with one synchronisation to read the per-class totals
+// that size the rest. `work` holds the per-pair and per-query buffers and
+// must outlive the plan's runs; the plan owns the task arrays and scratch.
+static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* d_scores,
+                       uint32_t* d_kernels, uint32_t max_len, uint32_t max_m, DevMem& work, st_plan** out) {
+  cudaStream_t st = c->stream;
+  TraceClock tc("dplan");
+  const uint32_t n_prof = static_cast<uint32_t>(c->profs.size());
+  const bool g16 = gaps16_ok(open, ext);
+  auto plan = std::make_unique<st_plan>();
+  plan->ctx = c;
+  plan->n = n;
+  plan->open = open;
+  plan->ext = ext;
+  plan->d_scores = d_scores;
+  plan->d_kernels = d_kernels;
+
+  DpClasses cls{};
+  cls.n = kNumClasses;
+  cls.sms = static_cast<uint32_t>(c->sms);
+  uint32_t max_m16 = 0;
+  for (int k = 0; k < kNumClasses; ++k) {
+    DpClass& d = cls.c[k];
+    d.G = kClasses[k].G;
+    d.R = kClasses[k].R;
+    d.C = kClasses[k].C;
+    d.W = kClasses[k].W;
+    d.rows = d.G * d.R;
+    d.S = 64 / d.G;
+    const uint32_t smem = static_cast<uint32_t>(std::min<int>(g_class_smem[k], 216 * 1024));
+    d.max_mpad = smem / kProfRows / d.rows * d.rows;
+    d.rate = c->tuning.rate[k];
+    max_m16 = std::max(max_m16, d.max_mpad);
+  }
+  memcpy(cls.table, c->tuning.table, sizeof(cls.table));
+
+  DpIn in{};
+  in.n = static_cast<uint32_t>(n);
+  in.db = db_view(c);
+  in.prof = prof_view(c);
+  in.n_prof = n_prof;
+  in.max_m16 = max_m16;
+  in.g16 = g16 ? 1u : 0u;
+  in.tbits = static_cast<uint32_t>(bits_for(max_len));
+  const int key_bits = std::min(64, bits_for(n_prof) + static_cast<int>(in.tbits));
+
+  // scratch sizes of the library sorts and scans (host-side queries)
+  using ull = unsigned long long;
+  size_t t_sort = 0, t_qsort = 0, t_scan = 0;
+  {
+    cub::DoubleBuffer<ull> kb(nullptr, nullptr);
+    cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, kb, vb, static_cast<int>(n), 0, key_bits, st));
+    cub::DoubleBuffer<uint32_t> qk(nullptr, nullptr), qv(nullptr, nullptr);
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t_qsort, qk, qv, static_cast<int>(n_prof), 0, 6, st));
+    ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t_scan, static_cast<uint32_t*>(nullptr),
+                                          static_cast<uint32_t*>(nullptr), static_cast<int>(n_prof + 1), st));
+  }
+  const size_t t_tmp = std::max(t_sort, std::max(t_qsort, t_scan));
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~static_cast<size_t>(255);
+    return o;
+  };
+  const size_t np1 = static_cast<size_t>(n_prof) + 1;
+  const size_t o_pairs = carve(n * 16), o_pq = carve(n * 4), o_pt = carve(n * 4), o_pc = carve(n * 4),
+               o_pr = carve(n * 4), o_k0 = carve(n * 8), o_k1 = carve(n * 8), o_v0 = carve(n * 4),
+               o_v1 = carve(n * 4), o_list = carve(n * 4), o_cnt = carve((kNumClasses + 2) * 4),
+               o_cinit = carve((kNumClasses + 2) * 4), o_qcnt = carve(np1 * 4), o_qstart = carve(np1 * 4),
+               o_qclass = carve(np1 * 4), o_nwt = carve(np1 * 4), o_ncta = carve(np1 * 4), o_qk0 = carve(np1 * 4),
+               o_qk1 = carve(np1 * 4), o_qi0 = carve(np1 * 4), o_qi1 = carve(np1 * 4), o_as = carve(np1 * 4),
+               o_aw = carve(np1 * 4), o_ac = carve(np1 * 4), o_os = carve(np1 * 4), o_ow = carve(np1 * 4),
+               o_oc = carve(np1 * 4), o_tot = carve(sizeof(DpTotals)), o_tmp = carve(t_tmp);
+  ST_TRY(pool_get(c, off, work));
+  char* b = work.as<char>();
+  DpWork w{};
+  w.pq = reinterpret_cast<uint32_t*>(b + o_pq);
+  w.pt = reinterpret_cast<uint32_t*>(b + o_pt);
+  w.pc = reinterpret_cast<int32_t*>(b + o_pc);
+  w.pr = reinterpret_cast<int32_t*>(b + o_pr);
+  w.keys = reinterpret_cast<ull*>(b + o_k0);
+  w.keys_alt = reinterpret_cast<ull*>(b + o_k1);
+  w.vals = reinterpret_cast<uint32_t*>(b + o_v0);
+  w.vals_alt = reinterpret_cast<uint32_t*>(b + o_v1);
+  w.list32 = reinterpret_cast<uint32_t*>(b + o_list);
+  uint32_t* counters = reinterpret_cast<uint32_t*>(b + o_cnt);
+  uint32_t* cinit = reinterpret_cast<uint32_t*>(b + o_cinit);
+  w.list_count = cinit + kNumClasses + 1;  // the static 32-bit list count is the runs' initial list count
+  w.qcnt = reinterpret_cast<uint32_t*>(b + o_qcnt);
+  w.qstart = reinterpret_cast<uint32_t*>(b + o_qstart);
+  w.qclass = reinterpret_cast<uint32_t*>(b + o_qclass);
+  w.nwt = reinterpret_cast<uint32_t*>(b + o_nwt);
+  w.ncta = reinterpret_cast<uint32_t*>(b + o_ncta);
+  w.qkey = reinterpret_cast<uint32_t*>(b + o_qk0);
+  w.qkey_alt = reinterpret_cast<uint32_t*>(b + o_qk1);
+  w.qid = reinterpret_cast<uint32_t*>(b + o_qi0);
+  w.qid_alt = reinterpret_cast<uint32_t*>(b + o_qi1);
+  w.a_slots = reinterpret_cast<uint32_t*>(b + o_as);
+  w.a_wt = reinterpret_cast<uint32_t*>(b + o_aw);
+  w.a_cta = reinterpret_cast<uint32_t*>(b + o_ac);
+  w.o_slots = reinterpret_cast<uint32_t*>(b + o_os);
+  w.o_wt = reinterpret_cast<uint32_t*>(b + o_ow);
+  w.o_cta = reinterpret_cast<uint32_t*>(b + o_oc);
+  w.totals = reinterpret_cast<DpTotals*>(b + o_tot);
+  void* tmp = b + o_tmp;
+  in.pairs = reinterpret_cast<const st_pair*>(b + o_pairs);
+
+  // stage 1: pairs in, classify, sort, per-query class and CTA-task counts, class order
+  ST_CUDA(cudaMemcpyAsync(b + o_pairs, pairs, n * 16, cudaMemcpyHostToDevice, st));
+  ST_CUDA(cudaMemsetAsync(cinit, 0, (kNumClasses + 2) * 4, st));
+  ST_CUDA(cudaMemsetAsync(w.qcnt, 0, np1 * 4, st));
+  ST_CUDA(cudaMemsetAsync(w.totals, 0, sizeof(DpTotals), st));
+  const uint32_t gb = static_cast<uint32_t>(std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(c->sms) * 8));
+  dp_classify_kernel<<<gb, 256, 0, st>>>(in, w);
+  cub::DoubleBuffer<ull> kb(w.keys, w.keys_alt);
+  cub::DoubleBuffer<uint32_t> vb(w.vals, w.vals_alt);
+  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_sort, kb, vb, static_cast<int>(n), 0, key_bits, st));
+  w.vals_sorted = vb.Current();
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.qcnt, w.qstart, static_cast<int>(np1), st));
+  const uint32_t gq32 = static_cast<uint32_t>((static_cast<uint64_t>(n_prof) * 32 + 255) / 256);
+  const uint32_t gq = static_cast<uint32_t>((np1 + 255) / 256);
+  dp_pick_kernel<<<gq32, 256, 0, st>>>(in, w, cls);
+  dp_split_kernel<<<gq, 256, 0, st>>>(in, w, cls);
+  cub::DoubleBuffer<uint32_t> qk(w.qkey, w.qkey_alt), qi(w.qid, w.qid_alt);
+  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_qsort, qk, qi, static_cast<int>(n_prof), 0, 6, st));
+  w.qid_sorted = qi.Current();
+  dp_counts_kernel<<<gq, 256, 0, st>>>(in, w, cls);
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_slots, w.o_slots, static_cast<int>(np1), st));
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_wt, w.o_wt, static_cast<int>(np1), st));
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_cta, w.o_cta, static_cast<int>(np1), st));
+  ST_CUDA(cudaGetLastError());
+  c->launches += 5;
+  DpTotals tot;
+  ST_CUDA(cudaMemcpyAsync(&tot, w.totals, sizeof(DpTotals), cudaMemcpyDeviceToHost, st));
+  ST_CUDA(cudaStreamSynchronize(st));
+  tc.lap("stage 1 (device)");
+
+  // stage 2: sizes known; task arrays, scratch, emission, LPT order
+  uint64_t n_slots = 0, n_wt = 0, n_cta = 0;
+  uint64_t cta_begin[kNumClasses];
+  uint32_t zcols = 64;
+  for (int k = 0; k < kNumClasses; ++k) {
+    cta_begin[k] = n_cta;
+    n_slots += static_cast<uint64_t>(tot.n_wt[k]) * (64 / kClasses[k].G);
+    n_wt += tot.n_wt[k];
+    n_cta += tot.n_cta[k];
+    if (tot.n_cta[k]) zcols = std::max(zcols, tot.max_cols[k] + 8);
+  }
+  for (int k = 0; k < kNumClasses; ++k) {
+    if (!tot.n_cta[k]) continue;
+    ClassPlan cp;
+    cp.cls = k;
+    cp.cells = tot.cost[k];  // the fork puts the costliest class on the launching stream
+    cp.smem = kProfRows * tot.max_mpad[k];
+    ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(kClasses[k].fn), kClasses[k].W * 32, cp.smem,
+                          tot.n_cta[k], &cp.grid));
+    cp.scratch_stride = tot.max_cols_multi[k];
+    plan->classes.push_back(std::move(cp));
+  }
+  ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0, 2 * c->sms,
+                        &plan->grid32));
+  plan->grid32 = std::min<uint32_t>(plan->grid32, 2 * c->sms);
+  plan->scratch32_stride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
+  size_t t_lpt = 0;
+  {
+    cub::DoubleBuffer<ull> ck(nullptr, nullptr);
+    cub::DoubleBuffer<uint32_t> ci(nullptr, nullptr);
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t_lpt, ck, ci, static_cast<int>(n_cta), 0, 44 + 6, st));
+  }
+  off = 0;
+  const size_t p_slots = carve(n_slots * sizeof(Sw16Slot)), p_wt = carve(n_wt * sizeof(Sw16WarpTask)),
+               p_craw = carve(n_cta * sizeof(Sw16CtaTask)), p_cta = carve(n_cta * sizeof(Sw16CtaTask)),
+               p_ck0 = carve(n_cta * 8), p_ck1 = carve(n_cta * 8), p_ci0 = carve(n_cta * 4),
+               p_ci1 = carve(n_cta * 4), p_z = carve(static_cast<size_t>(zcols) * sizeof(uint2)),
+               p_tmp = carve(t_lpt);
+  for (auto& cp : plan->classes) {
+    if (!cp.scratch_stride) continue;
+    const size_t groups = static_cast<size_t>(cp.grid) * kClasses[cp.cls].W * (32 / kClasses[cp.cls].G);
+    cp.o_scratch = carve(groups * cp.scratch_stride * sizeof(uint2));
+  }
+  const size_t p_s32 = carve(plan->scratch32_stride ? static_cast<size_t>(plan->grid32) * kWarps32 *
+                                                          plan->scratch32_stride * sizeof(int2)
+                                                    : 16);
+  ST_TRY(pool_get(c, off, plan->arena));
+  char* a = plan->arena.as<char>();
+  DpOut o{};
+  o.slots = reinterpret_cast<Sw16Slot*>(a + p_slots);
+  o.wt = reinterpret_cast<Sw16WarpTask*>(a + p_wt);
+  o.cta_raw = reinterpret_cast<Sw16CtaTask*>(a + p_craw);
+  o.cta = reinterpret_cast<Sw16CtaTask*>(a + p_cta);
+  o.cta_key = reinterpret_cast<ull*>(a + p_ck0);
+  o.cta_key_alt = reinterpret_cast<ull*>(a + p_ck1);
+  o.cta_idx = reinterpret_cast<uint32_t*>(a + p_ci0);
+  o.cta_idx_alt = reinterpret_cast<uint32_t*>(a + p_ci1);
+  o.n_cta = static_cast<uint32_t>(n_cta);
+  if (n_prof) dp_emit_kernel<<<gq32, 256, 0, st>>>(in, w, cls, o);
+  if (n_cta) {
+    cub::DoubleBuffer<ull> ck(o.cta_key, o.cta_key_alt);
+    cub::DoubleBuffer<uint32_t> ci(o.cta_idx, o.cta_idx_alt);
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(a + p_tmp, t_lpt, ck, ci, static_cast<int>(n_cta), 0, 44 + 6, st));
+    o.cta_idx_sorted = ci.Current();
+    dp_gather_cta_kernel<<<static_cast<uint32_t>((n_cta + 255) / 256), 256, 0, st>>>(o);
+  }
+  uint2* zline = reinterpret_cast<uint2*>(a + p_z);
+  dp_fill_zline_kernel<<<(zcols + 255) / 256, 256, 0, st>>>(zline, zcols, pk_splat(-open));
+  ST_CUDA(cudaGetLastError());
+  c->launches += 3;
+
+  plan->counters = counters;
+  plan->counters_init = cinit;
+  const DeviceDb db = db_view(c);
+  const DeviceProfiles pv = prof_view(c);
+  for (auto& cp : plan->classes) {
+    Sw16Params& prm = cp.prm;
+    prm.arena = db.arena;
+    prm.prof = pv;
+    prm.cta_tasks = o.cta + cta_begin[cp.cls];
+    prm.n_cta_tasks = tot.n_cta[cp.cls];
+    prm.warp_tasks = o.wt;
+    prm.slots = o.slots;
+    prm.scores = d_scores;
+    prm.kernels = d_kernels;
+    prm.ovf_count = counters + kNumClasses + 1;
+    prm.ovf_pairs = w.list32;
+    prm.work_counter = counters + cp.cls;
+    prm.scratch = reinterpret_cast<uint2*>(a + cp.o_scratch);
+    prm.zline = zline;
+    prm.scratch_stride = cp.scratch_stride;
+    prm.open = open;
+    prm.ext = ext;
+  }
+  Sw32Params& p32 = plan->p32;
+  p32.db = db;
+  p32.prof = pv;
+  p32.list = w.list32;
+  p32.list_count = counters + kNumClasses + 1;
+  p32.pair_query = w.pq;
+  p32.pair_target = w.pt;
+  p32.pair_center = w.pc;
+  p32.pair_radius = w.pr;
+  p32.scores = d_scores;
+  p32.kernels = d_kernels;
+  p32.work_counter = counters + kNumClasses;
+  p32.scratch = reinterpret_cast<int2*>(a + p_s32);
+  p32.scratch_stride = plan->scratch32_stride;
+  p32.open = open;
+  p32.ext = ext;
+  plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1;
+  tc.lap("stage 2 (enqueue)");
+  *out = plan.release();
+  return ST_OK;
+}
+
+// Batches of at least this many pairs are planned on the device
+// (ST_DEVICE_PLAN=0 keeps the host planner for every size).
+static bool use_device_plan(uint64_t n) {
+  if (!env_u64("ST_DEVICE_PLAN", 1)) return false;
+  return n >= env_u64("ST_DEVICE_PLAN_MIN", 16384);
+}
+
 extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
                                  int32_t* scores, uint32_t* kernels) {
   CTX_GUARD(c);
@@ -1567,6 +1875,32 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
       if (kernels) memcpy(kernels + a0, h_kern + a0, (a1 - a0) * 4);
     }
   };
+  if (use_device_plan(n)) {
+    uint32_t max_len = 0, max_m = 0;
+    ST_TRY(validate_pairs(c, pairs, n, &max_len, &max_m));
+    ST_TRY(sync_profiles(c));
+    tc.lap("validate");
+    DevMem work;
+    st_plan* p = nullptr;
+    const int rc = dplan_build(c, pairs, n, open, ext, d_scores, d_kern, max_len, max_m, work, &p);
+    std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
+    struct Drain {  // the stream finishes before the work buffers go back to the pool
+      st_ctx* c;
+      DevMem* m;
+      ~Drain() {
+        cudaStreamSynchronize(c->stream);
+        pool_put(c, std::move(*m));
+      }
+    } drain{c, &work};
+    ST_TRY(rc);
+    ST_TRY(plan_run(p));
+    ST_CUDA(cudaMemcpyAsync(h_scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (kernels) ST_CUDA(cudaMemcpyAsync(h_kern, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    copy_out();
+    tc.lap("run+download");
+    return ST_OK;
+  }
   const std::vector<uint64_t> bounds = pipeline_bounds(n);
   const uint64_t chunks = bounds.size() - 1;
   if (chunks <= 1) {

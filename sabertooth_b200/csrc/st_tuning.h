@@ -101,14 +101,17 @@ inline double tune_streamed(int c, uint32_t m, const uint32_t* tlen_desc, size_t
 inline int tuning_pick_batch(const Tuning* t, uint32_t m, const uint32_t* tlen_desc, size_t n, uint32_t mean_n) {
   const int forced = t->table[tune_mbin(m)][tune_nbin(mean_n)];
   if (forced >= 0 && forced < st_tuning_num_classes() && tune_streamed(forced, m, tlen_desc, n) < 1e300) return forced;
+  // classes with a rate first; if none of them stages this query, least streamed cells over all
   int best = -1;
-  double bt = 1e301;
-  for (int c = 0; c < st_tuning_num_classes() && c < kMaxTileClasses; ++c) {
-    if (!(t->rate[c] > 0.0f)) continue;
-    const double v = tune_streamed(c, m, tlen_desc, n) / t->rate[c];
-    if (v < bt) {
-      bt = v;
-      best = c;
+  for (int pass = 0; pass < 2 && best < 0; ++pass) {
+    double bt = 1e299;
+    for (int c = 0; c < st_tuning_num_classes() && c < kMaxTileClasses; ++c) {
+      if (pass == 0 && !(t->rate[c] > 0.0f)) continue;
+      const double v = tune_streamed(c, m, tlen_desc, n) / (pass == 0 ? t->rate[c] : 1.0f);
+      if (v < bt) {
+        bt = v;
+        best = c;
+      }
     }
   }
   return best;

@@ -35,3 +35,15 @@ def ctx():
     c = Context(0)
     yield c
     c.close()
+
+
+@pytest.fixture(params=["host", "device"])
+def planner(request, monkeypatch):
+    """Runs a batched-scoring test once with the host planner and once with the
+    device planner (every batch size planned on the GPU)."""
+    if request.param == "host":
+        monkeypatch.setenv("ST_DEVICE_PLAN", "0")
+    else:
+        monkeypatch.setenv("ST_DEVICE_PLAN", "1")
+        monkeypatch.setenv("ST_DEVICE_PLAN_MIN", "1")
+    return request.param

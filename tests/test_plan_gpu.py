@@ -7,7 +7,7 @@ from sabertooth_b200 import GapCosts
 from sabertooth_b200 import workloads as W
 from sabertooth_b200._lib import PAIR_DTYPE
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("planner")]
 
 
 def _pairs(ids, w):

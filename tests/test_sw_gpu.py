@@ -15,7 +15,7 @@ from sabertooth_b200 import GapCosts, Kernel, QueryProfile, blosum62, encode, ti
 from sabertooth_b200 import workloads as W
 from tests.refrng import XorShift, rand_seq
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("planner")]
 
 GAP_SWEEP = [(1, 1), (2, 1), (3, 1), (2, 0), (4, 1), (11, 1), (6, 2), (5, 5)]
 
