@@ -74,7 +74,9 @@ int st_profile_free(st_ctx* ctx, uint32_t id);
  * before it freed. A freed id may be handed out again by a later create. */
 int st_profiles_free(st_ctx* ctx, const uint32_t* ids, uint32_t n);
 /* Batch form: n_profiles profiles from one rows arena; row_offsets[k]..row_offsets[k+1]
- * are the rows of profile k; ids written to ids[0..n_profiles). */
+ * are the rows of profile k; ids written to ids[0..n_profiles).  Returns once
+ * the rows are on the device (they may be reused); the device layouts are built
+ * on the context's stream, before any later work that uses them. */
 int st_profiles_create(st_ctx* ctx, const int32_t* rows, const uint64_t* row_offsets, uint32_t n_profiles,
                        uint32_t* ids);
 
@@ -97,11 +99,24 @@ typedef struct {
 } st_pair;
 
 /* Batched scoring of many (profile, database target) pairs with host buffers:
- * copies pairs in and scores out, plans (length bins + autotuned tiles), runs
- * the persistent kernels and waits.  Replaces the per-candidate loop
- * Engine::search_query::score_one (src/search.rs:534-577).  kernels may be NULL. */
+ * copies pairs in and scores out, plans (a tile class per query; on the GPU
+ * for large batches), runs the persistent kernels and waits.  Replaces the
+ * per-candidate loop Engine::search_query::score_one (src/search.rs:534-577).
+ * kernels may be NULL. */
 int st_sw_score_pairs(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* scores,
                       uint32_t* kernels);
+
+/* The same in two halves, so that a caller can prepare the next batch (build
+ * its profiles, fill its pairs) while this one runs on the GPU.
+ * st_sw_score_pairs_async validates, uploads, plans and launches, then returns;
+ * pairs may be reused at once, scores/kernels must stay valid (and unread)
+ * until st_batch_wait, which waits, writes them and releases the batch.  Errors
+ * in the arguments are reported by the first call; every batch must be waited
+ * for.  (No reference counterpart: the reference scores candidates inline.) */
+typedef struct st_batch st_batch;
+int st_sw_score_pairs_async(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                            int32_t* scores, uint32_t* kernels, st_batch** batch);
+int st_batch_wait(st_batch* batch);
 
 /* Planned form over device buffers: a plan binds a pair list (copied at plan
  * time), gap costs and device output buffers; st_plan_run replays the captured

@@ -56,6 +56,8 @@ SIGNATURES = {
     "st_profile_create": (C.c_int, [_P, _P, _u32, _P]),
     "st_profile_free": (C.c_int, [_P, _u32]),
     "st_profiles_free": (C.c_int, [_P, _P, _u32]),
+    "st_sw_score_pairs_async": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P, _P]),
+    "st_batch_wait": (C.c_int, [_P]),
     "st_profiles_create": (C.c_int, [_P, _P, _P, _u32, _P]),
     "st_sw_score": (C.c_int, [_P, _u32, _P, _u32, _i32, _i32, _P, _P]),
     "st_sw_score_pairs": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P]),

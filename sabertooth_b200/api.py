@@ -158,6 +158,21 @@ class Context:
                                         ptr(kernels)))
         return (scores, kernels) if with_kernels else scores
 
+    def sw_score_pairs_async(self, pairs, gaps: GapCosts, scores=None, kernels=None, with_kernels=False):
+        """Starts scoring `pairs` and returns a Batch at once; Batch.wait() returns the scores
+        (and kernel tags). `scores` / `kernels` may be given (for instance pinned arrays) and
+        must not be read before wait()."""
+        pairs = as_pairs(pairs)
+        n = len(pairs)
+        if scores is None:
+            scores = np.zeros(n, dtype=np.int32)
+        if kernels is None and with_kernels:
+            kernels = np.zeros(n, dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib.st_sw_score_pairs_async(self._h, ptr(pairs), n, gaps.open, gaps.extend, ptr(scores),
+                                          ptr(kernels), C.byref(h)))
+        return Batch(h, scores, kernels)
+
     def plan(self, pairs, gaps: GapCosts, d_scores, d_kernels=None):
         return Plan(self, pairs, gaps, d_scores, d_kernels)
 
@@ -249,6 +264,29 @@ def as_hits(hits):
     for i, h in enumerate(hits):
         arr[i] = tuple(h)
     return arr
+
+
+class Batch:
+    """A batch started by Context.sw_score_pairs_async; wait() exactly once."""
+
+    def __init__(self, handle, scores, kernels):
+        self._h = handle
+        self.scores = scores
+        self.kernels = kernels
+
+    def wait(self):
+        if self._h is None:
+            raise RuntimeError("batch already waited for")
+        h, self._h = self._h, None
+        check(lib.st_batch_wait(h))
+        return (self.scores, self.kernels) if self.kernels is not None else self.scores
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None:
+            try:
+                lib.st_batch_wait(self._h)
+            except Exception:
+                pass
 
 
 class Plan:

@@ -236,6 +236,7 @@ struct st_ctx {
   int sms = 0;
   MemTracker mt;
   cudaStream_t own = nullptr;     // the context's stream (also used for graph capture)
+  cudaStream_t copy = nullptr;    // host->device uploads that may overlap queued kernels
   cudaStream_t stream = nullptr;  // where work is launched
   std::recursive_mutex mu;
   uint64_t launches = 0;
@@ -253,13 +254,29 @@ struct st_ctx {
   bool prof_dirty = true;
   uint32_t max_m = 0;
   std::vector<uint32_t> free_ids;  // ids of freed profiles, handed out again
+  cudaEvent_t prof_ev = nullptr;   // after the last profile build (work using profiles waits on it)
+  bool prof_ev_set = false;
+  cudaEvent_t copy_ev = nullptr;   // uploads on the copy stream
+  Pinned prof_desc;                // build descriptors on their way to the device
+  static constexpr int kMetaRing = 4;
+  Pinned meta_pin[kMetaRing];      // profile tables on their way to the device
+  cudaEvent_t meta_ev[kMetaRing] = {};
+  bool meta_used[kMetaRing] = {};
+  int meta_slot = 0;
   std::vector<int> free_blocks;    // blocks whose profiles are all freed
   // staging for the per-call paths
   Pinned pin;
   DevMem stage;
   DevMem scratch_small;
   Tuning tuning;
-  std::vector<DevMem> pool;  // device arenas of finished plans, reused by later plans
+  // device arenas of finished work, reused by later work; an arena with an
+  // event is reusable once the event has completed (work queued before it done)
+  struct PoolEntry {
+    DevMem mem;
+    cudaEvent_t ready = nullptr;
+  };
+  std::vector<PoolEntry> pool;
+  std::vector<cudaEvent_t> spare_events;
   // pipelined batches: pinned staging ring (one block per plan in flight) and two side streams
   static constexpr int kStageRing = 6;
   Pinned plan_pin[kStageRing];
@@ -268,6 +285,7 @@ struct st_ctx {
   static constexpr int kMaxSide = 4;
   cudaStream_t side[kMaxSide] = {};
   Pinned out_pin;  // scores and kernel tags on their way to pageable caller buffers
+  std::vector<std::unique_ptr<Pinned>> pin_free;  // staging blocks of finished batches
   cudaEvent_t side_ev[1 + kMaxSide] = {};  // [0] start of a batch, [1 + i] end of side stream i's work
   // fork streams of a plan's launches: the 16-bit classes run side by side, the 32-bit kernel after them.
   // Set 0 serves the context's own / caller's stream, set 1 + i side stream i.
@@ -293,24 +311,56 @@ struct st_ctx {
 // A device buffer of at least `bytes` from the context's pool (or a new allocation).
 static int pool_get(st_ctx* c, size_t bytes, DevMem& out) {
   int best = -1;
-  for (size_t i = 0; i < c->pool.size(); ++i)
-    if (c->pool[i].bytes >= bytes && c->pool[i].bytes <= 4 * bytes + (64 << 20) &&
-        (best < 0 || c->pool[i].bytes < c->pool[best].bytes))
-      best = static_cast<int>(i);
+  for (size_t i = 0; i < c->pool.size(); ++i) {
+    const DevMem& m = c->pool[i].mem;
+    if (m.bytes < bytes || m.bytes > 4 * bytes + (64 << 20)) continue;
+    if (best >= 0 && m.bytes >= c->pool[best].mem.bytes) continue;
+    cudaEvent_t e = c->pool[i].ready;
+    if (e && cudaEventQuery(e) != cudaSuccess) {
+      cudaGetLastError();  // cudaErrorNotReady: still in use
+      continue;
+    }
+    best = static_cast<int>(i);
+  }
   if (best >= 0) {
-    out = std::move(c->pool[best]);
+    out = std::move(c->pool[best].mem);
+    if (c->pool[best].ready) c->spare_events.push_back(c->pool[best].ready);
     c->pool.erase(c->pool.begin() + best);
     return ST_OK;
   }
   return dev_alloc(&c->mt, out, bytes + bytes / 8);
 }
 
-static void pool_put(st_ctx* c, DevMem&& m) {
-  if (!m.p) return;
-  c->pool.push_back(std::move(m));
-  while (c->pool.size() > 96) {  // keep the most recent arenas (one per chunk of a pipelined batch)
+static void pool_trim(st_ctx* c) {
+  while (c->pool.size() > 96) {  // keep the most recent arenas (freeing one waits for the device)
+    if (c->pool.front().ready) c->spare_events.push_back(c->pool.front().ready);
     c->pool.erase(c->pool.begin());
   }
+}
+
+// Back to the pool, reusable at once (no queued work uses it).
+static void pool_put(st_ctx* c, DevMem&& m) {
+  if (!m.p) return;
+  c->pool.push_back(st_ctx::PoolEntry{std::move(m), nullptr});
+  pool_trim(c);
+}
+
+// Back to the pool, reusable once the work queued on `s` so far has finished.
+static void pool_put_after(st_ctx* c, DevMem&& m, cudaStream_t s) {
+  if (!m.p) return;
+  cudaEvent_t e = nullptr;
+  if (!c->spare_events.empty()) {
+    e = c->spare_events.back();
+    c->spare_events.pop_back();
+  } else if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamSynchronize(s);  // no event: wait instead
+    pool_put(c, std::move(m));
+    return;
+  }
+  cudaEventRecord(e, s);
+  c->pool.push_back(st_ctx::PoolEntry{std::move(m), e});
+  pool_trim(c);
 }
 
 static DeviceDb db_view(st_ctx* c) {
@@ -322,14 +372,34 @@ static DeviceDb db_view(st_ctx* c) {
   return d;
 }
 
+// Orders the context's stream after the last profile build and, when
+// profiles were created or freed since, refreshes the device tables of
+// profile pointers, strides and lengths. The tables go up on the stream from
+// a ring of pinned blocks, so work already queued keeps reading the old ones.
 static int sync_profiles(st_ctx* c) {
+  if (c->prof_ev_set) {
+    ST_CUDA(cudaStreamWaitEvent(c->stream, c->prof_ev, 0));
+    if (c->own != c->stream) ST_CUDA(cudaStreamWaitEvent(c->own, c->prof_ev, 0));
+  }
   if (!c->prof_dirty) return ST_OK;
   const size_t n = std::max<size_t>(c->profs.size(), 1);
-  std::vector<const int8_t*> p8(n, nullptr);
-  std::vector<const int32_t*> p32(n, nullptr);
-  std::vector<uint32_t> s8(n, 0), s32(n, 0), ql(n, 0);
-  std::vector<int32_t> mx(n, 0);
-  std::vector<uint8_t> f8(n, 0);
+  const size_t o_p8 = 0, o_p32 = o_p8 + n * 8, o_s8 = o_p32 + n * 8, o_s32 = o_s8 + n * 4, o_ql = o_s32 + n * 4,
+               o_mx = o_ql + n * 4, o_f8 = o_mx + n * 4, total = o_f8 + n;
+  const int slot = c->meta_slot;
+  c->meta_slot = (slot + 1) % st_ctx::kMetaRing;
+  if (!c->meta_ev[slot]) ST_CUDA(cudaEventCreateWithFlags(&c->meta_ev[slot], cudaEventDisableTiming));
+  if (c->meta_used[slot]) ST_CUDA(cudaEventSynchronize(c->meta_ev[slot]));  // its last upload is done
+  c->meta_used[slot] = false;
+  ST_TRY(c->meta_pin[slot].reserve(total));
+  char* h = c->meta_pin[slot].as<char>();
+  memset(h, 0, total);
+  const int8_t** p8 = reinterpret_cast<const int8_t**>(h + o_p8);
+  const int32_t** p32 = reinterpret_cast<const int32_t**>(h + o_p32);
+  uint32_t* s8 = reinterpret_cast<uint32_t*>(h + o_s8);
+  uint32_t* s32 = reinterpret_cast<uint32_t*>(h + o_s32);
+  uint32_t* ql = reinterpret_cast<uint32_t*>(h + o_ql);
+  int32_t* mx = reinterpret_cast<int32_t*>(h + o_mx);
+  uint8_t* f8 = reinterpret_cast<uint8_t*>(h + o_f8);
   uint32_t max_m = 0;
   for (size_t i = 0; i < c->profs.size(); ++i) {
     const ProfileMeta& p = c->profs[i];
@@ -343,19 +413,24 @@ static int sync_profiles(st_ctx* c) {
     f8[i] = p.fits8 ? 1 : 0;
     max_m = std::max(max_m, p.m);
   }
-  auto up = [&](DevMem& d, const void* src, size_t bytes) -> int {
-    if (d.bytes < bytes) ST_TRY(dev_alloc(&c->mt, d, bytes * 2));
-    ST_CUDA(cudaMemcpyAsync(d.p, src, bytes, cudaMemcpyHostToDevice, c->own));
+  auto up = [&](DevMem& d, size_t off, size_t bytes) -> int {
+    if (d.bytes < bytes) {
+      ST_CUDA(cudaStreamSynchronize(c->stream));  // queued work may read the old table
+      ST_TRY(dev_alloc(&c->mt, d, bytes * 2));
+    }
+    ST_CUDA(cudaMemcpyAsync(d.p, h + off, bytes, cudaMemcpyHostToDevice, c->stream));
     return ST_OK;
   };
-  ST_TRY(up(c->d_p8, p8.data(), n * sizeof(void*)));
-  ST_TRY(up(c->d_p32, p32.data(), n * sizeof(void*)));
-  ST_TRY(up(c->d_stride8, s8.data(), n * 4));
-  ST_TRY(up(c->d_stride32, s32.data(), n * 4));
-  ST_TRY(up(c->d_qlen, ql.data(), n * 4));
-  ST_TRY(up(c->d_maxs, mx.data(), n * 4));
-  ST_TRY(up(c->d_fits8, f8.data(), n));
-  ST_CUDA(cudaStreamSynchronize(c->own));
+  ST_TRY(up(c->d_p8, o_p8, n * 8));
+  ST_TRY(up(c->d_p32, o_p32, n * 8));
+  ST_TRY(up(c->d_stride8, o_s8, n * 4));
+  ST_TRY(up(c->d_stride32, o_s32, n * 4));
+  ST_TRY(up(c->d_qlen, o_ql, n * 4));
+  ST_TRY(up(c->d_maxs, o_mx, n * 4));
+  ST_TRY(up(c->d_fits8, o_f8, n));
+  ST_CUDA(cudaEventRecord(c->meta_ev[slot], c->stream));
+  if (c->own != c->stream) ST_CUDA(cudaStreamWaitEvent(c->own, c->meta_ev[slot], 0));  // graphs run there too
+  c->meta_used[slot] = true;
   c->max_m = max_m;
   c->prof_dirty = false;
   return ST_OK;
@@ -420,6 +495,10 @@ extern "C" st_ctx* st_init(int device, size_t hbm_budget_bytes) {
     return nullptr;
   }
   c->stream = c->own;
+  if (cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) != cudaSuccess) {
+    fail(ST_ECUDA, "cudaStreamCreate failed");
+    return nullptr;
+  }
   if (set_smem_limits(device) != ST_OK) return nullptr;
   tuning_defaults(&c->tuning);
   return c.release();
@@ -438,6 +517,9 @@ extern "C" void st_shutdown(st_ctx* c) {
     if (e) cudaEventDestroy(e);
   for (auto e : c->plan_pin_ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : c->pool)
+    if (e.ready) cudaEventDestroy(e.ready);
+  for (auto e : c->spare_events) cudaEventDestroy(e);
   for (auto& f : c->forks) {
     for (auto s : f.s)
       if (s) {
@@ -448,6 +530,14 @@ extern "C" void st_shutdown(st_ctx* c) {
       if (e) cudaEventDestroy(e);
   }
   cudaStream_t own = c->own;
+  if (c->copy) {
+    cudaStreamSynchronize(c->copy);
+    cudaStreamDestroy(c->copy);
+  }
+  if (c->prof_ev) cudaEventDestroy(c->prof_ev);
+  if (c->copy_ev) cudaEventDestroy(c->copy_ev);
+  for (auto e : c->meta_ev)
+    if (e) cudaEventDestroy(e);
   delete c;
   cudaStreamDestroy(own);
 }
@@ -604,18 +694,21 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   struct Back {
     st_ctx* c;
     DevMem* m;
-    ~Back() {
-      cudaStreamSynchronize(c->own);
-      pool_put(c, std::move(*m));
-    }
+    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
   } back_tmp{c, &tmp};
+  if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+  if (!c->prof_ev) ST_CUDA(cudaEventCreateWithFlags(&c->prof_ev, cudaEventDisableTiming));
   tc.lap("alloc");
   char* base = blk_mem.as<char>();
   int32_t* d_src = tmp.as<int32_t>();
   ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + up16(src_bytes));
-  // the rows travel while the host computes their score ranges
+  // The rows travel on the copy stream (beside any kernels still queued) while
+  // the host computes their score ranges; the build runs on the context's
+  // stream after both. The call returns once the rows and descriptors are on
+  // the device (the caller may reuse them), not when the build is done: later
+  // work on the profiles is ordered after it.
   if (src_bytes)
-    ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->own));
+    ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->copy));
   // score range per profile (residues >= 21 score 0), in parallel over profiles
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) {
@@ -630,12 +723,18 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
     desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
   }
   tc.lap("range");
-  ST_CUDA(cudaMemcpyAsync(d_desc, desc.data(), n_profiles * sizeof(ProfBuildDesc), cudaMemcpyHostToDevice, c->own));
-  build_profiles_kernel<<<n_profiles, 256, 0, c->own>>>(d_src, d_desc, base);
+  ST_TRY(c->prof_desc.reserve(n_profiles * sizeof(ProfBuildDesc)));
+  memcpy(c->prof_desc.p, desc.data(), n_profiles * sizeof(ProfBuildDesc));
+  ST_CUDA(cudaMemcpyAsync(d_desc, c->prof_desc.p, n_profiles * sizeof(ProfBuildDesc), cudaMemcpyHostToDevice, c->copy));
+  ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
+  ST_CUDA(cudaStreamWaitEvent(c->stream, c->copy_ev, 0));
+  build_profiles_kernel<<<n_profiles, 256, 0, c->stream>>>(d_src, d_desc, base);
   ++c->launches;
   ST_CUDA(cudaGetLastError());
-  ST_CUDA(cudaStreamSynchronize(c->own));
-  tc.lap("upload+build");
+  ST_CUDA(cudaEventRecord(c->prof_ev, c->stream));
+  c->prof_ev_set = true;
+  ST_CUDA(cudaEventSynchronize(c->copy_ev));
+  tc.lap("upload");
   int bi;
   if (!c->free_blocks.empty()) {
     bi = c->free_blocks.back();
@@ -688,8 +787,7 @@ static int profile_free(st_ctx* c, uint32_t id) {
   p.live = false;
   ProfileBlock* b = c->blocks[p.block].get();
   if (--b->live == 0) {
-    ST_CUDA(cudaStreamSynchronize(c->stream));
-    pool_put(c, std::move(b->mem));
+    pool_put_after(c, std::move(b->mem), c->stream);  // reusable once work queued so far is done
     c->free_blocks.push_back(p.block);
   }
   p.block = -1;
@@ -1688,7 +1786,11 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   in.pairs = reinterpret_cast<const st_pair*>(b + o_pairs);
 
   // stage 1: pairs in, classify, sort, per-query class and CTA-task counts, class order
-  ST_CUDA(cudaMemcpyAsync(b + o_pairs, pairs, n * 16, cudaMemcpyHostToDevice, st));
+  // the pairs go up on the copy stream, beside kernels still queued on the stream
+  if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+  ST_CUDA(cudaMemcpyAsync(b + o_pairs, pairs, n * 16, cudaMemcpyHostToDevice, c->copy));
+  ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
+  ST_CUDA(cudaStreamWaitEvent(st, c->copy_ev, 0));
   ST_CUDA(cudaMemsetAsync(cinit, 0, (kNumClasses + 2) * 4, st));
   ST_CUDA(cudaMemsetAsync(w.qcnt, 0, np1 * 4, st));
   ST_CUDA(cudaMemsetAsync(w.totals, 0, sizeof(DpTotals), st));
@@ -1840,11 +1942,145 @@ static bool use_device_plan(uint64_t n) {
   return n >= env_u64("ST_DEVICE_PLAN_MIN", 16384);
 }
 
+// One batch of pairs in flight: its plan, device buffers, staging and the
+// event after its result copies.
+struct st_batch {
+  st_ctx* c = nullptr;
+  uint64_t n = 0;
+  int32_t* scores = nullptr;
+  uint32_t* kernels = nullptr;
+  DevMem out, work;
+  st_plan* plan = nullptr;
+  std::unique_ptr<Pinned> stage;  // null when the caller's buffers are pinned
+  cudaEvent_t done = nullptr;
+};
+
+static void batch_release(st_batch* b) {
+  st_ctx* c = b->c;
+  if (b->done) {
+    cudaEventSynchronize(b->done);
+    c->spare_events.push_back(b->done);
+  } else {
+    cudaStreamSynchronize(c->stream);
+  }
+  if (b->plan) plan_free(b->plan);
+  pool_put(c, std::move(b->out));
+  pool_put(c, std::move(b->work));
+  if (b->stage) c->pin_free.push_back(std::move(b->stage));
+  delete b;
+}
+
+// Validates, uploads, plans and launches a batch and queues its result copies;
+// does not wait for them. Batches of at least the device-plan size are planned
+// on the GPU (one short wait for the per-class totals); smaller ones on the host.
+static int batch_begin(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* scores,
+                       uint32_t* kernels, st_batch** out) {
+  std::unique_ptr<st_batch, void (*)(st_batch*)> b(new st_batch, batch_release);
+  b->c = c;
+  b->n = n;
+  b->scores = scores;
+  b->kernels = kernels;
+  TraceClock tc("pairs");
+  if (n == 0) {  // nothing to score: a batch that is done when the stream gets there
+    ST_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+    ST_CUDA(cudaEventRecord(b->done, c->stream));
+    *out = b.release();
+    return ST_OK;
+  }
+  ST_TRY(pool_get(c, n * 8, b->out));
+  int32_t* d_scores = b->out.as<int32_t>();
+  uint32_t* d_kern = reinterpret_cast<uint32_t*>(d_scores + n);
+  // Results come back through pinned memory unless the caller's buffers are
+  // pinned already.
+  int32_t* h_scores = scores;
+  uint32_t* h_kern = kernels;
+  if (!(host_pinned(scores) && (!kernels || host_pinned(kernels)))) {
+    for (size_t i = 0; i < c->pin_free.size(); ++i)
+      if (c->pin_free[i]->bytes >= n * 8) {
+        b->stage = std::move(c->pin_free[i]);
+        c->pin_free.erase(c->pin_free.begin() + i);
+        break;
+      }
+    if (!b->stage) b->stage.reset(new Pinned);
+    ST_TRY(b->stage->reserve(n * 8));
+    h_scores = b->stage->as<int32_t>();
+    h_kern = kernels ? b->stage->as<uint32_t>(n * 4) : nullptr;
+  }
+  if (use_device_plan(n)) {
+    uint32_t max_len = 0, max_m = 0;
+    ST_TRY(validate_pairs(c, pairs, n, &max_len, &max_m));
+    ST_TRY(sync_profiles(c));
+    tc.lap("validate");
+    ST_TRY(dplan_build(c, pairs, n, open, ext, d_scores, d_kern, max_len, max_m, b->work, &b->plan));
+  } else {
+    ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &b->plan, false, c->stream, 0));
+    tc.lap("plan");
+  }
+  ST_TRY(plan_run(b->plan));
+  ST_CUDA(cudaMemcpyAsync(h_scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (kernels) ST_CUDA(cudaMemcpyAsync(h_kern, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (!c->spare_events.empty()) {
+    b->done = c->spare_events.back();
+    c->spare_events.pop_back();
+  } else {
+    ST_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+  }
+  ST_CUDA(cudaEventRecord(b->done, c->stream));
+  *out = b.release();
+  return ST_OK;
+}
+
+// Waits for a batch, writes its results to the caller's buffers and releases it.
+static int batch_finish(st_batch* b) {
+  TraceClock tc("pairs");
+  st_ctx* c = b->c;
+  const cudaError_t e = cudaEventSynchronize(b->done);
+  if (e == cudaSuccess && b->stage) {
+    const uint64_t n = b->n;
+    const int32_t* hs = b->stage->as<int32_t>();
+    const uint32_t* hk = b->stage->as<uint32_t>(n * 4);
+    int32_t* scores = b->scores;
+    uint32_t* kernels = b->kernels;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < static_cast<int64_t>((n + 262143) / 262144); ++k) {
+      const uint64_t a0 = static_cast<uint64_t>(k) * 262144, a1 = std::min<uint64_t>(n, a0 + 262144);
+      memcpy(scores + a0, hs + a0, (a1 - a0) * 4);
+      if (kernels) memcpy(kernels + a0, hk + a0, (a1 - a0) * 4);
+    }
+  }
+  batch_release(b);
+  (void)c;
+  tc.lap("wait+copy");
+  if (e != cudaSuccess) return fail(ST_ECUDA, "batch failed: %s", cudaGetErrorString(e));
+  return ST_OK;
+}
+
+extern "C" int st_sw_score_pairs_async(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                                       int32_t* scores, uint32_t* kernels, st_batch** batch) {
+  CTX_GUARD(c);
+  if (!batch || (n && (!pairs || !scores))) return fail(ST_EINVAL, "st_sw_score_pairs_async: null argument");
+  *batch = nullptr;
+  return batch_begin(c, pairs, n, open, ext, scores, kernels, batch);
+}
+
+extern "C" int st_batch_wait(st_batch* batch) {
+  if (!batch) return fail(ST_EINVAL, "st_batch_wait: null batch");
+  st_ctx* c = batch->c;
+  CTX_GUARD(c);
+  return batch_finish(batch);
+}
+
 extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
                                  int32_t* scores, uint32_t* kernels) {
   CTX_GUARD(c);
   if (n && (!pairs || !scores)) return fail(ST_EINVAL, "st_sw_score_pairs: null argument");
   if (n == 0) return ST_OK;
+  if (use_device_plan(n) || pipeline_bounds(n).size() <= 2) {
+    st_batch* b = nullptr;
+    ST_TRY(batch_begin(c, pairs, n, open, ext, scores, kernels, &b));
+    return batch_finish(b);
+  }
+  // large batches with the host planner: pipelined chunks
   DevMem d_out;
   ST_TRY(pool_get(c, n * 8, d_out));
   struct Back {
@@ -1855,9 +2091,6 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
   int32_t* d_scores = d_out.as<int32_t>();
   uint32_t* d_kern = reinterpret_cast<uint32_t*>(d_scores + n);
   TraceClock tc("pairs");
-  // Results come back through pinned memory unless the caller's buffers are
-  // pinned already: a copy into pageable memory would block the host until
-  // the kernels before it finish, which serialises planning with the GPU.
   const bool direct = host_pinned(scores) && (!kernels || host_pinned(kernels));
   int32_t* h_scores = scores;
   uint32_t* h_kern = kernels;
@@ -1875,47 +2108,8 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
       if (kernels) memcpy(kernels + a0, h_kern + a0, (a1 - a0) * 4);
     }
   };
-  if (use_device_plan(n)) {
-    uint32_t max_len = 0, max_m = 0;
-    ST_TRY(validate_pairs(c, pairs, n, &max_len, &max_m));
-    ST_TRY(sync_profiles(c));
-    tc.lap("validate");
-    DevMem work;
-    st_plan* p = nullptr;
-    const int rc = dplan_build(c, pairs, n, open, ext, d_scores, d_kern, max_len, max_m, work, &p);
-    std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
-    struct Drain {  // the stream finishes before the work buffers go back to the pool
-      st_ctx* c;
-      DevMem* m;
-      ~Drain() {
-        cudaStreamSynchronize(c->stream);
-        pool_put(c, std::move(*m));
-      }
-    } drain{c, &work};
-    ST_TRY(rc);
-    ST_TRY(plan_run(p));
-    ST_CUDA(cudaMemcpyAsync(h_scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
-    if (kernels) ST_CUDA(cudaMemcpyAsync(h_kern, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
-    ST_CUDA(cudaStreamSynchronize(c->stream));
-    copy_out();
-    tc.lap("run+download");
-    return ST_OK;
-  }
   const std::vector<uint64_t> bounds = pipeline_bounds(n);
   const uint64_t chunks = bounds.size() - 1;
-  if (chunks <= 1) {
-    st_plan* p = nullptr;
-    ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &p, false, c->stream, 0));
-    std::unique_ptr<st_plan, void (*)(st_plan*)> guard(p, plan_free);
-    tc.lap("plan");
-    ST_TRY(plan_run(p));
-    ST_CUDA(cudaMemcpyAsync(h_scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
-    if (kernels) ST_CUDA(cudaMemcpyAsync(h_kern, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
-    ST_CUDA(cudaStreamSynchronize(c->stream));
-    copy_out();
-    tc.lap("run+download");
-    return ST_OK;
-  }
   // Pipelined: the pairs are cut into contiguous chunks, each planned on the
   // host while the chunks before it run. Chunks alternate between two side
   // streams, so the tail of one chunk's persistent grid overlaps the start of

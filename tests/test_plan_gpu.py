@@ -200,3 +200,46 @@ def test_profile_ids_are_reused_and_batch_free_checks_ids(ctx):
     want = O.sw_pairs(O.Arena(w.rows, w.targets()), w.pair_q, w.pair_t, 44, 4)
     assert np.array_equal(first, want)
     ctx.free_profiles(again)
+
+
+def test_async_batches_overlap_and_early_profile_free(ctx):
+    """Two batches in flight; the first batch's profiles are freed (and their ids reused by
+    the second batch's profiles) before it is waited for: queued work keeps its profiles."""
+    import torch
+    w1 = W.config3(seed=21, n_queries=30, db_residues=60_000, per_query=80)
+    w2 = W.config3(seed=22, n_queries=25, db_residues=60_000, per_query=90)
+    # one database for both: w2's targets appended after w1's
+    t1, t2 = w1.targets(), w2.targets()
+    ctx.upload_db_list(t1 + t2)
+    ids1 = ctx.create_profiles(w1.rows)
+    p1 = _pairs(ids1, w1)
+    out1 = torch.empty(w1.n_pairs, dtype=torch.int32, pin_memory=True).numpy()
+    b1 = ctx.sw_score_pairs_async(p1, GapCosts(44, 4), scores=out1)
+    ctx.free_profiles(ids1)  # before b1 is waited for
+    ids2 = ctx.create_profiles(w2.rows)
+    assert set(ids2.tolist()) & set(ids1.tolist())  # ids were handed out again
+    p2 = _pairs(ids2, w2)
+    p2["target"] += len(t1)
+    b2 = ctx.sw_score_pairs_async(p2, GapCosts(11, 1))  # pageable output
+    got2 = b2.wait()
+    got1 = b1.wait()
+    want1 = O.sw_pairs(O.Arena(w1.rows, t1), w1.pair_q, w1.pair_t, 44, 4)
+    want2 = O.sw_pairs(O.Arena(w2.rows, t2), w2.pair_q, w2.pair_t, 11, 1)
+    assert np.array_equal(got1, want1)
+    assert np.array_equal(got2, want2)
+    with pytest.raises(RuntimeError):
+        b1.wait()
+    ctx.free_profiles(ids2)
+
+
+def test_async_batch_of_nothing_and_sync_equals_async(ctx):
+    w = W.config3(seed=23, n_queries=12, db_residues=30_000, per_query=40)
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    pairs = _pairs(ids, w)
+    empty = ctx.sw_score_pairs_async(pairs[:0], GapCosts(44, 4))
+    assert len(empty.wait()) == 0
+    s, k = ctx.sw_score_pairs_async(pairs, GapCosts(44, 4), with_kernels=True).wait()
+    s2, k2 = ctx.sw_score_pairs(pairs, GapCosts(44, 4), with_kernels=True)
+    assert np.array_equal(s, s2) and np.array_equal(k, k2)
+    ctx.free_profiles(ids)
