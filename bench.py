@@ -360,7 +360,7 @@ def main():
         outs = [torch.empty(w.n_pairs, dtype=torch.int32, pin_memory=True).numpy() for _ in range(2)]
         kouts = [torch.empty(w.n_pairs, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
                  for _ in range(2)]
-        steps_ov = max(2, args.e2e_steps)
+        steps_ov = max(8, args.e2e_steps)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         prev = None
