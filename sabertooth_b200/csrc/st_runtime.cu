@@ -196,7 +196,9 @@ static const Sw16Class kClasses[] = {
     ST_CLASS(4, 8, 4),   ST_CLASS(8, 8, 4),   ST_CLASS(16, 8, 4),  ST_CLASS(32, 8, 4),
     ST_CLASS(4, 12, 4),  ST_CLASS(8, 12, 4),  ST_CLASS(16, 12, 4), ST_CLASS(32, 12, 4),
     ST_CLASS(4, 16, 4),  ST_CLASS(8, 16, 4),  ST_CLASS(16, 16, 4), ST_CLASS(32, 16, 4),
+    ST_CLASS(4, 20, 4),  ST_CLASS(8, 20, 4),  ST_CLASS(16, 20, 4), ST_CLASS(32, 20, 4),
     ST_CLASS(4, 24, 4),  ST_CLASS(8, 24, 4),  ST_CLASS(16, 24, 4), ST_CLASS(32, 24, 4),
+    ST_CLASS_W(4, 28, 4, 4), ST_CLASS_W(8, 28, 4, 4), ST_CLASS_W(16, 28, 4, 4),
     ST_CLASS_W(4, 32, 4, 4), ST_CLASS_W(8, 32, 4, 4), ST_CLASS_W(16, 32, 4, 4),
     ST_CLASS(32, 16, 2),
 };
@@ -290,7 +292,7 @@ struct st_ctx {
   // fork streams of a plan's launches: the 16-bit classes run side by side, the 32-bit kernel after them.
   // Set 0 serves the context's own / caller's stream, set 1 + i side stream i.
   struct ForkSet {
-    static constexpr int kForks = 3;
+    static constexpr int kForks = 15;
     cudaStream_t s[kForks] = {};
     cudaEvent_t ev[kForks + 1] = {};
   };

@@ -307,13 +307,18 @@ __global__ void __launch_bounds__(WARPS * 32) sw16_kernel(const Sw16Params prm) 
       my_rB = rB;
       const int col = static_cast<int>(ctl & 0xFFFFu);
       const int pass = static_cast<int>((ctl >> 16) & 0xFFu);
-      if (col == 0) {  // first column of a pass (or idle): left border H = 0, first-column E
+      // first column of a pass (or idle): left border H = 0, first-column E. The
+      // groups of a warp move in step, so lane l of every group resets on the
+      // same steps: the branch is skipped on the other steps of a pass.
+      if (__any_sync(FULL, col == 0)) {
+        if (col == 0) {
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-          Hp[k] = 0;
-          E[k] = E0;
+          for (int k = 0; k < R; ++k) {
+            Hp[k] = 0;
+            E[k] = E0;
+          }
+          hup_prev = 0;
         }
-        hup_prev = 0;
       }
       const int8_t* rows = prof_s + pass * (G * R) + gl * R;
 #pragma unroll

@@ -57,10 +57,13 @@ inline float tuning_default_rate(int G, int R, int C) {
     int G, R;
     float rate;
   } kRates[] = {
-      {4, 8, 3.545f},   {8, 8, 4.288f},   {16, 8, 4.434f},  {32, 8, 4.345f},  {4, 12, 3.638f},
-      {8, 12, 4.429f},  {16, 12, 4.630f}, {32, 12, 4.448f}, {4, 16, 3.801f},  {8, 16, 4.644f},
-      {16, 16, 4.813f}, {32, 16, 4.650f}, {4, 24, 4.439f},  {8, 24, 5.160f},  {16, 24, 5.247f},
-      {32, 24, 5.030f}, {4, 32, 4.923f},  {8, 32, 5.306f},  {16, 32, 5.244f},
+      {4, 8, 3.826f}, {8, 8, 4.573f}, {16, 8, 4.578f}, {32, 8, 4.483f},
+      {4, 12, 3.832f}, {8, 12, 4.817f}, {16, 12, 4.879f}, {32, 12, 4.665f},
+      {4, 16, 3.986f}, {8, 16, 4.959f}, {16, 16, 5.011f}, {32, 16, 4.788f},
+      {4, 20, 4.451f}, {8, 20, 5.240f}, {16, 20, 5.198f}, {32, 20, 5.069f},
+      {4, 24, 4.680f}, {8, 24, 5.405f}, {16, 24, 5.399f}, {32, 24, 5.128f},
+      {4, 28, 5.289f}, {8, 28, 5.362f}, {16, 28, 4.958f}, {4, 32, 5.194f},
+      {8, 32, 5.233f}, {16, 32, 5.126f},
   };
   for (const auto& r : kRates)
     if (r.G == G && r.R == R) return r.rate;
