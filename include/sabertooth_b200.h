@@ -117,6 +117,34 @@ typedef struct st_batch st_batch;
 int st_sw_score_pairs_async(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
                             int32_t* scores, uint32_t* kernels, st_batch** batch);
 int st_batch_wait(st_batch* batch);
+/* 0 when the batch's results are ready (st_batch_wait will not block), 1 while it runs. */
+int st_batch_query(st_batch* batch);
+
+/* ---- serving: continuous batching of requests ------------------------------
+ * (No reference counterpart: the reference scores a search's queries in one
+ * rayon pass.)  A server owns a worker thread on one context.  A request is
+ * one query, as int32 [m][21] rows, and n database targets to score it against
+ * (band_center/band_radius may be NULL: full local alignment).  Requests are
+ * batched in arrival order as they come, up to max_batch_pairs pairs per batch
+ * and hbm_budget_bytes of device memory for the batches in flight (two: one
+ * running while the next is built and launched).  Scores equal those of the
+ * same request scored alone.  submit copies its inputs and returns at once;
+ * wait blocks until the request is done and returns its scores (cap entries)
+ * and its latency from submit to completion in milliseconds. */
+typedef struct st_server st_server;
+st_server* st_server_create(st_ctx* ctx, int32_t open, int32_t ext, uint64_t max_batch_pairs,
+                            uint64_t hbm_budget_bytes);
+int st_server_submit(st_server* server, const int32_t* rows, uint32_t m, const uint32_t* targets,
+                     const int32_t* band_center, const int32_t* band_radius, uint32_t n, uint64_t* request_id);
+/* Many requests arriving together (one call, one lock): request k has rows
+ * [row_offsets[k], row_offsets[k+1]) of rows and targets [target_offsets[k],
+ * target_offsets[k+1]) of targets/band_center/band_radius; ids to request_ids[k]. */
+int st_server_submit_many(st_server* server, uint32_t n_requests, const int32_t* rows, const uint64_t* row_offsets,
+                          const uint32_t* targets, const uint64_t* target_offsets, const int32_t* band_center,
+                          const int32_t* band_radius, uint64_t* request_ids);
+int st_server_wait(st_server* server, uint64_t request_id, int32_t* scores, uint32_t cap, double* latency_ms);
+int st_server_stats(st_server* server, uint64_t* batches, uint64_t* pairs);
+void st_server_destroy(st_server* server);
 
 /* Planned form over device buffers: a plan binds a pair list (copied at plan
  * time), gap costs and device output buffers; st_plan_run replays the captured

@@ -6,8 +6,8 @@ rescore) and batched ungapped diagonal scoring, behind a C ABI
 signatures.  Importing the package loads libsabertooth_b200.so and fails if it
 is missing; build it with `python sabertooth_b200/_build.py`.
 """
-from .api import (Context, DiagProfile, GapCosts, Kernel, Lane, Plan, QueryProfile, default_context, diag_range,
-                  kadane_score, score_batch, tile_classes)
+from .api import (Batch, Context, DiagProfile, GapCosts, Kernel, Lane, Plan, QueryProfile, Server, default_context,
+                  diag_range, kadane_score, score_batch, tile_classes)
 from .matrix import SubstitutionMatrix, blosum62, decode, encode
 
 __all__ = ["Context", "DiagProfile", "GapCosts", "Kernel", "Lane", "Plan", "QueryProfile", "default_context",

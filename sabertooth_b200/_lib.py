@@ -58,6 +58,13 @@ SIGNATURES = {
     "st_profiles_free": (C.c_int, [_P, _P, _u32]),
     "st_sw_score_pairs_async": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P, _P]),
     "st_batch_wait": (C.c_int, [_P]),
+    "st_batch_query": (C.c_int, [_P]),
+    "st_server_create": (_P, [_P, _i32, _i32, _u64, _u64]),
+    "st_server_submit": (C.c_int, [_P, _P, _u32, _P, _P, _P, _u32, _P]),
+    "st_server_submit_many": (C.c_int, [_P, _u32, _P, _P, _P, _P, _P, _P, _P]),
+    "st_server_wait": (C.c_int, [_P, _u64, _P, _u32, _P]),
+    "st_server_stats": (C.c_int, [_P, _P, _P]),
+    "st_server_destroy": (None, [_P]),
     "st_profiles_create": (C.c_int, [_P, _P, _P, _u32, _P]),
     "st_sw_score": (C.c_int, [_P, _u32, _P, _u32, _i32, _i32, _P, _P]),
     "st_sw_score_pairs": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P]),

@@ -289,6 +289,70 @@ class Batch:
                 pass
 
 
+class Server:
+    """Continuous batching of scoring requests (st_server_*): submit() returns a request id at
+    once, wait(id) returns (scores, latency_ms). One worker thread per server batches requests
+    in arrival order and keeps two batches in flight."""
+
+    def __init__(self, ctx: Context, gaps: GapCosts, max_batch_pairs=0, hbm_budget_bytes=0):
+        self._ctx = ctx
+        self._h = lib.st_server_create(ctx.handle, gaps.open, gaps.extend, int(max_batch_pairs),
+                                       int(hbm_budget_bytes))
+        if not self._h:
+            check(-1)
+        self._n = {}
+
+    def submit(self, rows, targets, band_center=None, band_radius=None):
+        rows = np.ascontiguousarray(rows, dtype=np.int32).reshape(-1, 21)
+        targets = np.ascontiguousarray(targets, dtype=np.uint32)
+        bc = None if band_center is None else np.ascontiguousarray(band_center, dtype=np.int32)
+        br = None if band_radius is None else np.ascontiguousarray(band_radius, dtype=np.int32)
+        rid = C.c_uint64()
+        check(lib.st_server_submit(self._h, ptr(rows), rows.shape[0], ptr(targets), ptr(bc), ptr(br),
+                                   len(targets), C.byref(rid)))
+        self._n[rid.value] = len(targets)
+        return rid.value
+
+    def submit_many(self, rows_arena, row_offsets, targets, target_offsets, band_center=None, band_radius=None):
+        """Requests arriving together: request k = rows_arena[row_offsets[k]:row_offsets[k+1]] against
+        targets[target_offsets[k]:target_offsets[k+1]]. Returns the request ids."""
+        rows = np.ascontiguousarray(rows_arena, dtype=np.int32).reshape(-1, 21)
+        ro = np.ascontiguousarray(row_offsets, dtype=np.uint64)
+        t = np.ascontiguousarray(targets, dtype=np.uint32)
+        to = np.ascontiguousarray(target_offsets, dtype=np.uint64)
+        bc = None if band_center is None else np.ascontiguousarray(band_center, dtype=np.int32)
+        br = None if band_radius is None else np.ascontiguousarray(band_radius, dtype=np.int32)
+        k = len(ro) - 1
+        ids = np.zeros(k, dtype=np.uint64)
+        check(lib.st_server_submit_many(self._h, k, ptr(rows), ptr(ro), ptr(t), ptr(to), ptr(bc), ptr(br), ptr(ids)))
+        for j in range(k):
+            self._n[int(ids[j])] = int(to[j + 1] - to[j])
+        return ids
+
+    def wait(self, rid):
+        n = self._n.pop(int(rid))
+        out = np.zeros(n, dtype=np.int32)
+        lat = C.c_double()
+        check(lib.st_server_wait(self._h, int(rid), ptr(out), n, C.byref(lat)))
+        return out, lat.value
+
+    def stats(self):
+        b, p = C.c_uint64(), C.c_uint64()
+        check(lib.st_server_stats(self._h, C.byref(b), C.byref(p)))
+        return {"batches": b.value, "pairs": p.value}
+
+    def close(self):
+        if self._h:
+            lib.st_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Plan:
     """A captured batch over device buffers (d_scores / d_kernels: device pointers as ints)."""
 

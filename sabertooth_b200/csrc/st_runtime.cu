@@ -173,6 +173,16 @@ struct Pinned {
 };
 
 static inline size_t up16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+
+static bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // not a CUDA-known pointer: pageable
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 static inline size_t up4(size_t x) { return (x + 3) & ~static_cast<size_t>(3); }
 static inline size_t up256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
@@ -260,6 +270,9 @@ struct st_ctx {
   bool prof_ev_set = false;
   cudaEvent_t copy_ev = nullptr;   // uploads on the copy stream
   Pinned prof_desc;                // build descriptors on their way to the device
+  Pinned prof_stage[2];            // pageable rows staged on their way to the device
+  cudaEvent_t prof_stage_ev[2] = {};
+  bool prof_stage_used[2] = {};
   static constexpr int kMetaRing = 4;
   Pinned meta_pin[kMetaRing];      // profile tables on their way to the device
   cudaEvent_t meta_ev[kMetaRing] = {};
@@ -540,6 +553,8 @@ extern "C" void st_shutdown(st_ctx* c) {
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
   for (auto e : c->meta_ev)
     if (e) cudaEventDestroy(e);
+  for (auto e : c->prof_stage_ev)
+    if (e) cudaEventDestroy(e);
   delete c;
   cudaStreamDestroy(own);
 }
@@ -709,20 +724,52 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   // stream after both. The call returns once the rows and descriptors are on
   // the device (the caller may reuse them), not when the build is done: later
   // work on the profiles is ordered after it.
-  if (src_bytes)
-    ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->copy));
-  // score range per profile (residues >= 21 score 0), in parallel over profiles
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) {
+  // score range of profile k (residues >= 21 score 0); with dst, the rows are copied there in the same pass
+  auto range_of = [&](int64_t k, int32_t* dst) {
     const uint64_t m = desc[k].m;
     int32_t lo = 0, hi = 0;
     const int32_t* r = rows + row_offsets[k] * kAlpha;
     for (size_t i = 0; i < m * kAlpha; ++i) {
-      lo = std::min(lo, r[i]);
-      hi = std::max(hi, r[i]);
+      const int32_t v = r[i];
+      if (dst) dst[i] = v;
+      lo = std::min(lo, v);
+      hi = std::max(hi, v);
     }
     mx[k] = hi;
     desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
+  };
+  if (src_bytes && host_pinned(rows)) {
+    ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->copy));
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) range_of(k, nullptr);
+  } else if (src_bytes) {
+    // pageable rows: copied (with the range pass) into two pinned blocks in
+    // turn, each uploaded while the next fills
+    constexpr size_t kChunk = 32ull << 20;
+    uint32_t k0 = 0;
+    int slot = 0;
+    while (k0 < n_profiles) {
+      uint32_t k1 = k0 + 1;
+      while (k1 < n_profiles && (row_offsets[k1 + 1] - row_offsets[k0]) * kAlpha * 4 <= kChunk) ++k1;
+      const size_t r0 = row_offsets[k0] - row_offsets[0];
+      const size_t bytes = (row_offsets[k1] - row_offsets[k0]) * kAlpha * 4;
+      Pinned& st = c->prof_stage[slot];
+      if (!c->prof_stage_ev[slot]) ST_CUDA(cudaEventCreateWithFlags(&c->prof_stage_ev[slot], cudaEventDisableTiming));
+      if (c->prof_stage_used[slot]) ST_CUDA(cudaEventSynchronize(c->prof_stage_ev[slot]));
+      ST_TRY(st.reserve(std::max(bytes, kChunk)));
+      int32_t* h = st.as<int32_t>();
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int64_t k = k0; k < static_cast<int64_t>(k1); ++k)
+        range_of(k, h + (row_offsets[k] - row_offsets[k0]) * kAlpha);
+      ST_CUDA(cudaMemcpyAsync(d_src + r0 * kAlpha, h, bytes, cudaMemcpyHostToDevice, c->copy));
+      ST_CUDA(cudaEventRecord(c->prof_stage_ev[slot], c->copy));
+      c->prof_stage_used[slot] = true;
+      slot ^= 1;
+      k0 = k1;
+    }
+  } else {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) range_of(k, nullptr);
   }
   tc.lap("range");
   ST_TRY(c->prof_desc.reserve(n_profiles * sizeof(ProfBuildDesc)));
@@ -1602,15 +1649,6 @@ extern "C" void st_plan_destroy(st_plan* p) {
   plan_free(p);
 }
 
-static bool host_pinned(const void* p) {
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();  // not a CUDA-known pointer: pageable
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
-}
-
 // Pipelining of large batches: chunks of about 320K pairs (ST_PIPELINE_PAIRS
 // overrides; 0 turns pipelining off), the first two a quarter and a half of
 // that so the GPU starts early, rotating over side streams
@@ -2068,8 +2106,25 @@ extern "C" int st_sw_score_pairs_async(st_ctx* c, const st_pair* pairs, uint64_t
 extern "C" int st_batch_wait(st_batch* batch) {
   if (!batch) return fail(ST_EINVAL, "st_batch_wait: null batch");
   st_ctx* c = batch->c;
+  if (batch->done) {  // wait without holding the context, so other threads can use it meanwhile
+    cudaSetDevice(c->device);
+    cudaEventSynchronize(batch->done);
+  }
   CTX_GUARD(c);
   return batch_finish(batch);
+}
+
+extern "C" int st_batch_query(st_batch* batch) {
+  if (!batch) return fail(ST_EINVAL, "st_batch_query: null batch");
+  if (!batch->done) return ST_OK;
+  cudaSetDevice(batch->c->device);
+  const cudaError_t e = cudaEventQuery(batch->done);
+  if (e == cudaSuccess) return ST_OK;
+  if (e == cudaErrorNotReady) {
+    cudaGetLastError();
+    return 1;
+  }
+  return fail(ST_ECUDA, "batch failed: %s", cudaGetErrorString(e));
 }
 
 extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,

@@ -1,0 +1,353 @@
+// Serving loop: continuous batching of scoring requests on one context.
+//
+// A request is one query (its int32 [m][21] rows) and the database targets
+// to score it against (optionally banded). Client threads submit requests at
+// any time and wait for them by id. One worker thread forms batches from
+// the requests that have arrived, in arrival order, up to a pair cap and a
+// device-memory budget; it keeps two batches in flight: while one runs on
+// the GPU the next is built (profiles uploaded, pairs filled) and launched,
+// so requests that arrive during a batch join the next one and their work
+// overlaps the running one on the device. Results are the same as scoring
+// each request alone: every pair's score depends only on its own inputs.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/sabertooth_b200.h"
+
+__attribute__((visibility("hidden"))) void st_internal_set_error(const char* msg);
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t id = 0;
+  uint32_t m = 0;
+  std::vector<int32_t> rows;
+  std::vector<st_pair> pairs;  // profile field filled when batched
+  std::vector<int32_t> scores;
+  Clock::time_point t_submit, t_done;
+  bool done = false;
+  int status = ST_OK;
+  std::string error;
+  uint64_t bytes = 0;  // device-memory estimate while in flight
+};
+
+struct Batch {
+  std::vector<std::shared_ptr<Request>> reqs;
+  std::vector<uint32_t> ids;  // profile ids
+  std::vector<st_pair> pairs;
+  std::vector<int32_t> scores;
+  st_batch* handle = nullptr;
+  uint64_t bytes = 0;
+};
+
+// Device bytes a request holds while in flight: its profile layouts (int8
+// and int32, rounded as the library stores them) and per-pair plan buffers.
+uint64_t request_bytes(uint32_t m, uint64_t n_pairs) {
+  const uint64_t s8 = ((m + 15) / 16) * 16, s32 = std::max<uint64_t>(((m + 255) / 256) * 256, 256);
+  return 22 * s8 + 22 * 4 * s32 + 4096 + n_pairs * 256;
+}
+
+}  // namespace
+
+struct st_server {
+  st_ctx* ctx = nullptr;
+  int32_t open = 0, ext = 0;
+  uint64_t max_pairs = 0, budget = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<Request>> pending;
+  std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  uint64_t batches = 0, batched_pairs = 0;
+  int32_t* arena = nullptr;  // pinned rows of the batch being launched (uploaded before the next one fills it)
+  size_t arena_bytes = 0;
+
+  void run();
+  void finish(std::unique_ptr<Batch>& b);
+  int launch(std::unique_ptr<Batch>& b);
+};
+
+// Builds a batch's profiles and pairs and launches it; on failure every
+// request of the batch completes with the error.
+int st_server::launch(std::unique_ptr<Batch>& b) {
+  std::vector<uint64_t> offs(b->reqs.size() + 1, 0);
+  for (size_t i = 0; i < b->reqs.size(); ++i) offs[i + 1] = offs[i] + b->reqs[i]->m;
+  const size_t need = std::max<size_t>(static_cast<size_t>(offs.back()) * 21 * 4, 64);
+  if (arena_bytes < need) {
+    if (arena) cudaFreeHost(arena);
+    arena = nullptr;
+    arena_bytes = 0;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&arena), need + need / 4, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      st_internal_set_error("serving: pinned host allocation failed");
+      return ST_ENOMEM;
+    }
+    arena_bytes = need + need / 4;
+  }
+  size_t n_pairs = 0;
+  for (size_t i = 0; i < b->reqs.size(); ++i) n_pairs += b->reqs[i]->pairs.size();
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < static_cast<int64_t>(b->reqs.size()); ++i)
+    if (b->reqs[i]->m) memcpy(arena + offs[i] * 21, b->reqs[i]->rows.data(), b->reqs[i]->rows.size() * 4);
+  b->ids.assign(b->reqs.size(), 0);
+  int rc = st_profiles_create(ctx, arena, offs.data(), static_cast<uint32_t>(b->reqs.size()), b->ids.data());
+  if (rc != ST_OK) return rc;
+  b->pairs.reserve(n_pairs);
+  for (size_t i = 0; i < b->reqs.size(); ++i)
+    for (st_pair p : b->reqs[i]->pairs) {
+      p.profile = b->ids[i];
+      b->pairs.push_back(p);
+    }
+  b->scores.assign(n_pairs, 0);
+  rc = st_sw_score_pairs_async(ctx, b->pairs.data(), n_pairs, open, ext, b->scores.data(), nullptr, &b->handle);
+  if (rc != ST_OK) {
+    st_profiles_free(ctx, b->ids.data(), static_cast<uint32_t>(b->ids.size()));
+    b->ids.clear();
+  }
+  return rc;
+}
+
+void st_server::finish(std::unique_ptr<Batch>& b) {
+  int rc = ST_OK;
+  std::string err;
+  if (b->handle) {
+    rc = st_batch_wait(b->handle);
+    if (rc != ST_OK) err = st_last_error();
+  }
+  if (!b->ids.empty()) st_profiles_free(ctx, b->ids.data(), static_cast<uint32_t>(b->ids.size()));
+  const Clock::time_point now = Clock::now();
+  std::lock_guard<std::mutex> lk(mu);
+  size_t at = 0;
+  for (auto& r : b->reqs) {
+    r->scores.assign(b->scores.begin() + at, b->scores.begin() + at + r->pairs.size());
+    at += r->pairs.size();
+    r->status = rc;
+    r->error = err;
+    r->t_done = now;
+    r->done = true;
+  }
+  ++batches;
+  batched_pairs += at;
+  cv_done.notify_all();
+}
+
+void st_server::run() {
+  std::deque<std::unique_ptr<Batch>> inflight;
+  uint64_t inflight_bytes = 0;
+  for (;;) {
+    std::unique_ptr<Batch> b;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      if (inflight.empty()) {
+        cv_work.wait(lk, [&] { return stop || !pending.empty(); });
+      } else if (inflight.size() == 1 && pending.empty()) {
+        // one batch running and nothing waiting: watch for arrivals and for the batch's end
+        cv_work.wait_for(lk, std::chrono::microseconds(200), [&] { return stop || !pending.empty(); });
+        if (pending.empty() && st_batch_query(inflight.front()->handle) == 1) continue;
+      }
+      if (stop && pending.empty() && inflight.empty()) return;
+      if (inflight.size() < 2 && !pending.empty()) {
+        // arrival order, up to the pair cap and the memory left beside the batches in flight
+        b.reset(new Batch);
+        uint64_t pairs = 0;
+        while (!pending.empty()) {
+          const auto& r = pending.front();
+          const bool first = b->reqs.empty();
+          if (!first && (pairs + r->pairs.size() > max_pairs || inflight_bytes + b->bytes + r->bytes > budget)) break;
+          pairs += r->pairs.size();
+          b->bytes += r->bytes;
+          b->reqs.push_back(r);
+          pending.pop_front();
+        }
+      }
+    }
+    if (b) {
+      const int rc = launch(b);
+      if (rc != ST_OK) {
+        b->handle = nullptr;
+        const std::string err = st_last_error();
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& r : b->reqs) {
+          r->status = rc;
+          r->error = err;
+          r->t_done = Clock::now();
+          r->done = true;
+        }
+        cv_done.notify_all();
+      } else {
+        inflight_bytes += b->bytes;
+        inflight.push_back(std::move(b));
+      }
+      // with one batch in flight, build the next at once if requests are waiting
+      std::lock_guard<std::mutex> lk(mu);
+      if (inflight.size() < 2 && !pending.empty()) continue;
+    }
+    if (!inflight.empty()) {
+      inflight_bytes -= inflight.front()->bytes;
+      finish(inflight.front());
+      inflight.pop_front();
+    }
+  }
+}
+
+extern "C" st_server* st_server_create(st_ctx* ctx, int32_t open, int32_t ext, uint64_t max_batch_pairs,
+                                       uint64_t hbm_budget_bytes) {
+  if (!ctx) {
+    st_internal_set_error("st_server_create: null context");
+    return nullptr;
+  }
+  auto s = std::make_unique<st_server>();
+  s->ctx = ctx;
+  s->open = open;
+  s->ext = ext;
+  s->max_pairs = max_batch_pairs ? max_batch_pairs : (1ull << 22);
+  s->budget = hbm_budget_bytes ? hbm_budget_bytes : (16ull << 30);
+  st_server* p = s.get();
+  s->worker = std::thread([p] { p->run(); });
+  return s.release();
+}
+
+extern "C" int st_server_submit(st_server* s, const int32_t* rows, uint32_t m, const uint32_t* targets,
+                                const int32_t* band_center, const int32_t* band_radius, uint32_t n,
+                                uint64_t* request_id) {
+  if (!s || !request_id || (m && !rows) || (n && !targets)) {
+    st_internal_set_error("st_server_submit: null argument");
+    return ST_EINVAL;
+  }
+  auto r = std::make_shared<Request>();
+  r->m = m;
+  r->rows.assign(rows, rows + static_cast<size_t>(m) * 21);
+  r->pairs.resize(n);
+  for (uint32_t i = 0; i < n; ++i)
+    r->pairs[i] = st_pair{0, targets[i], band_center ? band_center[i] : 0, band_radius ? band_radius[i] : -1};
+  r->bytes = request_bytes(m, n);
+  if (r->bytes > s->budget) {
+    st_internal_set_error("st_server_submit: request needs more device memory than the server's budget");
+    return ST_ENOMEM;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) {
+    st_internal_set_error("st_server_submit: server is stopping");
+    return ST_ESTATE;
+  }
+  r->id = s->next_id++;
+  r->t_submit = Clock::now();
+  s->live[r->id] = r;
+  s->pending.push_back(r);
+  *request_id = r->id;
+  s->cv_work.notify_one();
+  return ST_OK;
+}
+
+extern "C" int st_server_submit_many(st_server* s, uint32_t n_requests, const int32_t* rows, const uint64_t* row_offsets,
+                                     const uint32_t* targets, const uint64_t* target_offsets, const int32_t* band_center,
+                                     const int32_t* band_radius, uint64_t* request_ids) {
+  if (!s || !request_ids || (n_requests && (!row_offsets || !target_offsets))) {
+    st_internal_set_error("st_server_submit_many: null argument");
+    return ST_EINVAL;
+  }
+  for (uint32_t k = 0; k < n_requests; ++k) {
+    const uint64_t r0 = row_offsets[k], r1 = row_offsets[k + 1], t0 = target_offsets[k], t1 = target_offsets[k + 1];
+    if (r1 < r0 || t1 < t0 || (r1 > r0 && !rows) || (t1 > t0 && !targets)) {
+      st_internal_set_error("st_server_submit_many: bad offsets");
+      return ST_EINVAL;
+    }
+    if (request_bytes(static_cast<uint32_t>(r1 - r0), t1 - t0) > s->budget) {
+      st_internal_set_error("st_server_submit_many: a request needs more device memory than the server's budget");
+      return ST_ENOMEM;
+    }
+  }
+  std::vector<std::shared_ptr<Request>> rs(n_requests);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < static_cast<int64_t>(n_requests); ++k) {
+    auto r = std::make_shared<Request>();
+    const uint64_t r0 = row_offsets[k], r1 = row_offsets[k + 1], t0 = target_offsets[k], t1 = target_offsets[k + 1];
+    r->m = static_cast<uint32_t>(r1 - r0);
+    r->rows.assign(rows + r0 * 21, rows + r1 * 21);
+    r->pairs.resize(t1 - t0);
+    for (uint64_t i = t0; i < t1; ++i)
+      r->pairs[i - t0] = st_pair{0, targets[i], band_center ? band_center[i] : 0, band_radius ? band_radius[i] : -1};
+    r->bytes = request_bytes(r->m, t1 - t0);
+    rs[k] = std::move(r);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) {
+    st_internal_set_error("st_server_submit_many: server is stopping");
+    return ST_ESTATE;
+  }
+  const Clock::time_point now = Clock::now();
+  for (uint32_t k = 0; k < n_requests; ++k) {
+    rs[k]->id = s->next_id++;
+    rs[k]->t_submit = now;
+    s->live[rs[k]->id] = rs[k];
+    s->pending.push_back(rs[k]);
+    request_ids[k] = rs[k]->id;
+  }
+  s->cv_work.notify_one();
+  return ST_OK;
+}
+
+extern "C" int st_server_wait(st_server* s, uint64_t request_id, int32_t* scores, uint32_t cap, double* latency_ms) {
+  if (!s) {
+    st_internal_set_error("st_server_wait: null server");
+    return ST_EINVAL;
+  }
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->live.find(request_id);
+    if (it == s->live.end()) {
+      st_internal_set_error("st_server_wait: unknown request id");
+      return ST_EINVAL;
+    }
+    r = it->second;
+    s->cv_done.wait(lk, [&] { return r->done; });
+    s->live.erase(request_id);
+  }
+  if (r->status != ST_OK) {
+    st_internal_set_error(r->error.c_str());
+    return r->status;
+  }
+  if (scores) memcpy(scores, r->scores.data(), std::min<size_t>(cap, r->scores.size()) * 4);
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+  return ST_OK;
+}
+
+extern "C" int st_server_stats(st_server* s, uint64_t* batches, uint64_t* pairs) {
+  if (!s) {
+    st_internal_set_error("st_server_stats: null server");
+    return ST_EINVAL;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (batches) *batches = s->batches;
+  if (pairs) *pairs = s->batched_pairs;
+  return ST_OK;
+}
+
+extern "C" void st_server_destroy(st_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  if (s->arena) cudaFreeHost(s->arena);
+  delete s;
+}

@@ -178,6 +178,14 @@ class SwWorkload:
             tot += band_cells(int(m[k]), int(n[k]), int(self.band_center[k]), int(self.band_radius[k]))
         return tot
 
+    def cells_of(self, i):
+        """Cells of pair i (m*n, or band cells for a banded pair)."""
+        m = len(self.rows[int(self.pair_q[i])])
+        n = int(self.db_offsets[int(self.pair_t[i]) + 1] - self.db_offsets[int(self.pair_t[i])])
+        if self.band_radius is None or self.band_radius[i] < 0:
+            return m * n
+        return band_cells(m, n, int(self.band_center[i]), int(self.band_radius[i]))
+
 
 def band_cells(m, n, center, radius):
     i = np.arange(1, m + 1, dtype=np.int64)
