@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--plain-pairs", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--serving-pairs", type=int, default=20000, help="config-4 requests for the serving measurement (0: skip)")
+    ap.add_argument("--ungapped-hits", type=int, default=20_000_000, help="config-2 hits for the ungapped measurement (0: skip)")
     ap.add_argument("--serving-seconds", type=float, default=2.0, help="arrival window per swept rate")
     return ap.parse_args()
 
@@ -130,9 +131,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_traffic():
-    """Per-launch DRAM traffic of the dominant kernel from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "sw16_pssm_config3.md")
+def read_traffic(name="sw16_pssm_config3.md"):
+    """Per-launch DRAM traffic of a kernel from its committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for ln in open(p):
@@ -423,6 +424,8 @@ def main():
             "step_ms_min_max": [round(min(step_ms), 3), round(max(step_ms), 3)],
         }
     plan.close()
+    if result is not None and args.ungapped_hits > 0:
+        result["ungapped"] = ungapped_measure(ctx, args)
     if result is not None and args.serving_pairs > 0:
         result["serving"] = serving_measure(ctx, args)
     if world > 1:
@@ -432,6 +435,84 @@ def main():
     if result is not None:
         print(json.dumps(result), flush=True)
     return 0
+
+
+def ungapped_measure(ctx, args):
+    """Row (U): ungapped diagonal scoring of prefilter seed hits (config 2: 1,000 queries, 374,000 targets,
+    68 M residues, 2x10^7 hits, 30% on planted-homolog diagonals). Hits resident on the device; per step one
+    st_ungapped_hits_device call (per-hit best + per-(query, target) best). Roofline: algorithmic bytes
+    (window residues + 12 B hit + 4 B output per hit) / time against the measured HBM copy bandwidth."""
+    import torch
+    from oracle import oracle as O
+    from sabertooth_b200 import workloads as W
+    t0 = time.perf_counter()
+    w = W.config2(seed=args.seed, n_hits=args.ungapped_hits)
+    t_gen = time.perf_counter() - t0
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    hits = w.hits.copy()
+    hits["query"] = ids[hits["query"]]
+    n = len(hits)
+    st = torch.cuda.Stream()
+    ctx.set_stream(st.cuda_stream)
+    d_hits = torch.from_numpy(hits.view(np.uint8)).cuda()
+    d_out = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_pb = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_pq = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_pt = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_np = torch.zeros(1, dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ab = w.algorithmic_bytes()
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            ctx.ungapped_hits_device(d_hits.data_ptr(), n, d_out.data_ptr(), d_pb.data_ptr(), d_pq.data_ptr(),
+                                     d_pt.data_ptr(), d_np.data_ptr())
+        ts = []
+        for _ in range(max(3, args.steps)):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            ctx.ungapped_hits_device(d_hits.data_ptr(), n, d_out.data_ptr(), d_pb.data_ptr(), d_pq.data_ptr(),
+                                     d_pt.data_ptr(), d_np.data_ptr())
+            b.record(st)
+            st.synchronize()
+            ts.append(a.elapsed_time(b))
+    ctx.set_stream(0)
+    ms = float(np.median(ts))
+    got = d_out.cpu().numpy()
+    n_runs = int(d_np.item())
+    # parity and the CPU baseline on a sample (the oracle: scalar Kadane, all host cores)
+    rng = np.random.default_rng(args.seed)
+    sel = np.sort(rng.choice(n, min(n, 2_000_000), replace=False))
+    targets = [w.db_residues[int(a_):int(b_)] for a_, b_ in zip(w.db_offsets[:-1], w.db_offsets[1:])]
+    arena = O.Arena(w.rows, targets)
+    t0 = time.perf_counter()
+    want = O.ungapped_hits(arena, w.hits["query"][sel], w.hits["target"][sel], w.hits["diag"][sel])
+    t_cpu = time.perf_counter() - t0
+    peak = hbm_peak_gbs()
+    gbs = ab / (ms * 1e-3) / 1e9
+    ctx.free_profiles(ids)
+    return {"workload": f"config 2: {len(w.rows)} queries, {len(w.db_offsets) - 1} targets "
+                        f"({int(w.db_offsets[-1]) / 1e6:.1f} M residues), {n} hits (30% homolog diagonals)",
+            "ms_per_step": round(ms, 3), "mhits_per_s": round(n / ms / 1e3, 1),
+            "algorithmic_bytes": int(ab), "runs": n_runs,
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "traffic": read_traffic("ungapped_config2.md")},
+            "matches_oracle_sample": bool(np.array_equal(got[sel], want)),
+            "cpu_baseline": {"value": round(len(sel) / t_cpu / 1e6, 2), "unit": "Mhits/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"{len(sel)} random hits of the workload, scalar Kadane "
+                                                       "(the reference's kadane_score restated in C), OpenMP"},
+            "setup_s": round(t_gen, 1)}
+
+
+def hbm_peak_gbs():
+    """The measured copy bandwidth of this pool's B200s, or the fallback figure."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"])
+    except Exception:
+        return 6650.0
 
 
 def serving_measure(ctx, args):

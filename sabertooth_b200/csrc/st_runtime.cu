@@ -25,7 +25,9 @@
 #include "st_dplan.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/iterator/transform_input_iterator.cuh>
 
 using namespace st;
 
@@ -464,6 +466,7 @@ static DeviceProfiles prof_view(st_ctx* c) {
 }
 
 static int g_class_smem[kNumClasses];  // dynamic shared memory each 16-bit class may use
+static int g_ung_smem = 0;              // dynamic shared memory the ungapped kernels may use
 
 static int set_smem_limits(int device) {
   int optin = 0;
@@ -474,8 +477,12 @@ static int set_smem_limits(int device) {
     g_class_smem[i] = std::min<int>(kMaxSmem, optin - static_cast<int>(fa.sharedSizeBytes));
     ST_CUDA(cudaFuncSetAttribute(kClasses[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, g_class_smem[i]));
   }
-  ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
-  ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
+  cudaFuncAttributes fa_t, fa_f;
+  ST_CUDA(cudaFuncGetAttributes(&fa_t, reinterpret_cast<const void*>(ungapped_kernel<true>)));
+  ST_CUDA(cudaFuncGetAttributes(&fa_f, reinterpret_cast<const void*>(ungapped_kernel<false>)));
+  g_ung_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(std::max(fa_t.sharedSizeBytes, fa_f.sharedSizeBytes)));
+  ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
+  ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
   return ST_OK;
 }
 
@@ -2421,7 +2428,8 @@ static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n,
   prm.out = d_out;
   prm.max_m_pad = ung_stride(c);
   const size_t smem = 16 + static_cast<size_t>(kProfRows) * prm.max_m_pad + 16;
-  if (smem > kMaxSmem) return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", c->max_m);
+  if (smem > static_cast<size_t>(g_ung_smem))
+    return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", c->max_m);
   const uint64_t grid = (n + kUngChunk - 1) / kUngChunk;
   if (grid > 0x7FFFFFFFull) return fail(ST_EINVAL, "too many ungapped jobs");
   if (hits)
@@ -2471,23 +2479,51 @@ extern "C" int st_ungapped_score(st_ctx* c, uint32_t profile, const st_lane* lan
   return ST_OK;
 }
 
+// Per-(query, target) runs of hits (consecutive hits with the same query and
+// target): one (best, query, target) entry per run, in hit order, by a
+// reduce-by-key over the packed (query, target) key. Asynchronous; the
+// scratch goes back to the pool behind the stream.
+struct HitPairKey {
+  __host__ __device__ uint64_t operator()(const HitRec& h) const {
+    return (static_cast<uint64_t>(h.query) << 32) | h.target;
+  }
+};
+struct MaxI32 {
+  __host__ __device__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
+};
+
+__global__ void __launch_bounds__(256) split_pair_keys_kernel(const uint64_t* keys, const uint64_t* n_runs,
+                                                              uint32_t* pair_q, uint32_t* pair_t, uint64_t* n_out) {
+  const uint64_t n = *n_runs;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = n;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t k = keys[i];
+    pair_q[i] = static_cast<uint32_t>(k >> 32);
+    pair_t[i] = static_cast<uint32_t>(k);
+  }
+}
+
 static int run_pairs_device(st_ctx* c, const st_hit* d_hits, uint64_t n, const int32_t* d_per_hit,
                             int32_t* d_pair_best, uint32_t* d_pair_q, uint32_t* d_pair_t, uint64_t* d_n_pairs) {
-  const uint64_t nb = (n + kRunBlock - 1) / kRunBlock;
-  if (nb > 0xFFFFFFFFull) return fail(ST_EINVAL, "too many hits");
-  DevMem tmp;
-  ST_TRY(dev_alloc(&c->mt, tmp, nb * 12 + 16));
-  uint32_t* counts = tmp.as<uint32_t>();
-  uint64_t* offs = reinterpret_cast<uint64_t*>(tmp.as<char>() + up16(nb * 4));
   const HitRec* h = reinterpret_cast<const HitRec*>(d_hits);
-  run_count_kernel<<<static_cast<uint32_t>(nb), kRunBlock, 0, c->stream>>>(h, n, counts);
-  run_scan_kernel<<<1, 1024, 0, c->stream>>>(counts, static_cast<uint32_t>(nb), offs, d_n_pairs);
-  run_write_kernel<<<static_cast<uint32_t>(nb), kRunBlock, 0, c->stream>>>(h, n, d_per_hit, offs, d_pair_best,
-                                                                            d_pair_q, d_pair_t);
-  c->launches += 3;
+  cub::TransformInputIterator<uint64_t, HitPairKey, const HitRec*> keys(h, HitPairKey());
+  size_t t_bytes = 0;
+  ST_CUDA(cub::DeviceReduce::ReduceByKey(nullptr, t_bytes, keys, static_cast<uint64_t*>(nullptr), d_per_hit,
+                                         d_pair_best, static_cast<uint64_t*>(nullptr), MaxI32(), n, c->stream));
+  DevMem tmp;
+  const size_t o_keys = 0, o_runs = up256(n * 8), o_cub = o_runs + 256;
+  ST_TRY(pool_get(c, o_cub + t_bytes, tmp));
+  char* b = tmp.as<char>();
+  uint64_t* ukeys = reinterpret_cast<uint64_t*>(b + o_keys);
+  uint64_t* runs = reinterpret_cast<uint64_t*>(b + o_runs);
+  ST_CUDA(cub::DeviceReduce::ReduceByKey(b + o_cub, t_bytes, keys, ukeys, d_per_hit, d_pair_best, runs, MaxI32(), n,
+                                         c->stream));
+  const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(c->sms) * 8));
+  split_pair_keys_kernel<<<grid, 256, 0, c->stream>>>(ukeys, runs, d_pair_q, d_pair_t, d_n_pairs);
+  ++c->launches;
   ST_CUDA(cudaGetLastError());
-  // tmp must outlive the kernels
-  ST_CUDA(cudaStreamSynchronize(c->stream));
+  pool_put_after(c, std::move(tmp), c->stream);
   return ST_OK;
 }
 
@@ -2532,7 +2568,12 @@ extern "C" int st_ungapped_hits(st_ctx* c, const st_hit* hits, uint64_t n, int32
   DevMem buf;
   const size_t hb = up16(n * sizeof(st_hit));
   const size_t ob = up16(n * 4);
-  ST_TRY(dev_alloc(&c->mt, buf, hb + ob + (want_pairs ? 3 * ob + 16 : 0)));
+  ST_TRY(pool_get(c, hb + ob + (want_pairs ? 3 * ob + 16 : 0), buf));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
+  } back{c, &buf};
   char* d = buf.as<char>();
   ST_CUDA(cudaMemcpyAsync(d, hits, n * sizeof(st_hit), cudaMemcpyHostToDevice, c->stream));
   int32_t* d_out = reinterpret_cast<int32_t*>(d + hb);

@@ -129,7 +129,26 @@ __global__ void __launch_bounds__(256) ungapped_kernel(const UngappedParams prm)
       int64_t lo, hi;
       ung_job<HITS>(prm, k, qq, tt, d, lo, hi);
       int32_t best = 0, cur = 0;
-      if (hi > lo) {
+      if (HITS && hi > lo && narrow) {
+        // Whole-diagonal windows (hits) on int8 profiles: every cell of a vector outside [lo, hi) scores
+        // 0 on its own: query rows before 0 or from m read the zero guard bytes and padding of the staged
+        // rows, target positions from n hold the sentinel code, whose row is zero. Zero cells at either
+        // end of the window cannot change Kadane's maximum, so whole vectors are scored without a test.
+        const uint8_t* tp = prm.db.arena + prm.db.offset[tt];
+        const int32_t p0 = static_cast<int32_t>(lo) + d, p1 = static_cast<int32_t>(hi) + d;
+        for (int32_t pa = p0 & ~15; pa < p1; pa += 16) {
+          const uint4 v = *reinterpret_cast<const uint4*>(tp + pa);
+          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+          const int8_t* rowbase = base + (pa - d);
+#pragma unroll
+          for (int bb = 0; bb < 16; ++bb) {
+            const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+            const int32_t sc = rowbase[static_cast<int32_t>(r * stride) + bb];
+            cur = wadd(max(cur, 0), sc);
+            best = max(best, cur);
+          }
+        }
+      } else if (hi > lo) {
         const uint8_t* tp = prm.db.arena + prm.db.offset[tt];
         // target positions [p0, p1); sequences are shorter than 2^31
         const int32_t p0 = static_cast<int32_t>(lo) + d, p1 = static_cast<int32_t>(hi) + d;
@@ -161,83 +180,6 @@ __global__ void __launch_bounds__(256) ungapped_kernel(const UngappedParams prm)
     }
     __syncthreads();
     a = b;
-  }
-}
-
-// ---- per-(query, target) runs of hits ------------------------------------
-// A run starts at hit k when k == 0 or (query, target) differs from hit k-1.
-// Three deterministic phases: count run starts per block, scan the counts,
-// then write one (best, query, target) entry per run in hit order.
-constexpr int kRunBlock = 1024;
-
-__device__ __forceinline__ bool run_start(const HitRec* h, uint64_t k) {
-  if (k == 0) return true;
-  const HitRec a = h[k - 1], b = h[k];
-  return a.query != b.query || a.target != b.target;
-}
-
-__global__ void __launch_bounds__(kRunBlock) run_count_kernel(const HitRec* h, uint64_t n, uint32_t* counts) {
-  __shared__ uint32_t s_cnt;
-  if (threadIdx.x == 0) s_cnt = 0;
-  __syncthreads();
-  const uint64_t k = static_cast<uint64_t>(blockIdx.x) * kRunBlock + threadIdx.x;
-  const bool st = k < n && run_start(h, k);
-  const uint32_t ball = __ballot_sync(0xFFFFFFFFu, st);
-  if ((threadIdx.x & 31) == 0 && ball) atomicAdd(&s_cnt, __popc(ball));
-  __syncthreads();
-  if (threadIdx.x == 0) counts[blockIdx.x] = s_cnt;
-}
-
-// exclusive scan of counts[0..nb) in one CTA; writes offsets and the total
-__global__ void __launch_bounds__(1024) run_scan_kernel(const uint32_t* counts, uint32_t nb, uint64_t* offsets,
-                                                        uint64_t* total) {
-  __shared__ uint64_t s_part[1024];
-  __shared__ uint64_t s_carry;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
-  for (uint32_t base = 0; base < nb; base += 1024) {
-    const uint32_t i = base + threadIdx.x;
-    const uint64_t v = i < nb ? counts[i] : 0;
-    s_part[threadIdx.x] = v;
-    __syncthreads();
-    for (uint32_t o = 1; o < 1024; o <<= 1) {
-      const uint64_t add = threadIdx.x >= o ? s_part[threadIdx.x - o] : 0;
-      __syncthreads();
-      s_part[threadIdx.x] += add;
-      __syncthreads();
-    }
-    if (i < nb) offsets[i] = s_carry + s_part[threadIdx.x] - v;
-    __syncthreads();
-    if (threadIdx.x == 1023) s_carry += s_part[1023];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *total = s_carry;
-}
-
-__global__ void __launch_bounds__(kRunBlock) run_write_kernel(const HitRec* h, uint64_t n, const int32_t* per_hit,
-                                                              const uint64_t* offsets, int32_t* pair_best,
-                                                              uint32_t* pair_query, uint32_t* pair_target) {
-  __shared__ uint32_t s_warp[kRunBlock / 32];
-  const uint64_t k = static_cast<uint64_t>(blockIdx.x) * kRunBlock + threadIdx.x;
-  const bool st = k < n && run_start(h, k);
-  const uint32_t ball = __ballot_sync(0xFFFFFFFFu, st);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) s_warp[warp] = __popc(ball);
-  __syncthreads();
-  if (st) {
-    uint32_t pos = __popc(ball & ((1u << lane) - 1u));
-    for (int w = 0; w < warp; ++w) pos += s_warp[w];
-    const uint64_t o = offsets[blockIdx.x] + pos;
-    const HitRec a = h[k];
-    int32_t b = per_hit[k];
-    for (uint64_t j = k + 1; j < n; ++j) {
-      const HitRec c = h[j];
-      if (c.query != a.query || c.target != a.target) break;
-      b = max(b, per_hit[j]);
-    }
-    pair_best[o] = b;
-    pair_query[o] = a.query;
-    pair_target[o] = a.target;
   }
 }
 
