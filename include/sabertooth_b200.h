@@ -196,6 +196,25 @@ int st_ungapped_hits_device(st_ctx* ctx, const st_hit* d_hits, uint64_t n, int32
                             int32_t* d_pair_best, uint32_t* d_pair_query, uint32_t* d_pair_target,
                             uint64_t* d_n_pairs);
 
+/* ---- end cells and alignment spans ---------------------------------------
+ * Score plus end cell, the first optimum in column-major order (smallest target
+ * position, then smallest query position): QueryProfile::sw_score_end_with
+ * (src/simd.rs:301-326, tie rule :375-381).  Positions are 0-based and
+ * inclusive; -1 when the score is 0 (the reference returns None).  Computed by
+ * the exact 32-bit kernel.  Unbanded pairs only. */
+int st_sw_score_end(st_ctx* ctx, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
+                    int32_t* score, int32_t* q_end, int32_t* t_end);
+/* Batched: ends[2i], ends[2i+1] = (query end, target end) of pair i. */
+int st_sw_score_end_pairs(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* scores,
+                          int32_t* ends);
+/* End cell plus start cell of each pair's alignment: the two score passes of
+ * align_canonical (src/align.rs:848-866): the forward end pass, then the same
+ * pass over the query rows [0, q_end] and target [0, t_end], both reversed,
+ * whose end cell (a, b) gives the start (q_end - a, t_end - b).
+ * starts[2i], starts[2i+1] = (query start, target start). */
+int st_sw_align_span_pairs(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                           int32_t* scores, int32_t* ends, int32_t* starts);
+
 /* ---- tile classes and autotuning ----------------------------------------- */
 /* The packed 16-bit kernel runs in tile classes: G lanes per alignment x R
  * query rows per lane x C target columns per wavefront step.  In a batch each

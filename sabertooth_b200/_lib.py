@@ -58,6 +58,9 @@ SIGNATURES = {
     "st_profiles_free": (C.c_int, [_P, _P, _u32]),
     "st_sw_score_pairs_async": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P, _P]),
     "st_batch_wait": (C.c_int, [_P]),
+    "st_sw_score_end": (C.c_int, [_P, _u32, _P, _u32, _i32, _i32, _P, _P, _P]),
+    "st_sw_score_end_pairs": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P]),
+    "st_sw_align_span_pairs": (C.c_int, [_P, _P, _u64, _i32, _i32, _P, _P, _P]),
     "st_batch_query": (C.c_int, [_P]),
     "st_server_create": (_P, [_P, _i32, _i32, _u64, _u64]),
     "st_server_submit": (C.c_int, [_P, _P, _u32, _P, _P, _P, _u32, _P]),

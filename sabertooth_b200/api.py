@@ -158,6 +158,29 @@ class Context:
                                         ptr(kernels)))
         return (scores, kernels) if with_kernels else scores
 
+    def sw_score_end_pairs(self, pairs, gaps: GapCosts):
+        """(scores, ends[n, 2]): score and end cell (query, target; -1 for a zero score) of every pair."""
+        pairs = as_pairs(pairs)
+        n = len(pairs)
+        scores = np.zeros(n, dtype=np.int32)
+        ends = np.zeros((n, 2), dtype=np.int32)
+        if n:
+            check(lib.st_sw_score_end_pairs(self._h, ptr(pairs), n, gaps.open, gaps.extend, ptr(scores), ptr(ends)))
+        return scores, ends
+
+    def align_span_pairs(self, pairs, gaps: GapCosts):
+        """(scores, starts[n, 2], ends[n, 2]): the alignment span of every pair (align_canonical's two score
+        passes); -1 for a zero score."""
+        pairs = as_pairs(pairs)
+        n = len(pairs)
+        scores = np.zeros(n, dtype=np.int32)
+        ends = np.zeros((n, 2), dtype=np.int32)
+        starts = np.zeros((n, 2), dtype=np.int32)
+        if n:
+            check(lib.st_sw_align_span_pairs(self._h, ptr(pairs), n, gaps.open, gaps.extend, ptr(scores), ptr(ends),
+                                             ptr(starts)))
+        return scores, starts, ends
+
     def sw_score_pairs_async(self, pairs, gaps: GapCosts, scores=None, kernels=None, with_kernels=False):
         """Starts scoring `pairs` and returns a Batch at once; Batch.wait() returns the scores
         (and kernel tags). `scores` / `kernels` may be given (for instance pinned arrays) and
@@ -434,6 +457,14 @@ class QueryProfile:
 
     def sw_score(self, target, gaps: GapCosts) -> int:
         return self.sw_score_with(target, gaps)[0]
+
+    def sw_score_end(self, target, gaps: GapCosts):
+        """QueryProfile::sw_score_end_with: (score, query end, target end), or None for a zero score."""
+        t = np.ascontiguousarray(target, dtype=np.uint8)
+        s, qe, te = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib.st_sw_score_end(self.ctx.handle, self.id, ptr(t) if t.size else None, t.size, gaps.open,
+                                  gaps.extend, C.byref(s), C.byref(qe), C.byref(te)))
+        return None if s.value <= 0 else (s.value, qe.value, te.value)
 
     def sw_score_with(self, target, gaps: GapCosts, scratch=None):
         """(score, Kernel) of one host target: the plain per-call drop-in."""

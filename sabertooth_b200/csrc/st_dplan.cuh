@@ -349,6 +349,10 @@ __global__ void __launch_bounds__(256) dp_gather_cta_kernel(const DpOut out) {
   if (i < out.n_cta) out.cta[i] = out.cta_raw[out.cta_idx_sorted[i]];
 }
 
+__global__ void __launch_bounds__(256) dp_iota_kernel(uint32_t* v, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
 __global__ void __launch_bounds__(256) dp_fill_zline_kernel(uint2* z, uint32_t n, uint32_t v) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) z[i] = make_uint2(0u, v);

@@ -963,6 +963,22 @@ struct st_plan {
   cudaGraphExec_t exec = nullptr;
 };
 
+static int occupancy_grid(st_ctx* c, const void* fn, int threads, size_t smem, uint32_t work, uint32_t* grid);
+
+// Grid of the 32-bit kernel: a few CTAs for the rare rescores; for a long
+// static list (banded pairs, wide rows, gap costs outside 16 bits) as many as
+// the SMs hold, bounded so its pass scratch stays within 1 GiB.
+static int grid_sw32(st_ctx* c, uint64_t n_static, uint32_t scratch_stride, uint32_t* grid) {
+  const uint64_t want = std::max<uint64_t>(2ull * c->sms, (n_static + kWarps32 - 1) / kWarps32);
+  ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0,
+                        static_cast<uint32_t>(std::min<uint64_t>(want, 1u << 20)), grid));
+  if (scratch_stride) {
+    const uint64_t cap = (1ull << 30) / (static_cast<uint64_t>(kWarps32) * scratch_stride * sizeof(int2));
+    *grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(*grid, cap)));
+  }
+  return ST_OK;
+}
+
 static int occupancy_grid(st_ctx* c, const void* fn, int threads, size_t smem, uint32_t work, uint32_t* grid) {
   int nb = 0;
   ST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem));
@@ -1381,12 +1397,9 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
                           static_cast<uint32_t>(cp.cta.size()), &cp.grid));
     cp.scratch_stride = multi ? max_cols : 0;
   }
-  // 32-bit kernel: a few persistent CTAs (rescoring is rare)
-  ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0,
-                        2 * c->sms, &plan->grid32));
-  plan->grid32 = std::min<uint32_t>(plan->grid32, 2 * c->sms);
   plan->scratch32_stride = max_m32 > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
   plan->n_static32 = static_cast<uint32_t>(list32.size());
+  ST_TRY(grid_sw32(c, plan->n_static32, plan->scratch32_stride, &plan->grid32));
 
   // one device arena: [initialised data (one upload)] [scratch]
   size_t off = 0;
@@ -1862,7 +1875,9 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   ST_CUDA(cudaGetLastError());
   c->launches += 5;
   DpTotals tot;
+  uint32_t n_list32 = 0;  // pairs the classify stage sent to the 32-bit kernel
   ST_CUDA(cudaMemcpyAsync(&tot, w.totals, sizeof(DpTotals), cudaMemcpyDeviceToHost, st));
+  ST_CUDA(cudaMemcpyAsync(&n_list32, w.list_count, 4, cudaMemcpyDeviceToHost, st));
   ST_CUDA(cudaStreamSynchronize(st));
   tc.lap("stage 1 (device)");
 
@@ -1888,10 +1903,8 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
     cp.scratch_stride = tot.max_cols_multi[k];
     plan->classes.push_back(std::move(cp));
   }
-  ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0, 2 * c->sms,
-                        &plan->grid32));
-  plan->grid32 = std::min<uint32_t>(plan->grid32, 2 * c->sms);
   plan->scratch32_stride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
+  ST_TRY(grid_sw32(c, n_list32, plan->scratch32_stride, &plan->grid32));
   size_t t_lpt = 0;
   {
     cub::DoubleBuffer<ull> ck(nullptr, nullptr);
@@ -2268,6 +2281,182 @@ extern "C" int st_sw_score_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, in
   copy_out();
   tc.lap("run+download");
   return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// end cells and alignment spans (sw_score_end_with + the reverse pass of
+// align_canonical), exact 32-bit kernel
+// ---------------------------------------------------------------------------
+// Scores n pairs (targets in `db`, unbanded) in end mode and, with `span`,
+// runs the reverse pass from each end cell. Outputs go to host buffers:
+// scores[i]; ends[2i..2i+1] = (query end, target end); with span,
+// starts[2i..2i+1] = (query start, target start); -1 where the score is 0.
+static int end_pairs_run(st_ctx* c, const DeviceDb& db, const uint32_t* pq_h, const uint32_t* pt_h, uint64_t n,
+                         uint32_t max_m, uint32_t max_len, int32_t open, int32_t ext, bool span, int32_t* scores,
+                         int32_t* ends, int32_t* starts) {
+  if (n == 0) return ST_OK;
+  if (n > 0xFFFFFFF0ull) return fail(ST_EINVAL, "too many pairs");
+  uint32_t grid = 0;
+  const uint32_t sstride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
+  ST_TRY(grid_sw32(c, n, sstride, &grid));
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~static_cast<size_t>(255);
+    return o;
+  };
+  const size_t o_pq = carve(n * 4), o_pt = carve(n * 4), o_zero = carve(n * 4), o_list = carve(n * 4),
+               o_cnt = carve(16), o_s = carve(n * 4), o_eq = carve(n * 4), o_et = carve(n * 4), o_rs = carve(n * 4),
+               o_sq = carve(n * 4), o_st = carve(n * 4),
+               o_scr = carve(sstride ? static_cast<size_t>(grid) * kWarps32 * sstride * sizeof(int2) : 16);
+  const size_t up_bytes = o_zero;  // pq, pt travel in one copy
+  DevMem a;
+  ST_TRY(pool_get(c, off, a));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
+  } back{c, &a};
+  char* d = a.as<char>();
+  ST_TRY(c->pin.reserve(up_bytes + 16));
+  ST_CUDA(cudaStreamSynchronize(c->stream));  // the pinned block may still feed an earlier copy
+  char* h = c->pin.as<char>();
+  memcpy(h + o_pq, pq_h, n * 4);
+  memcpy(h + o_pt, pt_h, n * 4);
+  ST_CUDA(cudaMemcpyAsync(d, h, up_bytes, cudaMemcpyHostToDevice, c->stream));
+  ST_CUDA(cudaMemsetAsync(d + o_zero, 0, n * 4, c->stream));
+  ST_CUDA(cudaMemsetAsync(d + o_cnt, 0, 16, c->stream));
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(d + o_cnt);  // [0] list count, [1], [2] work counters
+  const uint32_t n32 = static_cast<uint32_t>(n);
+  ST_CUDA(cudaMemcpyAsync(cnt, &n32, 4, cudaMemcpyHostToDevice, c->stream));
+  dp_iota_kernel<<<static_cast<uint32_t>(std::min<uint64_t>((n + 255) / 256, 65535)), 256, 0, c->stream>>>(
+      reinterpret_cast<uint32_t*>(d + o_list), n32);
+  Sw32Params p{};
+  p.db = db;
+  p.prof = prof_view(c);
+  p.list = reinterpret_cast<const uint32_t*>(d + o_list);
+  p.list_count = cnt;
+  p.pair_query = reinterpret_cast<const uint32_t*>(d + o_pq);
+  p.pair_target = reinterpret_cast<const uint32_t*>(d + o_pt);
+  p.pair_center = reinterpret_cast<const int32_t*>(d + o_zero);
+  p.pair_radius = reinterpret_cast<const int32_t*>(d + o_zero);  // unused in the end modes
+  p.scores = reinterpret_cast<int32_t*>(d + o_s);
+  p.kernels = nullptr;
+  p.work_counter = cnt + 1;
+  p.scratch = reinterpret_cast<int2*>(d + o_scr);
+  p.scratch_stride = sstride;
+  p.open = open;
+  p.ext = ext;
+  p.end_q = reinterpret_cast<int32_t*>(d + o_eq);
+  p.end_t = reinterpret_cast<int32_t*>(d + o_et);
+  sw32_end_kernel<kWarps32, kSw32End><<<grid, kWarps32 * 32, 0, c->stream>>>(p);
+  c->launches += 2;
+  if (span) {
+    Sw32Params r = p;
+    r.rev_q = p.end_q;
+    r.rev_t = p.end_t;
+    r.scores = reinterpret_cast<int32_t*>(d + o_rs);
+    r.end_q = reinterpret_cast<int32_t*>(d + o_sq);
+    r.end_t = reinterpret_cast<int32_t*>(d + o_st);
+    r.work_counter = cnt + 2;
+    sw32_end_kernel<kWarps32, kSw32RevEnd><<<grid, kWarps32 * 32, 0, c->stream>>>(r);
+    ++c->launches;
+  }
+  ST_CUDA(cudaGetLastError());
+  std::vector<int32_t> eq(n), et(n), rs, sq, st;
+  ST_CUDA(cudaMemcpyAsync(scores, d + o_s, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaMemcpyAsync(eq.data(), d + o_eq, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaMemcpyAsync(et.data(), d + o_et, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (span) {
+    rs.resize(n);
+    sq.resize(n);
+    st.resize(n);
+    ST_CUDA(cudaMemcpyAsync(rs.data(), d + o_rs, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(cudaMemcpyAsync(sq.data(), d + o_sq, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(cudaMemcpyAsync(st.data(), d + o_st, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  }
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  for (uint64_t i = 0; i < n; ++i) {
+    ends[2 * i] = eq[i];
+    ends[2 * i + 1] = et[i];
+    if (!span) continue;
+    if (scores[i] > 0 && rs[i] != scores[i])  // impossible: the best alignment ending at the end cell lies in the prefix
+      return fail(ST_ECUDA, "pair %llu: reverse pass scored %d, forward %d", static_cast<unsigned long long>(i),
+                  rs[i], scores[i]);
+    starts[2 * i] = scores[i] > 0 ? eq[i] - sq[i] : -1;
+    starts[2 * i + 1] = scores[i] > 0 ? et[i] - st[i] : -1;
+  }
+  return ST_OK;
+}
+
+static int end_pairs_entry(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, bool span,
+                           int32_t* scores, int32_t* ends, int32_t* starts) {
+  if (n && (!pairs || !scores || !ends || (span && !starts))) return fail(ST_EINVAL, "null argument");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  uint32_t max_len = 0, max_m = 0;
+  ST_TRY(validate_pairs(c, pairs, n, &max_len, &max_m));
+  std::vector<uint32_t> pq(n), pt(n);
+  for (uint64_t i = 0; i < n; ++i) {
+    if (pairs[i].band_radius >= 0)
+      return fail(ST_EINVAL, "pair %llu: end cells are defined for full local alignments (band_radius < 0)",
+                  static_cast<unsigned long long>(i));
+    pq[i] = pairs[i].profile;
+    pt[i] = pairs[i].target;
+  }
+  ST_TRY(sync_profiles(c));
+  return end_pairs_run(c, db_view(c), pq.data(), pt.data(), n, max_m, max_len, open, ext, span, scores, ends, starts);
+}
+
+extern "C" int st_sw_score_end_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                                     int32_t* scores, int32_t* ends) {
+  CTX_GUARD(c);
+  return end_pairs_entry(c, pairs, n, open, ext, false, scores, ends, nullptr);
+}
+
+extern "C" int st_sw_score_end(st_ctx* c, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open,
+                               int32_t ext, int32_t* score, int32_t* q_end, int32_t* t_end) {
+  CTX_GUARD(c);
+  if (!score || !q_end || !t_end || (n && !target)) return fail(ST_EINVAL, "st_sw_score_end: null argument");
+  ST_TRY(check_profile(c, profile));
+  ST_TRY(sync_profiles(c));
+  const uint32_t m = c->profs[profile].m;
+  if (m == 0 || n == 0) {  // src/simd.rs:302-304
+    *score = 0;
+    *q_end = *t_end = -1;
+    return ST_OK;
+  }
+  // the target as a one-sequence database in a pooled device block
+  const size_t tb = up16(n) + 16;
+  std::vector<uint8_t> h(tb + 16, kSentinel);
+  for (uint32_t i = 0; i < n; ++i) h[i] = target[i] < kSentinel ? target[i] : kSentinel;
+  const uint64_t zero = 0;
+  memcpy(h.data() + tb, &zero, 8);
+  memcpy(h.data() + tb + 8, &n, 4);
+  DevMem a;
+  ST_TRY(pool_get(c, h.size(), a));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
+  } back{c, &a};
+  ST_CUDA(cudaMemcpyAsync(a.p, h.data(), h.size(), cudaMemcpyHostToDevice, c->stream));
+  DeviceDb db;
+  db.arena = a.as<uint8_t>();
+  db.offset = reinterpret_cast<const uint64_t*>(a.as<char>() + tb);
+  db.length = reinterpret_cast<const uint32_t*>(a.as<char>() + tb + 8);
+  db.n_seqs = 1;
+  const uint32_t t0 = 0;
+  int32_t ends[2];
+  ST_TRY(end_pairs_run(c, db, &profile, &t0, 1, m, n, open, ext, false, score, ends, nullptr));
+  *q_end = ends[0];
+  *t_end = ends[1];
+  return ST_OK;
+}
+
+extern "C" int st_sw_align_span_pairs(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext,
+                                      int32_t* scores, int32_t* ends, int32_t* starts) {
+  CTX_GUARD(c);
+  return end_pairs_entry(c, pairs, n, open, ext, true, scores, ends, starts);
 }
 
 // ---------------------------------------------------------------------------

@@ -34,22 +34,44 @@ struct Sw32Params {
   int2* scratch;  // pass boundary rows, scratch_stride per warp
   uint32_t scratch_stride;
   int32_t open, ext;
+  // end-cell modes (sw32_end_kernel): the first optimum in column-major order
+  // (src/simd.rs:375-381), -1 when the score is 0; in the reverse mode the
+  // pair's query rows [0, rev_q] and target columns [0, rev_t] are scored
+  // reversed (the start search of align_canonical, src/align.rs:848-866)
+  int32_t* end_q;
+  int32_t* end_t;
+  const int32_t* rev_q;
+  const int32_t* rev_t;
 };
+
+enum Sw32Mode { kSw32Score = 0, kSw32End = 1, kSw32RevEnd = 2 };
 
 constexpr int kSw32G = 32;
 constexpr int kSw32R = 8;
 constexpr int kSw32Rows = kSw32G * kSw32R;  // rows per pass; profiles' int32 stride is a multiple of this
 
+// (score, column, row) of a candidate optimum; a < b when a comes first: higher
+// score, then smaller target column, then smaller query row
+__device__ __forceinline__ bool end_before(int32_t s, int32_t c, int32_t r, int32_t bs, int32_t bc, int32_t br) {
+  return s > bs || (s == bs && (c < bc || (c == bc && r < br)));
+}
+
+template <int MODE>
 __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int2* bnd) {
   constexpr int G = kSw32G, R = kSw32R;
   const int lane = threadIdx.x & 31;
   const uint32_t FULL = 0xFFFFFFFFu;
   const uint32_t q = prm.pair_query[p];
   const uint32_t tid = prm.pair_target[p];
-  const int m = static_cast<int>(prm.prof.qlen[q]);
-  const int n = static_cast<int>(prm.db.length[tid]);
-  const int32_t center = prm.pair_center[p];
-  const int32_t radius = prm.pair_radius[p];
+  const int m_full = static_cast<int>(prm.prof.qlen[q]);
+  const int n_full = static_cast<int>(prm.db.length[tid]);
+  // the reverse mode scores the prefix [0, rev_q] x [0, rev_t], both reversed
+  const int rq = MODE == kSw32RevEnd ? prm.rev_q[p] : 0;
+  const int rt = MODE == kSw32RevEnd ? prm.rev_t[p] : 0;
+  const int m = MODE == kSw32RevEnd ? (rq >= 0 ? min(rq + 1, m_full) : 0) : m_full;
+  const int n = MODE == kSw32RevEnd ? (rt >= 0 ? min(rt + 1, n_full) : 0) : n_full;
+  const int32_t center = MODE == kSw32Score ? prm.pair_center[p] : 0;
+  const int32_t radius = MODE == kSw32Score ? prm.pair_radius[p] : -1;
   const bool banded = radius >= 0;
   // columns that can hold band cells: row + center - radius .. row + center + radius
   int64_t c_lo = 0, c_hi = n;  // [c_lo, c_hi)
@@ -61,6 +83,10 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     if (lane == 0) {
       prm.scores[p] = 0;
       if (prm.kernels) prm.kernels[p] = 2u;
+      if (MODE != kSw32Score) {
+        prm.end_q[p] = -1;
+        prm.end_t[p] = -1;
+      }
     }
     return;
   }
@@ -81,11 +107,17 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     E[k] = E0;
   }
   int32_t best = 0, hup_prev = 0, h_bot = 0, f_out = F0;
+  int32_t bcol = 0x7FFFFFFF, brow = 0x7FFFFFFF;  // end modes: this lane's first optimum
   uint32_t res = kSentinel;
   int c = -lane;
   int pass = 0;
   uint32_t nxt = kSentinel;
-  if (lane == 0) nxt = min(static_cast<uint32_t>(__ldg(t + cstart)), static_cast<uint32_t>(kSentinel));
+  // target column j of the scored sequence (reversed in the reverse mode)
+  auto tcol = [&](int j) -> uint32_t {
+    const int jj = MODE == kSw32RevEnd ? rt - j : j;
+    return min(static_cast<uint32_t>(__ldg(t + jj)), static_cast<uint32_t>(kSentinel));
+  };
+  if (lane == 0) nxt = tcol(cstart);
   const int steps = P * ncols + G - 1;
 
   for (int s = 0; s < steps; ++s) {
@@ -98,9 +130,7 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
         int cn = c + 1;
         bool last = (cn == ncols);
         if (last) cn = 0;
-        nxt = (last && pass + 1 >= P)
-                  ? kSentinel
-                  : min(static_cast<uint32_t>(__ldg(t + cstart + cn)), static_cast<uint32_t>(kSentinel));
+        nxt = (last && pass + 1 >= P) ? kSentinel : tcol(cstart + cn);
         if (pass > 0) {
           int2 bv = bnd[c];
           hin = bv.x;
@@ -128,7 +158,12 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     const int row0 = pp * G * R + lane * R;
     const int32_t* prow = prof + static_cast<size_t>(res) * stride + row0;
     int32_t S[R];
-    {
+    if constexpr (MODE == kSw32RevEnd) {
+      // row r of the reversed query is row rq - r of the profile (rows past the prefix: any in-range row)
+      const int32_t* rb = prof + static_cast<size_t>(res) * stride;
+#pragma unroll
+      for (int k = 0; k < R; ++k) S[k] = __ldg(rb + max(rq - (row0 + k), 0));
+    } else {
       const int4 a = __ldg(reinterpret_cast<const int4*>(prow));
       const int4 b = __ldg(reinterpret_cast<const int4*>(prow + 4));
       S[0] = a.x; S[1] = a.y; S[2] = a.z; S[3] = a.w;
@@ -154,7 +189,16 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
         const int32_t Ho = wsub(H, open);
         En = max(wsub(E[k], ext), Ho);
         Fn = max(wsub(F, ext), Ho);
-        if (row < m) lmax = max(lmax, H);
+        if (row < m) {
+          lmax = max(lmax, H);
+          if constexpr (MODE != kSw32Score) {
+            if (live && end_before(H, col, row, best, bcol, brow)) {
+              best = H;
+              bcol = col;
+              brow = row;
+            }
+          }
+        }
       } else {
         H = 0;
         En = E0;
@@ -165,7 +209,7 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
       hd = Hp[k];
       Hp[k] = H;
     }
-    if (live) best = max(best, lmax);
+    if (MODE == kSw32Score && live) best = max(best, lmax);
     hup_prev = hin;
     h_bot = Hp[R - 1];
     f_out = F;
@@ -176,11 +220,29 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     }
     __syncwarp();
   }
+  if constexpr (MODE == kSw32Score) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(FULL, best, o));
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(FULL, best, o));
+  } else {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const int32_t ob = __shfl_xor_sync(FULL, best, o);
+      const int32_t oc = __shfl_xor_sync(FULL, bcol, o);
+      const int32_t orow = __shfl_xor_sync(FULL, brow, o);
+      if (end_before(ob, oc, orow, best, bcol, brow)) {
+        best = ob;
+        bcol = oc;
+        brow = orow;
+      }
+    }
+  }
   if (lane == 0) {
     prm.scores[p] = best;
     if (prm.kernels) prm.kernels[p] = 2u;
+    if (MODE != kSw32Score) {
+      prm.end_q[p] = best > 0 ? brow : -1;
+      prm.end_t[p] = best > 0 ? bcol : -1;
+    }
   }
 }
 
@@ -195,7 +257,24 @@ __global__ void __launch_bounds__(WARPS * 32) sw32_kernel(const Sw32Params prm) 
     if (lane == 0) w = atomicAdd(prm.work_counter, 1u);
     w = __shfl_sync(0xFFFFFFFFu, w, 0);
     if (w >= count) break;
-    sw32_pair(prm, prm.list[w], bnd);
+    sw32_pair<kSw32Score>(prm, prm.list[w], bnd);
+  }
+}
+
+// Score and end cell of every listed pair (MODE kSw32End), or of the reversed
+// prefixes ending at (rev_q, rev_t) (MODE kSw32RevEnd). Unbanded pairs only.
+template <int WARPS, int MODE>
+__global__ void __launch_bounds__(WARPS * 32) sw32_end_kernel(const Sw32Params prm) {
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int2* bnd = prm.scratch + static_cast<size_t>(blockIdx.x * WARPS + warp) * prm.scratch_stride;
+  const uint32_t count = *prm.list_count;
+  for (;;) {
+    uint32_t w = 0;
+    if (lane == 0) w = atomicAdd(prm.work_counter, 1u);
+    w = __shfl_sync(0xFFFFFFFFu, w, 0);
+    if (w >= count) break;
+    sw32_pair<MODE>(prm, prm.list[w], bnd);
   }
 }
 
