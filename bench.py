@@ -61,6 +61,18 @@ def dist_env():
     return rank, world, local
 
 
+def combine_ranks(ms, cells, device):
+    """Whole-job step time and work across ranks: the slowest rank's step time (every rank scores its own
+    instance of the workload, so the job ends with the slowest) and the sum of the ranks' cells."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(cells)], device=device, dtype=torch.float64)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def make_workload(args, rank):
     from sabertooth_b200 import workloads as W
     nq = max(8, int(round(4000 * args.scale)))
@@ -277,12 +289,7 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     ms = float(np.mean(step_ms))
     if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        c = torch.tensor([cells], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
-        total_cells = float(c.item())
+        ms, total_cells = combine_ranks(ms, cells, "cuda")
     else:
         total_cells = float(cells)
     gcups = total_cells / (ms * 1e-3) / 1e9

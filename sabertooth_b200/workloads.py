@@ -285,7 +285,7 @@ def config3(seed=0, n_queries=4000, db_residues=2_600_000, per_query=300, plante
     pick_rng = rng.child(40_000_000)
     for i in range(n_queries):
         own = np.nonzero(owner == i)[0] if planted_per_query else np.zeros(0, np.int64)
-        want = per_query - own.size
+        want = max(0, min(per_query - own.size, n_db - own.size))  # a small database caps the targets per query
         cand = pick_rng.below(want * 2 + 16, n_db)
         cand = np.unique(cand[~np.isin(cand, own)])[:want]
         while cand.size < want:
