@@ -489,14 +489,20 @@ def ungapped_measure(ctx, args):
     ms = float(np.median(ts))
     got = d_out.cpu().numpy()
     n_runs = int(d_np.item())
-    # parity and the CPU baseline on a sample (the oracle: scalar Kadane, all host cores)
-    rng = np.random.default_rng(args.seed)
-    sel = np.sort(rng.choice(n, min(n, 2_000_000), replace=False))
+    # CPU baseline: the reference's AVX2 batched Kadane restated in C over the whole workload, all host
+    # cores (median of three runs); its results are the parity check of the GPU's
     targets = [w.db_residues[int(a_):int(b_)] for a_, b_ in zip(w.db_offsets[:-1], w.db_offsets[1:])]
     arena = O.Arena(w.rows, targets)
-    t0 = time.perf_counter()
-    want = O.ungapped_hits(arena, w.hits["query"][sel], w.hits["target"][sel], w.hits["diag"][sel])
-    t_cpu = time.perf_counter() - t0
+    t_runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        want = O.ungapped_hits_avx2(arena, w.hits["query"], w.hits["target"], w.hits["diag"])
+        t_runs.append(time.perf_counter() - t0)
+    t_cpu = float(np.median(t_runs))
+    rng = np.random.default_rng(args.seed)
+    sel = np.sort(rng.choice(n, min(n, 200_000), replace=False))
+    scalar_ok = bool(np.array_equal(O.ungapped_hits(arena, w.hits["query"][sel], w.hits["target"][sel],
+                                                    w.hits["diag"][sel]), want[sel]))
     peak = hbm_peak_gbs()
     gbs = ab / (ms * 1e-3) / 1e9
     ctx.free_profiles(ids)
@@ -506,10 +512,12 @@ def ungapped_measure(ctx, args):
             "algorithmic_bytes": int(ab), "runs": n_runs,
             "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(gbs / peak, 4), "traffic": read_traffic("ungapped_config2.md")},
-            "matches_oracle_sample": bool(np.array_equal(got[sel], want)),
-            "cpu_baseline": {"value": round(len(sel) / t_cpu / 1e6, 2), "unit": "Mhits/s", "cores": os.cpu_count(),
-                             "kind": "port", "sample": f"{len(sel)} random hits of the workload, scalar Kadane "
-                                                       "(the reference's kadane_score restated in C), OpenMP"},
+            "matches_cpu_baseline": bool(np.array_equal(got, want)), "cpu_baseline_matches_scalar_sample": scalar_ok,
+            "cpu_baseline": {"value": round(n / t_cpu / 1e6, 2), "unit": "Mhits/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"the whole workload ({n} hits), median of 3 runs: the "
+                                                       "reference's AVX2 batched Kadane (biased u8 tables, 32 lanes, "
+                                                       "window-start order, exact rescore) restated in C, queries in "
+                                                       "parallel over all host threads"},
             "setup_s": round(t_gen, 1)}
 
 

@@ -56,6 +56,10 @@ void or_sw_pairs(const int32_t* rows_arena, const uint64_t* row_off, const uint3
 void or_ungapped_hits(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
                       const uint8_t* tgt_arena, const uint64_t* tgt_off, const uint32_t* hq, const uint32_t* ht,
                       const int32_t* hd, uint64_t n_hits, int32_t* out, int nthreads);
+/* The reference's AVX2 batched Kadane over seed-hit diagonals (kadane_avx2.c): the CPU baseline of (U). */
+void or_ungapped_hits_avx2(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
+                           const uint8_t* tgt_arena, const uint64_t* tgt_off, const uint32_t* hq, const uint32_t* ht,
+                           const int32_t* hd, uint64_t n_hits, int32_t* out, int nthreads);
 
 /* CPU baseline (striped.c): the reference's default AVX2 path (u8 striped -> i16 striped ->
  * scalar) over pairs grouped by query; query q's targets are tlist[qstart[q] .. qstart[q+1]).

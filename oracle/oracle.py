@@ -39,6 +39,7 @@ def _load():
     lib.or_band_score.argtypes = [P, u32, P, u32, i32, i32, i64, i64]
     lib.or_sw_pairs.argtypes = [P, P, P, P, P, P, P, P, P, u64, i32, i32, P, C.c_int]
     lib.or_ungapped_hits.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
+    lib.or_ungapped_hits_avx2.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
     lib.or_striped_queries.argtypes = [P, P, P, u32, P, P, P, P, i32, i32, P, P, C.c_int]
     return lib
 
@@ -135,6 +136,17 @@ def ungapped_hits(arena: Arena, hq, ht, hd, threads=0):
     out = np.zeros(n, dtype=np.int32)
     lib.or_ungapped_hits(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(arena.tgt), _p(arena.tgt_off),
                          _p(hq), _p(ht), _p(hd), n, _p(out), threads or os.cpu_count() or 1)
+    return out
+
+
+def ungapped_hits_avx2(arena: Arena, hq, ht, hd, threads=0):
+    """The reference's AVX2 batched Kadane over hits (grouped by query), results in hit order."""
+    hq = np.ascontiguousarray(hq, dtype=np.uint32)
+    ht = np.ascontiguousarray(ht, dtype=np.uint32)
+    hd = np.ascontiguousarray(hd, dtype=np.int32)
+    out = np.zeros(len(hq), dtype=np.int32)
+    lib.or_ungapped_hits_avx2(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(arena.tgt), _p(arena.tgt_off),
+                              _p(hq), _p(ht), _p(hd), len(hq), _p(out), threads or os.cpu_count() or 1)
     return out
 
 

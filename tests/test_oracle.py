@@ -184,3 +184,21 @@ def test_striped_cpu_baseline_equals_scalar_oracle():
     pw = W.config3(seed=5, n_queries=10, db_residues=30_000, per_query=30)
     ar = O.Arena(pw.rows, pw.targets())
     assert np.array_equal(O.striped_pairs(ar, pw.pair_q, pw.pair_t, 44, 4), O.sw_pairs(ar, pw.pair_q, pw.pair_t, 44, 4))
+
+
+def test_avx2_ungapped_baseline_equals_scalar_kadane():
+    """The AVX2 restatement of the reference's batched Kadane (the CPU baseline of ungapped scoring)
+    gives the scalar oracle's score on every hit: BLOSUM62 rows on the u8 path, rows with scores
+    high enough to saturate u8 (rescored), and PSSM-like rows outside the u8 range (scalar)."""
+    from sabertooth_b200 import workloads as W
+    w = W.config2(seed=7, n_queries=40, n_targets=3000, n_hits=60_000)
+    targets = [w.db_residues[int(a):int(b)] for a, b in zip(w.db_offsets[:-1], w.db_offsets[1:])]
+    rows = list(w.rows)
+    rows[3] = rows[3] * 9           # max 99 -> u8 headroom exceeded on long windows, lanes rescored
+    rows[5] = rows[5] * 40          # outside u8 -> every lane scalar
+    ar = O.Arena(rows, targets)
+    h = w.hits
+    want = O.ungapped_hits(ar, h["query"], h["target"], h["diag"])
+    got = O.ungapped_hits_avx2(ar, h["query"], h["target"], h["diag"])
+    assert np.array_equal(got, want)
+    assert (want[h["query"] == 3] > 160).any()
