@@ -196,6 +196,81 @@ int st_ungapped_hits_device(st_ctx* ctx, const st_hit* d_hits, uint64_t n, int32
                             int32_t* d_pair_best, uint32_t* d_pair_query, uint32_t* d_pair_target,
                             uint64_t* d_n_pairs);
 
+/* ---- prefilter evidence, chain and gate -----------------------------------
+ * The segment-evidence stage of prefilter_query (xdrop = 0, the default) for
+ * the seed hits of many queries in one call: evaluate_block_kadane and
+ * score_and_gate (src/prefilter.rs:1412-1660) followed by the candidate ranking
+ * (:1074-1083).  Per (query, target): targets with fewer than min_hits hits are
+ * dropped; the max_diagonals diagonals with the most hits (top_diagonals
+ * :1194-1225, at most 16 scored) must include one with diag_hits hits; each is
+ * scored by its best ungapped segment (kadane_segment, src/ungapped.rs:69-88)
+ * over [qmin - diag_window, qmax + span + diag_window) clipped to diag_range
+ * (the whole diagonal when diag_window = 0); the target's score is the best
+ * segment or the best chain of two co-linear segments, sx + sy - gap(|dy - dx|)
+ * (GapCosts::cost, src/align.rs:216-222), and it passes when the score is at
+ * least min_diag_score. */
+
+/* A seed hit: query profile id, database ordinal, diagonal = target position -
+ * query position, query position (the reference's packed hit key,
+ * src/prefilter.rs:1021-1036). */
+typedef struct {
+  uint32_t query;
+  uint32_t target;
+  int32_t diag;
+  uint32_t qpos;
+} st_seed_hit;
+
+/* The evidence fields of PrefilterParams (src/prefilter.rs:262-303) plus the
+ * seed span and the gap costs. */
+typedef struct {
+  uint32_t min_hits;
+  uint32_t diag_hits;       /* >= 1 */
+  uint32_t max_diagonals;   /* >= 1 */
+  uint32_t diag_window;     /* 0 = whole diagonal */
+  uint32_t span;            /* seed pattern span (k for contiguous seeds) */
+  int32_t min_diag_score;
+  int32_t gap_open;
+  int32_t gap_ext;
+  uint32_t max_candidates;  /* per query, 0 = all */
+  uint32_t regions;         /* 1 = compute t_lo..t_hi, 0 = report 0..UINT32_MAX */
+} st_prefilter_params;
+
+/* Candidate (src/prefilter.rs:370-381) plus its query id. */
+typedef struct {
+  uint32_t query;
+  uint32_t target;
+  uint32_t hits;
+  int32_t diag_score;
+  int64_t best_diag;
+  uint32_t t_lo;
+  uint32_t t_hi;
+} st_candidate;
+
+/* The evidence counters of PrefilterStats, summed over the call's queries,
+ * plus hits_rejected: hits outside their query or target, or with an unknown
+ * profile id (they are skipped and the call returns ST_EINVAL). */
+typedef struct {
+  uint64_t targets_hit;
+  uint64_t targets_evaluated;
+  uint64_t diagonals_scored;
+  uint64_t chains_used;
+  uint64_t candidates;
+  uint64_t candidates_capped;
+  uint64_t hits_rejected;
+} st_prefilter_stats;
+
+/* Host buffers.  Candidates are ordered by query id, then score descending,
+ * then target ascending, at most max_candidates per query.  *n_out receives the
+ * total; the first min(cap, total) are written to out (cap = n always
+ * suffices).  stats may be NULL.  Fewer than 2^31 - 1 hits per call. */
+int st_prefilter_gate(st_ctx* ctx, const st_seed_hit* hits, uint64_t n, const st_prefilter_params* params,
+                      st_candidate* out, uint64_t cap, uint64_t* n_out, st_prefilter_stats* stats);
+/* Device buffers (d_out has room for n candidates); n_out and stats are host
+ * pointers.  Returns once the candidates are written (it reads the candidate
+ * count from the device to size the ranking). */
+int st_prefilter_gate_device(st_ctx* ctx, const st_seed_hit* d_hits, uint64_t n, const st_prefilter_params* params,
+                             st_candidate* d_out, uint64_t* n_out, st_prefilter_stats* stats);
+
 /* ---- end cells and alignment spans ---------------------------------------
  * Score plus end cell, the first optimum in column-major order (smallest target
  * position, then smallest query position): QueryProfile::sw_score_end_with

@@ -204,3 +204,39 @@ void or_ungapped_hits_avx2(const int32_t* rows_arena, const uint64_t* row_off, c
   }
   free(run);
 }
+
+/* One query's jobs with explicit windows (the reference's score_batch calls from
+ * score_and_gate, src/prefilter.rs:1529-1575): tp[j] = target residues,
+ * window [lo[j], hi[j]) on diagonal d[j]; out[j] = kadane_score. */
+void or_kadane_jobs_avx2(const int32_t* rows, uint32_t m, const uint8_t* const* tp, const int64_t* d,
+                         const uint32_t* lo, const uint32_t* hi, uint32_t n, int32_t* out) {
+  if (n == 0) return;
+  int32_t mn = 0, mx = 0;
+  for (size_t i = 0; i < (size_t)m * NPROF; ++i) {
+    if (rows[i] < mn) mn = rows[i];
+    if (rows[i] > mx) mx = rows[i];
+  }
+  const int32_t bias = -mn, limit = 255 - (mx + bias);
+  const int simd = m > 0 && bias <= 255 && limit >= MIN_LIMIT;
+  uint8_t* tables = (uint8_t*)malloc(((size_t)m + 2) * 32);
+  if (simd)
+    for (uint32_t i = 0; i < m; ++i) {
+      for (int res = 0; res < 32; ++res) tables[(size_t)i * 32 + res] = (uint8_t)bias;
+      for (int res = 0; res < NPROF; ++res) tables[(size_t)i * 32 + res] = (uint8_t)(rows[(size_t)i * NPROF + res] + bias);
+    }
+  uint32_t* cnt = (uint32_t*)malloc(((size_t)m + 4) * sizeof(uint32_t));
+  lane_job* jobs = (lane_job*)malloc((size_t)n * sizeof(lane_job));
+  lane_job* ord = (lane_job*)malloc((size_t)n * sizeof(lane_job));
+  const size_t wmax = ((size_t)m + 31) & ~(size_t)15;
+  uint8_t* lm = (uint8_t*)malloc(wmax * LANES + 64);
+  uint8_t* pm = (uint8_t*)malloc(wmax * LANES + 64);
+  for (uint32_t j = 0; j < n; ++j) jobs[j] = (lane_job){lo[j], hi[j] > lo[j] ? hi[j] : lo[j], d[j], tp[j], j};
+  score_query(rows, m, tables, simd, (uint8_t)(simd ? bias : 0), (uint8_t)(simd ? limit : 0), jobs, n, out, lm, pm, cnt,
+              ord);
+  free(tables);
+  free(cnt);
+  free(jobs);
+  free(ord);
+  free(lm);
+  free(pm);
+}

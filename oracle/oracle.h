@@ -69,6 +69,58 @@ void or_striped_queries(const int32_t* rows_arena, const uint64_t* row_off, cons
                         const uint32_t* tlist, int32_t open, int32_t ext, int32_t* out, uint8_t* used,
                         int nthreads);
 
+/* ---- prefilter evidence, chain and gate (gate.c) ----------------------------
+ * One query's seed hits (target, diagonal = target_pos - query_pos, query
+ * position) -> ranked candidates: the segment-evidence stage of prefilter_query
+ * (src/prefilter.rs:1412-1660, ranking :1074-1083).  out needs room for one
+ * candidate per distinct target (n_hits suffices). */
+typedef struct {
+  uint32_t query;
+  uint32_t target;
+  uint32_t hits;
+  int32_t diag_score;
+  int64_t best_diag;
+  uint32_t t_lo;
+  uint32_t t_hi;
+} or_candidate;
+
+typedef struct {
+  uint32_t min_hits;
+  uint32_t diag_hits;
+  uint32_t max_diagonals;
+  uint32_t diag_window;
+  uint32_t span;
+  int32_t min_diag_score;
+  int32_t gap_open;
+  int32_t gap_ext;
+  uint32_t max_candidates;
+  uint32_t regions;
+} or_prefilter_params;
+
+typedef struct {
+  uint64_t targets_hit;
+  uint64_t targets_evaluated;
+  uint64_t diagonals_scored;
+  uint64_t chains_used;
+  uint64_t candidates;
+  uint64_t candidates_capped;
+} or_prefilter_stats;
+
+uint64_t or_prefilter_query(const int32_t* rows, uint32_t m, uint32_t query, const uint8_t* tgt_arena,
+                            const uint64_t* tgt_off, const uint32_t* ht, const int32_t* hd, const uint32_t* hqpos,
+                            uint64_t n_hits, const or_prefilter_params* p, int simd, or_candidate* out,
+                            or_prefilter_stats* st);
+/* Queries in parallel: query q (profile id qids[q]) owns hits hstart[q] .. hstart[q+1]
+ * and writes n_out[q] candidates at out + hstart[q], stats[q] its counters. */
+void or_prefilter_queries(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
+                          const uint32_t* qids, uint32_t n_queries, const uint8_t* tgt_arena, const uint64_t* tgt_off,
+                          const uint64_t* hstart, const uint32_t* ht, const int32_t* hd, const uint32_t* hqpos,
+                          const or_prefilter_params* p, int simd, or_candidate* out, uint64_t* n_out,
+                          or_prefilter_stats* stats, int nthreads);
+/* The AVX2 batched Kadane over one query's jobs with explicit windows (kadane_avx2.c). */
+void or_kadane_jobs_avx2(const int32_t* rows, uint32_t m, const uint8_t* const* tp, const int64_t* d,
+                         const uint32_t* lo, const uint32_t* hi, uint32_t n, int32_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,7 @@ def _load():
     lib.or_ungapped_hits.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
     lib.or_ungapped_hits_avx2.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
     lib.or_striped_queries.argtypes = [P, P, P, u32, P, P, P, P, i32, i32, P, P, C.c_int]
+    lib.or_prefilter_queries.argtypes = [P, P, P, P, u32, P, P, P, P, P, P, P, C.c_int, P, P, P, C.c_int]
     return lib
 
 
@@ -169,3 +170,45 @@ def striped_pairs(arena: Arena, pq, pt, open_, ext, threads=0, with_kinds=False)
     kinds = np.zeros_like(used)
     kinds[order] = used
     return (res, kinds) if with_kinds else res
+
+
+# ---- prefilter evidence, chain and gate (gate.c) -------------------------------
+CANDIDATE_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("hits", "<u4"), ("diag_score", "<i4"),
+                            ("best_diag", "<i8"), ("t_lo", "<u4"), ("t_hi", "<u4")])
+STATS_FIELDS = ("targets_hit", "targets_evaluated", "diagonals_scored", "chains_used", "candidates",
+                "candidates_capped")
+PARAM_FIELDS = ("min_hits", "diag_hits", "max_diagonals", "diag_window", "span", "min_diag_score", "gap_open",
+                "gap_ext", "max_candidates", "regions")
+_PARAM_DTYPE = np.dtype([(f, "<i4" if f in ("min_diag_score", "gap_open", "gap_ext") else "<u4")
+                         for f in PARAM_FIELDS])
+
+
+def prefilter_queries(arena: Arena, hq, ht, hd, hqpos, params: dict, simd=True, threads=0):
+    """The reference's segment evidence + chain + gate + ranking per query
+    (src/prefilter.rs:1412-1660, 1074-1083).  params: the PARAM_FIELDS keys.
+    Returns (candidates ordered by query id, then rank; summed stats dict)."""
+    hq = np.asarray(hq, dtype=np.uint32)
+    order = np.argsort(hq, kind="stable")
+    ht = np.ascontiguousarray(np.asarray(ht, dtype=np.uint32)[order])
+    hd = np.ascontiguousarray(np.asarray(hd, dtype=np.int32)[order])
+    hqpos = np.ascontiguousarray(np.asarray(hqpos, dtype=np.uint32)[order])
+    qs = hq[order]
+    qids, first = np.unique(qs, return_index=True)
+    qids = np.ascontiguousarray(qids, dtype=np.uint32)
+    hstart = np.zeros(len(qids) + 1, dtype=np.uint64)
+    hstart[:-1] = first
+    hstart[-1] = len(qs)
+    prm = np.zeros(1, dtype=_PARAM_DTYPE)
+    for f in PARAM_FIELDS:
+        prm[f] = params[f]
+    out = np.zeros(max(len(qs), 1), dtype=CANDIDATE_DTYPE)
+    n_out = np.zeros(max(len(qids), 1), dtype=np.uint64)
+    stats = np.zeros((max(len(qids), 1), len(STATS_FIELDS)), dtype=np.uint64)
+    if len(qids):
+        lib.or_prefilter_queries(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(qids), len(qids),
+                                 _p(arena.tgt), _p(arena.tgt_off), _p(hstart), _p(ht), _p(hd), _p(hqpos), _p(prm),
+                                 1 if simd else 0, _p(out), _p(n_out), _p(stats), threads or os.cpu_count() or 1)
+    parts = [out[int(hstart[i]):int(hstart[i]) + int(n_out[i])] for i in range(len(qids))]
+    cands = np.concatenate(parts) if parts else np.zeros(0, dtype=CANDIDATE_DTYPE)
+    tot = stats[:len(qids)].sum(axis=0) if len(qids) else np.zeros(len(STATS_FIELDS), np.uint64)
+    return cands, {f: int(v) for f, v in zip(STATS_FIELDS, tot)}

@@ -39,6 +39,22 @@ class st_hit(C.Structure):
 PAIR_DTYPE = np.dtype([("profile", "<u4"), ("target", "<u4"), ("band_center", "<i4"), ("band_radius", "<i4")])
 LANE_DTYPE = np.dtype([("target", "<u4"), ("lo", "<u4"), ("hi", "<u4"), ("diag", "<i4")])
 HIT_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("diag", "<i4")])
+SEED_HIT_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("diag", "<i4"), ("qpos", "<u4")])
+CANDIDATE_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("hits", "<u4"), ("diag_score", "<i4"),
+                            ("best_diag", "<i8"), ("t_lo", "<u4"), ("t_hi", "<u4")])
+PREFILTER_STATS_FIELDS = ("targets_hit", "targets_evaluated", "diagonals_scored", "chains_used", "candidates",
+                          "candidates_capped", "hits_rejected")
+
+
+class PrefilterParamsC(C.Structure):
+    _fields_ = [("min_hits", C.c_uint32), ("diag_hits", C.c_uint32), ("max_diagonals", C.c_uint32),
+                ("diag_window", C.c_uint32), ("span", C.c_uint32), ("min_diag_score", C.c_int32),
+                ("gap_open", C.c_int32), ("gap_ext", C.c_int32), ("max_candidates", C.c_uint32),
+                ("regions", C.c_uint32)]
+
+
+class PrefilterStatsC(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in PREFILTER_STATS_FIELDS]
 
 _P = C.c_void_p
 _u32, _i32, _u64, _i64, _sz = C.c_uint32, C.c_int32, C.c_uint64, C.c_int64, C.c_size_t
@@ -79,6 +95,8 @@ SIGNATURES = {
     "st_ungapped_score": (C.c_int, [_P, _u32, _P, _u32, _P]),
     "st_ungapped_hits": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
     "st_ungapped_hits_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
+    "st_prefilter_gate": (C.c_int, [_P, _P, _u64, _P, _P, _u64, _P, _P]),
+    "st_prefilter_gate_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P]),
     "st_tune_num_classes": (C.c_int, []),
     "st_tune_class_shape": (C.c_int, [C.c_int, _P, _P, _P]),
     "st_tune_get": (C.c_int, [_P, _P]),

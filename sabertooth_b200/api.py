@@ -16,7 +16,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import HIT_DTYPE, LANE_DTYPE, PAIR_DTYPE, check, lib, ptr
+from ._lib import (CANDIDATE_DTYPE, HIT_DTYPE, LANE_DTYPE, PAIR_DTYPE, PREFILTER_STATS_FIELDS, SEED_HIT_DTYPE,
+                   check, lib, ptr)
 
 ALPHABET_SIZE = 21
 
@@ -38,6 +39,36 @@ class GapCosts:
 
     def cost(self, length):
         return 0 if length == 0 else self.open + (length - 1) * self.extend
+
+
+@dataclass(frozen=True)
+class PrefilterParams:
+    """The segment-evidence fields of the reference's PrefilterParams
+    (src/prefilter.rs:262-303; defaults sequence_default :309-331 and
+    profile_default :333-341), plus span: the seed pattern's span (k for a
+    contiguous seed), which widens each diagonal's window past its last hit."""
+
+    min_hits: int = 1
+    min_diag_score: int = 42
+    diag_hits: int = 1
+    max_diagonals: int = 4
+    max_candidates: int = 0
+    regions: bool = False
+    diag_window: int = 48
+    span: int = 6
+
+    @staticmethod
+    def sequence_default():
+        return PrefilterParams()
+
+    @staticmethod
+    def profile_default():
+        return PrefilterParams(min_diag_score=30, span=5)
+
+    def to_c(self, gaps: GapCosts):
+        return _lib.PrefilterParamsC(self.min_hits, self.diag_hits, self.max_diagonals, self.diag_window, self.span,
+                                     self.min_diag_score, gaps.open, gaps.extend, self.max_candidates,
+                                     1 if self.regions else 0)
 
 
 class Kernel(enum.IntEnum):
@@ -223,6 +254,35 @@ class Context:
                                           _vp(d_pair_best), _vp(d_pair_query), _vp(d_pair_target),
                                           _vp(d_n_pairs)))
 
+    def prefilter_gate(self, hits, params: PrefilterParams = None, gaps: GapCosts = None):
+        """Seed hits (query profile id, target, diagonal, query position) -> ranked
+        candidates (CANDIDATE_DTYPE: per query id, score descending, target
+        ascending) and the evidence counters, the reference's score_and_gate stage
+        (src/prefilter.rs:1412-1660, 1074-1083) for every query of the batch."""
+        hits = as_seed_hits(hits)
+        params = params or PrefilterParams.sequence_default()
+        gaps = gaps or GapCosts.sequence_default()
+        n = len(hits)
+        out = np.zeros(max(n, 1), dtype=CANDIDATE_DTYPE)
+        n_out = C.c_uint64()
+        st = _lib.PrefilterStatsC()
+        prm = params.to_c(gaps)
+        check(lib.st_prefilter_gate(self._h, ptr(hits), n, C.byref(prm), ptr(out), n, C.byref(n_out),
+                                    C.byref(st)))
+        return out[:n_out.value].copy(), {f: getattr(st, f) for f in PREFILTER_STATS_FIELDS}
+
+    def prefilter_gate_device(self, d_hits_ptr, n, d_out_ptr, params: PrefilterParams = None,
+                              gaps: GapCosts = None):
+        """Device-buffer form: returns (candidate count, counters); d_out has room for n candidates."""
+        params = params or PrefilterParams.sequence_default()
+        gaps = gaps or GapCosts.sequence_default()
+        n_out = C.c_uint64()
+        st = _lib.PrefilterStatsC()
+        prm = params.to_c(gaps)
+        check(lib.st_prefilter_gate_device(self._h, C.c_void_p(d_hits_ptr), n, C.byref(prm), C.c_void_p(d_out_ptr),
+                                           C.byref(n_out), C.byref(st)))
+        return n_out.value, {f: getattr(st, f) for f in PREFILTER_STATS_FIELDS}
+
     # -- tuning / measurement ---------------------------------------------------
     def autotune(self, pairs, gaps: GapCosts, max_pairs=200_000):
         """Measures every tile class's rate on a sample of `pairs`; returns the number of classes measured."""
@@ -284,6 +344,15 @@ def as_hits(hits):
     if isinstance(hits, np.ndarray) and hits.dtype == HIT_DTYPE:
         return np.ascontiguousarray(hits)
     arr = np.zeros(len(hits), dtype=HIT_DTYPE)
+    for i, h in enumerate(hits):
+        arr[i] = tuple(h)
+    return arr
+
+
+def as_seed_hits(hits):
+    if isinstance(hits, np.ndarray) and hits.dtype == SEED_HIT_DTYPE:
+        return np.ascontiguousarray(hits)
+    arr = np.zeros(len(hits), dtype=SEED_HIT_DTYPE)
     for i, h in enumerate(hits):
         arr[i] = tuple(h)
     return arr

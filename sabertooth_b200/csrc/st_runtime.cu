@@ -23,10 +23,13 @@
 #include "st_tuning.h"
 #include "st_ungapped.cuh"
 #include "st_dplan.cuh"
+#include "st_gate.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 #include <cub/iterator/transform_input_iterator.cuh>
 
 using namespace st;
@@ -259,6 +262,7 @@ struct st_ctx {
   std::vector<uint32_t> h_db_len;
   std::vector<uint64_t> h_db_off;  // arena offset of each sequence (multiple of 16)
   uint32_t n_seqs = 0;
+  uint32_t max_len = 0;  // longest sequence
   uint64_t n_res = 0;
   bool has_db = false;
   // profiles
@@ -467,6 +471,7 @@ static DeviceProfiles prof_view(st_ctx* c) {
 
 static int g_class_smem[kNumClasses];  // dynamic shared memory each 16-bit class may use
 static int g_ung_smem = 0;              // dynamic shared memory the ungapped kernels may use
+static int g_gate_smem = 0;             // dynamic shared memory of the prefilter segment kernel
 
 static int set_smem_limits(int device) {
   int optin = 0;
@@ -483,6 +488,10 @@ static int set_smem_limits(int device) {
   g_ung_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(std::max(fa_t.sharedSizeBytes, fa_f.sharedSizeBytes)));
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
+  cudaFuncAttributes fa_g;
+  ST_CUDA(cudaFuncGetAttributes(&fa_g, reinterpret_cast<const void*>(gate_segment_kernel)));
+  g_gate_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(fa_g.sharedSizeBytes));
+  ST_CUDA(cudaFuncSetAttribute(gate_segment_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_gate_smem));
   return ST_OK;
 }
 
@@ -637,6 +646,7 @@ extern "C" int st_db_upload(st_ctx* c, const uint8_t* residues, const uint64_t* 
   ST_CUDA(cudaMemcpyAsync(c->db_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, c->own));
   if (n_seqs) ST_CUDA(cudaMemcpyAsync(c->db_len.p, len.data(), len.size() * 4, cudaMemcpyHostToDevice, c->own));
   ST_CUDA(cudaStreamSynchronize(c->own));
+  c->max_len = len.empty() ? 0 : *std::max_element(len.begin(), len.end());
   c->h_db_len = std::move(len);
   c->h_db_off.assign(off.begin(), off.end() - 1);
   c->n_seqs = n_seqs;
@@ -2786,6 +2796,261 @@ extern "C" int st_ungapped_hits(st_ctx* c, const st_hit* hits, uint64_t n, int32
   ST_CUDA(cudaMemcpyAsync(per_hit, d_out, n * 4, cudaMemcpyDeviceToHost, c->stream));
   ST_CUDA(cudaStreamSynchronize(c->stream));
   return ST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// prefilter evidence, chain and gate (st_gate.cuh)
+// ---------------------------------------------------------------------------
+static_assert(sizeof(st_seed_hit) == sizeof(GateSeedHit), "seed hit layout");
+static_assert(sizeof(st_candidate) == sizeof(GateCandidate), "candidate layout");
+static_assert(sizeof(st_prefilter_stats) == sizeof(GateStats), "stats layout");
+
+static int gate_conf(st_ctx* c, const st_prefilter_params* p, GateConf& g, int& qbits) {
+  if (!p) return fail(ST_EINVAL, "null prefilter parameters");
+  if (p->max_diagonals == 0) return fail(ST_EINVAL, "max_diagonals must be at least 1");
+  if (p->diag_hits == 0) return fail(ST_EINVAL, "diag_hits must be at least 1");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  ST_TRY(sync_profiles(c));
+  g.min_hits = p->min_hits;
+  g.diag_hits = p->diag_hits;
+  g.kmax = std::min<uint32_t>(p->max_diagonals, kGateMaxDiags);
+  g.window = p->diag_window;
+  g.span = p->span;
+  g.min_score = p->min_diag_score;
+  g.open = p->gap_open;
+  g.ext = p->gap_ext;
+  g.max_cand = p->max_candidates;
+  g.regions = p->regions ? 1u : 0u;
+  g.n_prof = static_cast<uint32_t>(c->profs.size());
+  g.tbits = static_cast<uint32_t>(bits_for(c->n_seqs ? c->n_seqs - 1 : 0));
+  g.doff = c->max_m;
+  g.dbits = static_cast<uint32_t>(bits_for(static_cast<uint64_t>(c->max_m) + c->max_len));
+  qbits = bits_for(g.n_prof);  // n_prof itself marks rejected hits
+  if (qbits + static_cast<int>(g.tbits + g.dbits) > 64 || qbits > 32)
+    return fail(ST_EINVAL, "seed-hit key needs %d bits (query %d, target %u, diagonal %u); at most 64",
+                qbits + static_cast<int>(g.tbits + g.dbits), qbits, g.tbits, g.dbits);
+  if (16 + static_cast<size_t>(kProfRows) * ung_stride(c) + 16 > static_cast<size_t>(g_gate_smem))
+    return fail(ST_EINVAL, "query too long for the prefilter segment kernel (%u rows)", c->max_m);
+  return ST_OK;
+}
+
+// The whole pipeline on the context stream, one host synchronisation (the
+// number of candidates, which sizes the ranking sort) and a final one for the
+// counts.  Ranked candidates go to d_out (room for n entries).
+static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const GateConf& g, int qbits,
+                         GateCandidate* d_out, uint64_t* n_out, GateStats* h_stats) {
+  const int key_bits = qbits + static_cast<int>(g.tbits + g.dbits);
+  const size_t P = static_cast<size_t>(g.n_prof) + 1;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o += up256(std::max<size_t>(bytes, 1));
+    return r;
+  };
+  const size_t o_k0 = take(8ull * n), o_k1 = take(8ull * n), o_v0 = take(4ull * n), o_v1 = take(4ull * n);
+  const size_t o_start = take(4ull * n), o_ng = take(4), o_ns = take(4ull * (n + 1)), o_joff = take(4ull * (n + 1));
+  const size_t o_jobs = take(sizeof(GateJob) * n), o_sc = take(4ull * n), o_qs = take(4ull * n),
+               o_qe = take(4ull * n);
+  const size_t o_cand = take(sizeof(GateCandidate) * n), o_flag = take(n), o_sel = take(4ull * n), o_nc = take(4);
+  const size_t o_stats = take(sizeof(GateStats)), o_nout = take(8);
+  const size_t o_qf = take(4 * P), o_qend = take(4 * P), o_kept = take(4 * P), o_koff = take(4 * P);
+  // CUB scratch, sized for the largest input of each call
+  size_t t_max = 0, t = 0;
+  {
+    cub::DoubleBuffer<uint64_t> kb(nullptr, nullptr);
+    cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t, kb, vb, n, 0, key_bits, c->stream));
+    t_max = std::max(t_max, t);
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t, kb, vb, n, 0, 31 + qbits, c->stream));
+    t_max = std::max(t_max, t);
+    cub::CountingInputIterator<uint32_t> it(0);
+    ST_CUDA(cub::DeviceSelect::Flagged(nullptr, t, it, static_cast<const uint8_t*>(nullptr),
+                                       static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr), n,
+                                       c->stream));
+    t_max = std::max(t_max, t);
+    ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t, static_cast<uint32_t*>(nullptr),
+                                          static_cast<uint32_t*>(nullptr), n + 1, c->stream));
+    t_max = std::max(t_max, t);
+    ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t, static_cast<uint32_t*>(nullptr),
+                                          static_cast<uint32_t*>(nullptr), P, c->stream));
+    t_max = std::max(t_max, t);
+  }
+  const size_t o_tmp = take(t_max);
+  DevMem mem;
+  ST_TRY(pool_get(c, o, mem));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
+  } back{c, &mem};
+  char* b = mem.as<char>();
+  auto at = [&](size_t off) { return static_cast<void*>(b + off); };
+  uint64_t* k0 = static_cast<uint64_t*>(at(o_k0));
+  uint64_t* k1 = static_cast<uint64_t*>(at(o_k1));
+  uint32_t* v0 = static_cast<uint32_t*>(at(o_v0));
+  uint32_t* v1 = static_cast<uint32_t*>(at(o_v1));
+  uint32_t* start = static_cast<uint32_t*>(at(o_start));
+  uint32_t* ng = static_cast<uint32_t*>(at(o_ng));
+  uint32_t* ns = static_cast<uint32_t*>(at(o_ns));
+  uint32_t* joff = static_cast<uint32_t*>(at(o_joff));
+  GateJob* jobs = static_cast<GateJob*>(at(o_jobs));
+  int32_t* sc = static_cast<int32_t*>(at(o_sc));
+  int32_t* qs = static_cast<int32_t*>(at(o_qs));
+  int32_t* qe = static_cast<int32_t*>(at(o_qe));
+  GateCandidate* cand = static_cast<GateCandidate*>(at(o_cand));
+  uint8_t* flag = static_cast<uint8_t*>(at(o_flag));
+  uint32_t* sel = static_cast<uint32_t*>(at(o_sel));
+  uint32_t* nc = static_cast<uint32_t*>(at(o_nc));
+  GateStats* st = static_cast<GateStats*>(at(o_stats));
+  unsigned long long* nout = static_cast<unsigned long long*>(at(o_nout));
+  uint32_t* qf = static_cast<uint32_t*>(at(o_qf));
+  uint32_t* qend = static_cast<uint32_t*>(at(o_qend));
+  uint32_t* kept = static_cast<uint32_t*>(at(o_kept));
+  uint32_t* koff = static_cast<uint32_t*>(at(o_koff));
+  void* tmp = at(o_tmp);
+  cudaStream_t s = c->stream;
+  const uint32_t cap_grid = static_cast<uint32_t>(c->sms) * 8;
+  auto grid_for = [&](uint64_t items, uint32_t block) {
+    return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>((items + block - 1) / block, cap_grid)));
+  };
+  ST_CUDA(cudaMemsetAsync(st, 0, sizeof(GateStats), s));
+  // keys, sort, groups
+  DeviceDb db = db_view(c);
+  DeviceProfiles pv = prof_view(c);
+  gate_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_hits, n, db, pv.qlen, g, k0, v0, st);
+  cub::DoubleBuffer<uint64_t> kb(k0, k1);
+  cub::DoubleBuffer<uint32_t> vb(v0, v1);
+  t = t_max;
+  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t, kb, vb, n, 0, key_bits, s));
+  GateGroups G{kb.Current(), vb.Current(), start, ng, n};
+  {
+    cub::CountingInputIterator<uint32_t> it(0);
+    cub::TransformInputIterator<bool, GateHeadFlag, cub::CountingInputIterator<uint32_t>> heads(
+        it, GateHeadFlag{kb.Current(), g.dbits});
+    t = t_max;
+    ST_CUDA(cub::DeviceSelect::Flagged(tmp, t, it, heads, start, ng, n, s));
+  }
+  // jobs
+  gate_count_kernel<<<grid_for(static_cast<uint64_t>(n) + 1, 256), 256, 0, s>>>(G, g, ns, st);
+  t = t_max;
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t, ns, joff, n + 1, s));
+  if (g.kmax <= 4)
+    gate_emit_kernel<4><<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv.qlen, ns, joff, jobs);
+  else
+    gate_emit_kernel<kGateMaxDiags><<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv.qlen, ns, joff, jobs);
+  // segments
+  GateSegParams sp{db, pv, jobs, ng, joff, sc, qs, qe, ung_stride(c)};
+  const size_t smem = 16 + static_cast<size_t>(kProfRows) * sp.max_m_pad + 16;
+  gate_segment_kernel<<<static_cast<uint32_t>((static_cast<uint64_t>(n) + kGateChunk - 1) / kGateChunk), 256, smem,
+                        s>>>(sp);
+  // chain, gate, compaction
+  ST_CUDA(cudaMemsetAsync(flag, 0, n, s));
+  gate_chain_kernel<<<grid_for(n, 128), 128, 0, s>>>(G, g, joff, jobs, sc, qs, qe, cand, flag, st);
+  {
+    cub::CountingInputIterator<uint32_t> it(0);
+    t = t_max;
+    ST_CUDA(cub::DeviceSelect::Flagged(tmp, t, it, flag, sel, nc, n, s));
+  }
+  c->launches += 7;
+  ST_CUDA(cudaGetLastError());
+  ST_TRY(c->pin.reserve(64));
+  uint32_t* h_nc = c->pin.as<uint32_t>();
+  ST_CUDA(cudaMemcpyAsync(h_nc, nc, 4, cudaMemcpyDeviceToHost, s));
+  ST_CUDA(cudaStreamSynchronize(s));
+  const uint32_t n_cand = *h_nc;
+  // ranking: the sort keys reuse the hit-key buffers (free after the jobs are emitted)
+  if (n_cand) {
+    gate_rank_keys_kernel<<<grid_for(n_cand, 256), 256, 0, s>>>(cand, sel, nc, k0, v0);
+    cub::DoubleBuffer<uint64_t> rk(k0, k1);
+    cub::DoubleBuffer<uint32_t> ri(v0, v1);
+    t = t_max;
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t, rk, ri, n_cand, 0, 31 + qbits, s));
+    if (g.max_cand) {
+      ST_CUDA(cudaMemsetAsync(qf, 0, 4 * P, s));
+      ST_CUDA(cudaMemsetAsync(qend, 0, 4 * P, s));
+      gate_query_bounds_kernel<<<grid_for(n_cand, 256), 256, 0, s>>>(rk.Current(), nc, qf, qend);
+      gate_query_kept_kernel<<<grid_for(P, 256), 256, 0, s>>>(qf, qend, g.n_prof, g.max_cand, kept);
+      t = t_max;
+      ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t, kept, koff, P, s));
+      c->launches += 2;
+    }
+    gate_gather_kernel<<<grid_for(n_cand, 256), 256, 0, s>>>(cand, rk.Current(), ri.Current(), nc, g.max_cand, qf,
+                                                             koff, d_out);
+    c->launches += 2;
+  }
+  gate_finish_kernel<<<1, 1, 0, s>>>(ng, joff, nc, koff, g.n_prof, n_cand ? g.max_cand : 0, st, nout);
+  ++c->launches;
+  ST_CUDA(cudaGetLastError());
+  GateStats* h_st = reinterpret_cast<GateStats*>(c->pin.as<char>());
+  ST_CUDA(cudaMemcpyAsync(h_st, st, sizeof(GateStats), cudaMemcpyDeviceToHost, s));
+  ST_CUDA(cudaStreamSynchronize(s));
+  *h_stats = *h_st;
+  *n_out = h_st->candidates;
+  return ST_OK;
+}
+
+static int gate_check_n(uint64_t n) {
+  if (n >= 0x7FFFFFFFull) return fail(ST_EINVAL, "too many seed hits in one call (%llu; fewer than 2^31 - 1)",
+                                      static_cast<unsigned long long>(n));
+  return ST_OK;
+}
+
+static int gate_result(const GateStats& st, st_prefilter_stats* stats) {
+  if (stats) memcpy(stats, &st, sizeof st);
+  if (st.hits_rejected)
+    return fail(ST_EINVAL, "%llu seed hits lie outside their query or target (unknown ids or positions)",
+                st.hits_rejected);
+  return ST_OK;
+}
+
+extern "C" int st_prefilter_gate_device(st_ctx* c, const st_seed_hit* d_hits, uint64_t n,
+                                        const st_prefilter_params* params, st_candidate* d_out, uint64_t* n_out,
+                                        st_prefilter_stats* stats) {
+  CTX_GUARD(c);
+  if (!n_out || (n && (!d_hits || !d_out))) return fail(ST_EINVAL, "st_prefilter_gate_device: null argument");
+  ST_TRY(gate_check_n(n));
+  GateConf g;
+  int qbits = 0;
+  ST_TRY(gate_conf(c, params, g, qbits));
+  GateStats st{};
+  *n_out = 0;
+  if (n)
+    ST_TRY(gate_pipeline(c, reinterpret_cast<const GateSeedHit*>(d_hits), static_cast<uint32_t>(n), g, qbits,
+                         reinterpret_cast<GateCandidate*>(d_out), n_out, &st));
+  return gate_result(st, stats);
+}
+
+extern "C" int st_prefilter_gate(st_ctx* c, const st_seed_hit* hits, uint64_t n, const st_prefilter_params* params,
+                                 st_candidate* out, uint64_t cap, uint64_t* n_out, st_prefilter_stats* stats) {
+  CTX_GUARD(c);
+  if (!n_out || (n && !hits) || (cap && !out)) return fail(ST_EINVAL, "st_prefilter_gate: null argument");
+  ST_TRY(gate_check_n(n));
+  GateConf g;
+  int qbits = 0;
+  ST_TRY(gate_conf(c, params, g, qbits));
+  GateStats st{};
+  *n_out = 0;
+  if (n) {
+    DevMem buf;
+    const size_t hb = up256(n * sizeof(st_seed_hit));
+    ST_TRY(pool_get(c, hb + n * sizeof(st_candidate), buf));
+    struct Back {
+      st_ctx* c;
+      DevMem* m;
+      ~Back() { pool_put_after(c, std::move(*m), c->stream); }
+    } back{c, &buf};
+    char* d = buf.as<char>();
+    ST_CUDA(cudaMemcpyAsync(d, hits, n * sizeof(st_seed_hit), cudaMemcpyHostToDevice, c->stream));
+    GateCandidate* d_out = reinterpret_cast<GateCandidate*>(d + hb);
+    ST_TRY(gate_pipeline(c, reinterpret_cast<const GateSeedHit*>(d), static_cast<uint32_t>(n), g, qbits, d_out,
+                         n_out, &st));
+    const uint64_t k = std::min<uint64_t>(cap, *n_out);
+    if (k) {
+      ST_CUDA(cudaMemcpyAsync(out, d_out, k * sizeof(st_candidate), cudaMemcpyDeviceToHost, c->stream));
+      ST_CUDA(cudaStreamSynchronize(c->stream));
+    }
+  }
+  return gate_result(st, stats);
 }
 
 // ---------------------------------------------------------------------------

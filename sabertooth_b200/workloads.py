@@ -410,3 +410,94 @@ def config2(seed=0, n_queries=1000, n_targets=374_000, n_hits=20_000_000, homolo
     return HitWorkload("config2-ungapped-hits", [seq_rows(model, q) for q in queries], arena, offs, hits,
                        info={"queries": n_queries, "targets": n_targets, "hits": n_hits, "db_residues": total,
                              "seed": seed})
+
+
+# ---- seed hits for the evidence / chain / gate stage -------------------------
+@dataclass
+class SeedHitWorkload:
+    name: str
+    rows: list
+    db_residues: np.ndarray
+    db_offsets: np.ndarray
+    hits: np.ndarray  # SEED_HIT_DTYPE, in generation order (not sorted)
+    info: dict = field(default_factory=dict)
+
+
+def seed_hits(seed=0, n_queries=1000, n_targets=374_000, n_hits=20_000_000, homolog_frac=0.10,
+              homolog_hit_frac=0.30, keep=0.55, max_gap=12, model=None):
+    """Seed hits with query positions on the config-2 database shape.  Each
+    homolog target holds a copy of a random query segment in two pieces on
+    diagonals that differ by an insertion or deletion of 1..max_gap residues
+    (substitutions keep `keep` of the sites); homolog hits lie on either
+    piece's diagonal at a position inside that piece, the rest are uniform over
+    random (query, target, valid diagonal, position on it)."""
+    from ._lib import SEED_HIT_DTYPE
+    model = model or Model()
+    rng = Rng(seed)
+    ql = lognormal_lengths(rng, n_queries, 250, 0.5, 30, 1000)
+    queries = [model.background(rng.child(i), int(l)) for i, l in enumerate(ql)]
+    tl = lognormal_lengths(rng, n_targets, 160, 0.55, 30, 1000)
+    hom = rng.uniform(n_targets) < homolog_frac
+    src_q = rng.below(n_targets, n_queries)
+    total = int(tl.sum())
+    arena = model.background(rng.child(99), total)
+    offs = np.zeros(n_targets + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum(tl)
+    hom_t = np.nonzero(hom)[0]
+    # piece k of target t: query positions [pq0, pq1) on diagonal pd
+    pq0 = np.zeros((n_targets, 2), dtype=np.int64)
+    pq1 = np.zeros((n_targets, 2), dtype=np.int64)
+    pd = np.zeros((n_targets, 2), dtype=np.int64)
+    hr = rng.child(98)
+    for t in hom_t:
+        q = queries[src_q[t]]
+        n = int(tl[t])
+        a = int(offs[t])
+        L = min(q.size, n) - max_gap
+        if L < 20:
+            continue
+        qs = int(hr.below(1, q.size - L + 1)[0])
+        g = int(hr.below(1, 2 * max_gap + 1)[0]) - max_gap  # > 0: insertion in the target, < 0: deletion
+        g = g if g != 0 else 1
+        ts = int(hr.below(1, n - L - max(g, 0) + 1)[0])
+        cut = L // 2
+        seg = model.mutate(hr, q[qs:qs + L], keep)
+        # piece 0: q[qs, qs+cut) at ts; piece 1 continues after the indel
+        arena[a + ts:a + ts + cut] = seg[:cut]
+        if g > 0:
+            arena[a + ts + cut:a + ts + cut + g] = model.background(hr, g)
+            q1, t1 = qs + cut, ts + cut + g
+        else:
+            q1, t1 = qs + cut - g, ts + cut
+        l1 = min(qs + L - q1, n - t1)
+        arena[a + t1:a + t1 + l1] = seg[q1 - qs:q1 - qs + l1]
+        pq0[t] = (qs, q1)
+        pq1[t] = (qs + cut, q1 + l1)
+        pd[t] = (ts - qs, t1 - q1)
+    hom_t = hom_t[pq1[hom_t, 0] > pq0[hom_t, 0]]
+    n_hom = int(n_hits * homolog_hit_frac) if hom_t.size else 0
+    n_rand = n_hits - n_hom
+    ht = hom_t[rng.below(n_hom, max(hom_t.size, 1))] if n_hom else np.zeros(0, np.int64)
+    piece = rng.below(n_hom, 2)
+    a0 = pq0[ht, piece]
+    a1 = pq1[ht, piece]
+    hqp = a0 + (rng.u64(n_hom) % np.maximum(a1 - a0, 1).astype(np.uint64)).astype(np.int64)
+    hd = pd[ht, piece]
+    hq = src_q[ht]
+    rq = rng.below(n_rand, n_queries)
+    rt = rng.below(n_rand, n_targets)
+    m_r = ql[rq]
+    n_r = tl[rt]
+    rd = -(m_r - 1) + (rng.u64(n_rand) % (m_r + n_r - 1).astype(np.uint64)).astype(np.int64)
+    lo = np.maximum(-rd, 0)
+    hi = np.minimum(m_r, n_r - rd)
+    rqp = lo + (rng.u64(n_rand) % np.maximum(hi - lo, 1).astype(np.uint64)).astype(np.int64)
+    hits = np.zeros(n_hom + n_rand, dtype=SEED_HIT_DTYPE)
+    hits["query"] = np.concatenate([hq, rq]).astype(np.uint32)
+    hits["target"] = np.concatenate([ht, rt]).astype(np.uint32)
+    hits["diag"] = np.concatenate([hd, rd]).astype(np.int32)
+    hits["qpos"] = np.concatenate([hqp, rqp]).astype(np.uint32)
+    perm = np.argsort(rng.u64(hits.size), kind="stable")
+    return SeedHitWorkload("seed-hits-gate", [seq_rows(model, q) for q in queries], arena, offs, hits[perm],
+                           info={"queries": n_queries, "targets": n_targets, "hits": int(hits.size),
+                                 "db_residues": total, "homolog_targets": int(hom_t.size), "seed": seed})
