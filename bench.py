@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--serving-pairs", type=int, default=20000, help="config-4 requests for the serving measurement (0: skip)")
     ap.add_argument("--ungapped-hits", type=int, default=20_000_000, help="config-2 hits for the ungapped measurement (0: skip)")
     ap.add_argument("--serving-seconds", type=float, default=2.0, help="arrival window per swept rate")
+    ap.add_argument("--gate-hits", type=int, default=20_000_000,
+                    help="seed hits for the evidence / chain / gate measurement (0: skip)")
     return ap.parse_args()
 
 
@@ -433,6 +435,8 @@ def main():
     plan.close()
     if result is not None and args.ungapped_hits > 0:
         result["ungapped"] = ungapped_measure(ctx, args)
+    if result is not None and args.gate_hits > 0:
+        result["gate"] = gate_measure(ctx, args)
     if result is not None and args.serving_pairs > 0:
         result["serving"] = serving_measure(ctx, args)
     if world > 1:
@@ -519,6 +523,136 @@ def ungapped_measure(ctx, args):
                                                        "window-start order, exact rescore) restated in C, queries in "
                                                        "parallel over all host threads"},
             "setup_s": round(t_gen, 1)}
+
+
+def gate_measure(ctx, args):
+    """Prefilter evidence -> chain -> gate (score_and_gate, src/prefilter.rs:1412-1660, ranking :1074-1083) on
+    seed hits with query positions over the config-2 database shape: 1,000 queries, 374,000 targets (68 M
+    residues), 2x10^7 hits (30% on two-piece planted homologs), sequence defaults (4 diagonals, window 48,
+    span 6, gate 42, gaps 11/1), regions on.  Device-resident hits per step: one st_prefilter_gate_device call
+    (sort, groups, top diagonals, segments, chains, gate, ranking).  e2e: st_prefilter_gate from host hits to
+    host candidates.  Algorithmic bytes: 16 B per hit + the residues of every scored window + 32 B per
+    candidate, against the measured HBM copy bandwidth."""
+    import torch
+    from oracle import oracle as O
+    from sabertooth_b200 import GapCosts, PrefilterParams
+    from sabertooth_b200 import workloads as W
+    t0 = time.perf_counter()
+    w = W.seed_hits(seed=args.seed, n_hits=args.gate_hits)
+    t_gen = time.perf_counter() - t0
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    hits = w.hits.copy()
+    hits["query"] = ids[hits["query"]]
+    n = len(hits)
+    params = PrefilterParams(regions=True)
+    gaps = GapCosts.sequence_default()
+    st = torch.cuda.Stream()
+    ctx.set_stream(st.cuda_stream)
+    d_hits = torch.from_numpy(hits.view(np.uint8)).cuda()
+    d_out = torch.empty(n * 32, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            n_c, stats = ctx.prefilter_gate_device(d_hits.data_ptr(), n, d_out.data_ptr(), params, gaps)
+        ts = []
+        for _ in range(max(3, args.steps)):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            n_c, stats = ctx.prefilter_gate_device(d_hits.data_ptr(), n, d_out.data_ptr(), params, gaps)
+            b.record(st)
+            st.synchronize()
+            ts.append(a.elapsed_time(b))
+    got_dev = d_out[:n_c * 32].cpu().numpy().view(O.CANDIDATE_DTYPE)
+    ctx.set_stream(0)
+    ms = float(np.median(ts))
+    # e2e: host hits in, host candidates out
+    te = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        got, _ = ctx.prefilter_gate(hits, params, gaps)
+        te.append(time.perf_counter() - t0)
+    ms_e2e = float(np.median(te)) * 1e3
+    # CPU baseline: the oracle's restatement of the reference's evidence stage with its AVX2 batched Kadane,
+    # queries in parallel over all host threads, on the whole workload; its candidates are the parity check
+    targets = [w.db_residues[int(a_):int(b_)] for a_, b_ in zip(w.db_offsets[:-1], w.db_offsets[1:])]
+    arena = O.Arena(w.rows, targets)
+    p = {"min_hits": params.min_hits, "diag_hits": params.diag_hits, "max_diagonals": params.max_diagonals,
+         "diag_window": params.diag_window, "span": params.span, "min_diag_score": params.min_diag_score,
+         "gap_open": gaps.open, "gap_ext": gaps.extend, "max_candidates": params.max_candidates, "regions": 1}
+    t_runs = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        want, wst = O.prefilter_queries(arena, w.hits["query"], w.hits["target"], w.hits["diag"], w.hits["qpos"], p)
+        t_runs.append(time.perf_counter() - t0)
+    t_cpu = float(np.median(t_runs))
+    mapped = got.copy()
+    inv = np.zeros(int(ids.max()) + 1, dtype=np.int64)
+    inv[ids] = np.arange(len(ids))
+    mapped["query"] = inv[got["query"]]
+    order = np.argsort(mapped["query"], kind="stable")
+    same = bool(len(mapped) == len(want) and np.array_equal(mapped[order], want))
+    same_stats = all(stats[k] == wst[k] for k in wst)
+    # algorithmic bytes: hits, scored windows, candidates
+    win = gate_window_bytes(w, params)
+    ab = 16 * n + win + 32 * int(n_c)
+    peak = hbm_peak_gbs()
+    gbs = ab / (ms * 1e-3) / 1e9
+    ctx.free_profiles(ids)
+    return {"workload": f"seed hits: {len(w.rows)} queries, {len(w.db_offsets) - 1} targets "
+                        f"({int(w.db_offsets[-1]) / 1e6:.1f} M residues), {n} hits (30% on two-piece homologs); "
+                        "sequence defaults, regions on",
+            "ms_per_step": round(ms, 3), "mhits_per_s": round(n / ms / 1e3, 1),
+            "e2e": {"ms_per_call": round(ms_e2e, 3), "mhits_per_s": round(n / ms_e2e / 1e3, 1),
+                    "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(32 * int(n_c))},
+            "candidates": int(n_c), "stats": {k: int(v) for k, v in stats.items()},
+            "algorithmic_bytes": int(ab),
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "traffic": None},
+            "matches_cpu_baseline": same, "stats_match_cpu_baseline": same_stats,
+            "device_matches_host": bool(np.array_equal(got_dev, got)),
+            "cpu_baseline": {"value": round(n / t_cpu / 1e6, 2), "unit": "Mhits/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"the whole workload ({n} hits), median of 2 runs: the "
+                                                       "reference's evidence stage (hits sorted per query, top "
+                                                       "diagonals, AVX2 batched Kadane, lazy segment positions, "
+                                                       "chains, gate, ranking) restated in C, queries in parallel "
+                                                       "over all host threads"},
+            "setup_s": round(t_gen, 1)}
+
+
+def gate_window_bytes(w, params):
+    """Residues of every scored window: per (query, target), its top diagonals by hit count (at most
+    max_diagonals, ties to the smaller diagonal), each over [qmin - window, qmax + span + window) clipped
+    to the diagonal."""
+    h = w.hits
+    q = h["query"].astype(np.int64)
+    t = h["target"].astype(np.int64)
+    d = h["diag"].astype(np.int64)
+    qp = h["qpos"].astype(np.int64)
+    order = np.lexsort((d, t, q))
+    q, t, d, qp = q[order], t[order], d[order], qp[order]
+    run = np.ones(len(q), dtype=bool)
+    run[1:] = (q[1:] != q[:-1]) | (t[1:] != t[:-1]) | (d[1:] != d[:-1])
+    idx = np.nonzero(run)[0]
+    cnt = np.diff(np.append(idx, len(q)))
+    qmin = np.minimum.reduceat(qp, idx)
+    qmax = np.maximum.reduceat(qp, idx)
+    rq, rt, rd = q[idx], t[idx], d[idx]
+    # rank of each run inside its (query, target) by count desc, diagonal asc
+    o2 = np.lexsort((rd, -cnt, rt, rq))
+    rq, rt, rd, cnt, qmin, qmax = rq[o2], rt[o2], rd[o2], cnt[o2], qmin[o2], qmax[o2]
+    grp = np.ones(len(rq), dtype=bool)
+    grp[1:] = (rq[1:] != rq[:-1]) | (rt[1:] != rt[:-1])
+    gstart = np.maximum.accumulate(np.where(grp, np.arange(len(rq)), 0))
+    keep = (np.arange(len(rq)) - gstart) < min(params.max_diagonals, 16)
+    m = np.array([len(r) for r in w.rows], dtype=np.int64)[rq]
+    nl = np.diff(w.db_offsets.astype(np.int64))[rt]
+    lo = np.maximum(np.maximum(-rd, 0), np.maximum(qmin - params.diag_window, 0))
+    hi = np.minimum(np.minimum(m, nl - rd), qmax + params.span + params.diag_window)
+    return int(np.maximum(hi - lo, 0)[keep].sum())
 
 
 def hbm_peak_gbs():

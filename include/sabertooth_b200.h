@@ -271,6 +271,32 @@ int st_prefilter_gate(st_ctx* ctx, const st_seed_hit* hits, uint64_t n, const st
 int st_prefilter_gate_device(st_ctx* ctx, const st_seed_hit* d_hits, uint64_t n, const st_prefilter_params* params,
                              st_candidate* d_out, uint64_t* n_out, st_prefilter_stats* stats);
 
+/* ---- per-profile calibration ----------------------------------------------
+ * calibrate_profile (src/evalue.rs:714-748) for many profiles at once: sample i
+ * (0 <= i < samples) is a background target drawn from the SplitMix64 stream
+ * stream_seed(seed, 0xBEEF, i) (src/evalue.rs:53-81): length
+ * lengths[below(n_lengths)] (at least 1), residues from BackgroundSampler
+ * (:84-114) over p_back (the 20 standard background probabilities of the
+ * matrix).  Every profile is scored against every sample (exact SW-Gotoh, the
+ * batched path; the targets are generated on the device and replace the
+ * database for this call only), then a Gumbel is fitted by maximum likelihood
+ * (fit_gumbel_ml, :138-182) and K = exp(lambda (mu + 1/2)) / (m * mean length).
+ * The reference calls it per PSSM with the search's seed (0x5EED) and a sample
+ * of database lengths (src/search.rs:467-481), so all profiles of a search
+ * share the same targets.  out[p].ok = 0 where the reference returns None
+ * (no lengths, an empty profile, fewer than 10 samples, a degenerate fit).
+ * scores may be NULL, else [n_profiles][samples]. */
+typedef struct {
+  double lambda;
+  double k;
+  double mu;
+  uint32_t n;  /* samples */
+  int32_t ok;
+} st_calibration;
+int st_calibrate_profiles(st_ctx* ctx, const uint32_t* profiles, uint32_t n_profiles, const uint32_t* lengths,
+                          uint32_t n_lengths, uint32_t samples, uint64_t seed, const double* p_back, int32_t open,
+                          int32_t ext, int32_t* scores, st_calibration* out);
+
 /* ---- end cells and alignment spans ---------------------------------------
  * Score plus end cell, the first optimum in column-major order (smallest target
  * position, then smallest query position): QueryProfile::sw_score_end_with

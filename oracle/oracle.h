@@ -121,6 +121,22 @@ void or_prefilter_queries(const int32_t* rows_arena, const uint64_t* row_off, co
 void or_kadane_jobs_avx2(const int32_t* rows, uint32_t m, const uint8_t* const* tp, const int64_t* d,
                          const uint32_t* lo, const uint32_t* hi, uint32_t n, int32_t* out);
 
+/* ---- per-profile calibration (calib.c) ----------------------------------------
+ * calibrate_profile (src/evalue.rs:714-748): background targets from per-sample
+ * SplitMix64 streams, exact SW scores, ML Gumbel fit.  Returns 0 where the
+ * reference returns None; scores[samples] are written whenever n_lengths and m
+ * are non-zero. */
+uint64_t or_stream_seed(uint64_t seed, uint64_t c, uint64_t i);
+void or_background_cum(const double* p_back20, double* cum20);
+uint32_t or_calibration_length(const uint32_t* lengths, uint32_t n_lengths, uint64_t seed, uint64_t i);
+void or_calibration_target(const uint32_t* lengths, uint32_t n_lengths, uint64_t seed, uint64_t i, const double* cum20,
+                           uint8_t* out, uint32_t* len);
+double or_gumbel_mu_given_lambda(const double* xs, uint64_t n, double lambda);
+int or_fit_gumbel_ml(const double* xs, uint64_t n, double* lambda, double* mu);
+int or_calibrate_profile(const int32_t* rows, uint32_t m, const uint32_t* lengths, uint32_t n_lengths,
+                         uint32_t samples, uint64_t seed, const double* p_back20, int32_t open, int32_t ext,
+                         int32_t* scores, double* lambda, double* k, double* mu, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,6 +42,14 @@ def _load():
     lib.or_ungapped_hits_avx2.argtypes = [P, P, P, P, P, P, P, P, u64, P, C.c_int]
     lib.or_striped_queries.argtypes = [P, P, P, u32, P, P, P, P, i32, i32, P, P, C.c_int]
     lib.or_prefilter_queries.argtypes = [P, P, P, P, u32, P, P, P, P, P, P, P, C.c_int, P, P, P, C.c_int]
+    lib.or_background_cum.argtypes = [P, P]
+    lib.or_stream_seed.restype = u64
+    lib.or_stream_seed.argtypes = [u64, u64, u64]
+    lib.or_calibration_target.argtypes = [P, u32, u64, u64, P, P, P]
+    lib.or_fit_gumbel_ml.restype = C.c_int
+    lib.or_fit_gumbel_ml.argtypes = [P, u64, P, P]
+    lib.or_calibrate_profile.restype = C.c_int
+    lib.or_calibrate_profile.argtypes = [P, u32, P, u32, u32, u64, P, i32, i32, P, P, P, P, C.c_int]
     return lib
 
 
@@ -212,3 +220,40 @@ def prefilter_queries(arena: Arena, hq, ht, hd, hqpos, params: dict, simd=True, 
     cands = np.concatenate(parts) if parts else np.zeros(0, dtype=CANDIDATE_DTYPE)
     tot = stats[:len(qids)].sum(axis=0) if len(qids) else np.zeros(len(STATS_FIELDS), np.uint64)
     return cands, {f: int(v) for f, v in zip(STATS_FIELDS, tot)}
+
+
+# ---- per-profile calibration (calib.c) ------------------------------------------
+def background_cum(p_back20):
+    p = np.ascontiguousarray(p_back20, dtype=np.float64)
+    out = np.zeros(20, dtype=np.float64)
+    lib.or_background_cum(_p(p), _p(out))
+    return out
+
+
+def calibration_target(lengths, seed, i, p_back20):
+    """Background target i of the calibration stream (src/evalue.rs:728-731)."""
+    lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+    cum = background_cum(p_back20)
+    out = np.zeros(int(lengths.max()) + 1, dtype=np.uint8)
+    n = C.c_uint32()
+    lib.or_calibration_target(_p(lengths), len(lengths), seed, i, _p(cum), _p(out), C.byref(n))
+    return out[:n.value].copy()
+
+
+def fit_gumbel_ml(xs):
+    xs = np.ascontiguousarray(xs, dtype=np.float64)
+    lam, mu = C.c_double(), C.c_double()
+    ok = lib.or_fit_gumbel_ml(_p(xs), len(xs), C.byref(lam), C.byref(mu))
+    return (lam.value, mu.value) if ok else None
+
+
+def calibrate_profile(rows, lengths, samples, seed, p_back20, open_, ext, threads=0):
+    """(lambda, k, mu, scores) of calibrate_profile (src/evalue.rs:714-748); None parameters where it returns None."""
+    r = _rows(rows)
+    lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+    p = np.ascontiguousarray(p_back20, dtype=np.float64)
+    scores = np.zeros(max(samples, 1), dtype=np.int32)
+    lam, k, mu = C.c_double(), C.c_double(), C.c_double()
+    ok = lib.or_calibrate_profile(_p(r), r.shape[0], _p(lengths), len(lengths), samples, seed, _p(p), open_, ext,
+                                  _p(scores), C.byref(lam), C.byref(k), C.byref(mu), threads or os.cpu_count() or 1)
+    return ((lam.value, k.value, mu.value) if ok else None), scores[:samples].copy()

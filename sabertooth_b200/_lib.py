@@ -53,6 +53,11 @@ class PrefilterParamsC(C.Structure):
                 ("regions", C.c_uint32)]
 
 
+class CalibrationC(C.Structure):
+    _fields_ = [("lambda_", C.c_double), ("k", C.c_double), ("mu", C.c_double), ("n", C.c_uint32),
+                ("ok", C.c_int32)]
+
+
 class PrefilterStatsC(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in PREFILTER_STATS_FIELDS]
 
@@ -97,6 +102,7 @@ SIGNATURES = {
     "st_ungapped_hits_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
     "st_prefilter_gate": (C.c_int, [_P, _P, _u64, _P, _P, _u64, _P, _P]),
     "st_prefilter_gate_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P]),
+    "st_calibrate_profiles": (C.c_int, [_P, _P, _u32, _P, _u32, _u32, _u64, _P, _i32, _i32, _P, _P]),
     "st_tune_num_classes": (C.c_int, []),
     "st_tune_class_shape": (C.c_int, [C.c_int, _P, _P, _P]),
     "st_tune_get": (C.c_int, [_P, _P]),

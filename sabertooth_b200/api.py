@@ -140,6 +140,12 @@ class Context:
         self.n_seqs = n
         self.db_lengths = np.diff(offsets).astype(np.uint32)
 
+    def db_info(self):
+        """(sequences, residues) of the device database."""
+        n, r = C.c_uint32(), C.c_uint64()
+        check(lib.st_db_info(self._h, C.byref(n), C.byref(r)))
+        return n.value, r.value
+
     def upload_db_list(self, seqs):
         offs = np.zeros(len(seqs) + 1, dtype=np.uint64)
         offs[1:] = np.cumsum([len(s) for s in seqs])
@@ -282,6 +288,28 @@ class Context:
         check(lib.st_prefilter_gate_device(self._h, C.c_void_p(d_hits_ptr), n, C.byref(prm), C.c_void_p(d_out_ptr),
                                            C.byref(n_out), C.byref(st)))
         return n_out.value, {f: getattr(st, f) for f in PREFILTER_STATS_FIELDS}
+
+    def calibrate_profiles(self, profile_ids, lengths, samples=2000, seed=0x5EED, gaps: GapCosts = None,
+                           p_back=None, with_scores=False):
+        """calibrate_profile (src/evalue.rs:714-748) for each profile id: a list of
+        (lambda, k, mu) per profile, None where the reference returns None.  All
+        profiles are scored against the same `samples` background targets (the
+        reference's per-search seed 0x5EED and database length sample); the
+        scoring runs on the GPU, the maximum-likelihood fits on the host."""
+        ids = np.ascontiguousarray(profile_ids, dtype=np.uint32)
+        lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+        gaps = gaps or GapCosts.profile_default()
+        if p_back is None:
+            from .matrix import blosum62
+            p_back = blosum62().p_back[:20]
+        pb = np.ascontiguousarray(p_back, dtype=np.float64)
+        out = (_lib.CalibrationC * max(len(ids), 1))()
+        sc = np.zeros((len(ids), samples), dtype=np.int32) if with_scores else None
+        check(lib.st_calibrate_profiles(self._h, ptr(ids), len(ids), ptr(lengths) if len(lengths) else None,
+                                        len(lengths), samples, seed, ptr(pb), gaps.open, gaps.extend,
+                                        ptr(sc) if sc is not None and sc.size else None, out))
+        res = [(o.lambda_, o.k, o.mu) if o.ok else None for o in out[:len(ids)]]
+        return (res, sc) if with_scores else res
 
     # -- tuning / measurement ---------------------------------------------------
     def autotune(self, pairs, gaps: GapCosts, max_pairs=200_000):

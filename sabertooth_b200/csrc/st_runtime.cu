@@ -24,6 +24,7 @@
 #include "st_ungapped.cuh"
 #include "st_dplan.cuh"
 #include "st_gate.cuh"
+#include "st_calib.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
@@ -3051,6 +3052,190 @@ extern "C" int st_prefilter_gate(st_ctx* c, const st_seed_hit* hits, uint64_t n,
     }
   }
   return gate_result(st, stats);
+}
+
+// ---------------------------------------------------------------------------
+// per-profile calibration (st_calib.cuh)
+// ---------------------------------------------------------------------------
+// The context's database, swapped out while calibration targets take its place
+// for one batched scoring call (the planner and the kernels read the context's
+// database; kernels already queued keep the pointers they were launched with).
+struct DbState {
+  DevMem arena, off, len;
+  std::vector<uint32_t> h_len;
+  std::vector<uint64_t> h_off;
+  uint32_t n_seqs = 0, max_len = 0;
+  uint64_t n_res = 0;
+  bool has = false;
+};
+
+static void swap_db(st_ctx* c, DbState& s) {
+  std::swap(c->db_arena, s.arena);
+  std::swap(c->db_off, s.off);
+  std::swap(c->db_len, s.len);
+  std::swap(c->h_db_len, s.h_len);
+  std::swap(c->h_db_off, s.h_off);
+  std::swap(c->n_seqs, s.n_seqs);
+  std::swap(c->max_len, s.max_len);
+  std::swap(c->n_res, s.n_res);
+  std::swap(c->has_db, s.has);
+}
+
+// fit_gumbel_ml and gumbel_mu_given_lambda (src/evalue.rs:129-182) in binary64
+// with the reference's summation order (index order).
+static double gumbel_mu_given_lambda(const std::vector<double>& xs, double lambda) {
+  double xmin = INFINITY;
+  for (double x : xs) xmin = std::fmin(xmin, x);
+  double s = 0.0;
+  for (double x : xs) s += std::exp(-lambda * (x - xmin));
+  return xmin - std::log(s / static_cast<double>(xs.size())) / lambda;
+}
+
+static bool fit_gumbel_ml(const std::vector<double>& xs, double* lambda, double* mu) {
+  const size_t n = xs.size();
+  if (n < 10) return false;
+  double sum = 0.0;
+  for (double x : xs) sum += x;
+  const double mean = sum / static_cast<double>(n);
+  double ss = 0.0;
+  for (double x : xs) ss += (x - mean) * (x - mean);
+  const double var = ss / (static_cast<double>(n) - 1.0);
+  if (std::isnan(var) || var <= 0.0) return false;
+  double xmin = INFINITY;
+  for (double x : xs) xmin = std::fmin(xmin, x);
+  auto g = [&](double lam) {
+    double s0 = 0.0, s1 = 0.0;
+    for (double x : xs) {
+      const double w = std::exp(-lam * (x - xmin));
+      s0 += w;
+      s1 += x * w;
+    }
+    return 1.0 / lam - mean + s1 / s0;
+  };
+  const double kPi = 3.141592653589793238462643383279502884;
+  const double lam0 = kPi / (std::sqrt(var) * std::sqrt(6.0));
+  double lo = lam0 / 10.0, hi = lam0 * 10.0;
+  if (g(lo) < 0.0 || g(hi) > 0.0) return false;
+  for (int it = 0; it < 200; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (g(mid) > 0.0)
+      lo = mid;
+    else
+      hi = mid;
+    if (hi - lo < 1e-12 * hi) break;
+  }
+  *lambda = 0.5 * (lo + hi);
+  *mu = gumbel_mu_given_lambda(xs, *lambda);
+  return true;
+}
+
+extern "C" int st_calibrate_profiles(st_ctx* c, const uint32_t* profiles, uint32_t n_profiles, const uint32_t* lengths,
+                                     uint32_t n_lengths, uint32_t samples, uint64_t seed, const double* p_back,
+                                     int32_t open, int32_t ext, int32_t* scores, st_calibration* out) {
+  CTX_GUARD(c);
+  if ((n_profiles && (!profiles || !out)) || (n_lengths && !lengths) || !p_back)
+    return fail(ST_EINVAL, "st_calibrate_profiles: null argument");
+  std::vector<uint32_t> m(n_profiles);
+  for (uint32_t i = 0; i < n_profiles; ++i) {
+    ST_TRY(check_profile(c, profiles[i]));
+    m[i] = c->profs[profiles[i]].m;
+    out[i] = st_calibration{0.0, 0.0, 0.0, samples, 0};
+  }
+  if (n_lengths == 0 || samples == 0 || n_profiles == 0) return ST_OK;  // the reference returns None
+  ST_TRY(sync_profiles(c));
+  // BackgroundSampler::new (src/evalue.rs:90-100)
+  CalibGen gen;
+  {
+    double total = 0.0;
+    for (int i = 0; i < 20; ++i) total += p_back[i];
+    double acc = 0.0;
+    for (int i = 0; i < 20; ++i) {
+      acc += p_back[i] / total;
+      gen.cum[i] = acc;
+    }
+    gen.cum[19] = 1.0;
+  }
+  // per sample: stream seed, length draw, layout
+  DbState cal;
+  cal.h_len.resize(samples);
+  cal.h_off.resize(samples);
+  std::vector<uint64_t> state(samples), off(static_cast<size_t>(samples) + 1);
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < samples; ++i) {
+    uint64_t s = seed ^ (0xBEEFull * 0xA24BAED4963EE407ull) ^ (static_cast<uint64_t>(i) * 0x9FB21C651E98DF25ull);
+    s += kSplitMixGamma;
+    s = splitmix_mix(s);  // stream_seed: the first output of the derived generator
+    s += kSplitMixGamma;
+    const uint32_t n = std::max<uint32_t>(lengths[splitmix_mix(s) % n_lengths], 1u);
+    state[i] = s;
+    cal.h_len[i] = n;
+    cal.h_off[i] = total;
+    off[i] = total;
+    cal.max_len = std::max(cal.max_len, n);
+    cal.n_res += n;
+    total += up16(n);
+  }
+  off[samples] = total;
+  cal.n_seqs = samples;
+  cal.has = true;
+  const size_t arena_bytes = total + 32;
+  ST_TRY(dev_alloc(&c->mt, cal.arena, arena_bytes));
+  ST_TRY(dev_alloc(&c->mt, cal.off, off.size() * 8));
+  ST_TRY(dev_alloc(&c->mt, cal.len, static_cast<size_t>(samples) * 4));
+  DevMem st_dev;
+  ST_TRY(pool_get(c, static_cast<size_t>(samples) * 8, st_dev));
+  ST_CUDA(cudaMemsetAsync(cal.arena.p, kSentinel, arena_bytes, c->stream));
+  ST_CUDA(cudaMemcpyAsync(cal.off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, c->stream));
+  ST_CUDA(cudaMemcpyAsync(cal.len.p, cal.h_len.data(), static_cast<size_t>(samples) * 4, cudaMemcpyHostToDevice,
+                          c->stream));
+  ST_CUDA(cudaMemcpyAsync(st_dev.p, state.data(), static_cast<size_t>(samples) * 8, cudaMemcpyHostToDevice,
+                          c->stream));
+  gen.state = st_dev.as<uint64_t>();
+  gen.offset = cal.off.as<uint64_t>();
+  gen.length = cal.len.as<uint32_t>();
+  gen.arena = cal.arena.as<uint8_t>();
+  calib_targets_kernel<<<samples, 256, 0, c->stream>>>(gen);
+  ++c->launches;
+  ST_CUDA(cudaGetLastError());
+  // every (profile, sample) pair in one batched call against the calibration targets
+  std::vector<st_pair> pairs;
+  std::vector<uint32_t> row;  // profile index of each block of `samples` pairs
+  pairs.reserve(static_cast<size_t>(n_profiles) * samples);
+  for (uint32_t p = 0; p < n_profiles; ++p) {
+    if (m[p] == 0) continue;  // the reference returns None for an empty table
+    row.push_back(p);
+    for (uint32_t i = 0; i < samples; ++i) pairs.push_back(st_pair{profiles[p], i, 0, -1});
+  }
+  std::vector<int32_t> sc(pairs.size());
+  swap_db(c, cal);
+  const int rc = pairs.empty() ? ST_OK : st_sw_score_pairs(c, pairs.data(), pairs.size(), open, ext, sc.data(), nullptr);
+  swap_db(c, cal);
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  pool_put(c, std::move(st_dev));
+  if (rc != ST_OK) return rc;
+  if (scores) {
+    memset(scores, 0, static_cast<size_t>(n_profiles) * samples * 4);
+    for (size_t r = 0; r < row.size(); ++r)
+      memcpy(scores + static_cast<size_t>(row[r]) * samples, sc.data() + r * samples, static_cast<size_t>(samples) * 4);
+  }
+  // ML Gumbel fit per profile, K over the search space m * (N_t * mean length) (src/evalue.rs:739-747)
+  uint64_t lsum = 0;
+  for (uint32_t i = 0; i < n_lengths; ++i) lsum += lengths[i];
+  const double mean_len = static_cast<double>(lsum) / static_cast<double>(n_lengths);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t r = 0; r < static_cast<int64_t>(row.size()); ++r) {
+    std::vector<double> xs(samples);
+    for (uint32_t i = 0; i < samples; ++i) xs[i] = static_cast<double>(sc[static_cast<size_t>(r) * samples + i]);
+    double lambda = 0.0, mu = 0.0;
+    st_calibration& o = out[row[r]];
+    if (fit_gumbel_ml(xs, &lambda, &mu)) {
+      o.lambda = lambda;
+      o.mu = mu;
+      o.k = std::exp(lambda * (mu + 0.5)) / (static_cast<double>(m[row[r]]) * mean_len);
+      o.ok = 1;
+    }
+  }
+  return ST_OK;
 }
 
 // ---------------------------------------------------------------------------

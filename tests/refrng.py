@@ -37,6 +37,10 @@ class SplitMix64:
     def below(self, n):
         return self.next_u64() % n
 
+    def next_f64(self):
+        # (next_u64() >> 11) / 2^53, exact in binary64 (src/evalue.rs:70-72)
+        return (self.next_u64() >> 11) / float(1 << 53)
+
 
 def rand_seq(rng, length, alpha):
     return [rng.range(alpha) for _ in range(length)]
