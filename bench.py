@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--serving-pairs", type=int, default=20000, help="config-4 requests for the serving measurement (0: skip)")
     ap.add_argument("--ungapped-hits", type=int, default=20_000_000, help="config-2 hits for the ungapped measurement (0: skip)")
     ap.add_argument("--serving-seconds", type=float, default=2.0, help="arrival window per swept rate")
+    ap.add_argument("--calib-profiles", type=int, default=1000,
+                    help="config-3 profiles for the per-profile calibration measurement (0: skip)")
     ap.add_argument("--gate-hits", type=int, default=20_000_000,
                     help="seed hits for the evidence / chain / gate measurement (0: skip)")
     return ap.parse_args()
@@ -433,6 +435,8 @@ def main():
             "step_ms_min_max": [round(min(step_ms), 3), round(max(step_ms), 3)],
         }
     plan.close()
+    if result is not None and args.calib_profiles > 0:
+        result["calibration"] = calibration_measure(ctx, args, w, ids, gaps)
     if result is not None and args.ungapped_hits > 0:
         result["ungapped"] = ungapped_measure(ctx, args)
     if result is not None and args.gate_hits > 0:
@@ -523,6 +527,57 @@ def ungapped_measure(ctx, args):
                                                        "window-start order, exact rescore) restated in C, queries in "
                                                        "parallel over all host threads"},
             "setup_s": round(t_gen, 1)}
+
+
+def calibration_measure(ctx, args, w, ids, gaps):
+    """Per-profile calibration (calibrate_profile, src/evalue.rs:714-748) of config-3 PSSMs as the reference's
+    profile search runs it: 2,000 background samples per profile from the search seed 0x5EED, lengths from
+    the database's length sample (every k-th record, SeedIndex::length_sample(2000), src/index.rs:2038-2042),
+    gaps 44/4.  One st_calibrate_profiles call per step (targets generated on the device, all profiles scored
+    in one batched call, ML fits on the host threads); cells = sum over profiles of m x sum of sample lengths."""
+    from oracle import oracle as O
+    from sabertooth_b200.matrix import blosum62
+    n_db = len(w.db_offsets) - 1
+    tl = np.diff(w.db_offsets.astype(np.int64))
+    lengths = tl[::max(n_db // 2000, 1)].astype(np.uint32)
+    samples, seed = 2000, 0x5EED
+    sel = ids[:min(args.calib_profiles, len(ids))]
+    m = np.array([len(r) for r in w.rows], dtype=np.int64)[:len(sel)]
+    p_back = blosum62().p_back[:20]
+    res = ctx.calibrate_profiles(sel, lengths, samples=samples, seed=seed, gaps=gaps, p_back=p_back)  # warm-up
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        res, sc = ctx.calibrate_profiles(sel, lengths, samples=samples, seed=seed, gaps=gaps, p_back=p_back,
+                                         with_scores=True)
+        ts.append(time.perf_counter() - t0)
+    t_gpu = float(np.median(ts))
+    targets = [O.calibration_target(lengths, seed, i, p_back) for i in range(samples)]
+    cells = int(m.sum()) * int(sum(len(t) for t in targets))
+    # CPU baseline: the reference's AVX2 striped kernels (u8 -> i16 -> scalar) restated in C over the same
+    # targets for a sample of profiles, all host threads, plus the ML fits
+    k = min(48, len(sel))
+    arena = O.Arena([w.rows[i] for i in range(k)], targets)
+    pq = np.repeat(np.arange(k, dtype=np.uint32), samples)
+    pt = np.tile(np.arange(samples, dtype=np.uint32), k)
+    t0 = time.perf_counter()
+    cpu_sc = O.striped_pairs(arena, pq, pt, gaps.open, gaps.extend).reshape(k, samples)
+    fits = [O.fit_gumbel_ml(cpu_sc[i].astype(np.float64)) for i in range(k)]
+    t_cpu = time.perf_counter() - t0
+    same_scores = bool(np.array_equal(cpu_sc, sc[:k]))
+    same_fits = all((f is None and r is None) or (f is not None and r is not None and
+                                                   abs(f[0] - r[0]) <= 1e-12 * abs(f[0]))
+                    for f, r in zip(fits, res[:k]))
+    return {"workload": f"config 3 PSSMs: {len(sel)} profiles x {samples} background samples (seed 0x5EED, lengths "
+                        f"from every {max(n_db // 2000, 1)}th of {n_db} database records), gaps {gaps.open}/{gaps.extend}",
+            "ms_per_call": round(t_gpu * 1e3, 2), "profiles_per_s": round(len(sel) / t_gpu, 1),
+            "gcups": round(cells / t_gpu / 1e9, 1), "cells": cells,
+            "fits_ok": int(sum(r is not None for r in res)),
+            "matches_cpu_baseline": same_scores, "fits_match_cpu_baseline": bool(same_fits),
+            "cpu_baseline": {"value": round(k / t_cpu, 2), "unit": "profiles/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"{k} profiles x {samples} samples: the reference's AVX2 "
+                                                       "striped SW (u8 -> i16 -> scalar) restated in C over all host "
+                                                       "threads, plus the ML Gumbel fits"}}
 
 
 def gate_measure(ctx, args):

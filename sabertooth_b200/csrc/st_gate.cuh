@@ -20,10 +20,11 @@
 //   scan     job offsets (CUB exclusive sum)
 //   emit     one thread per group: the top diagonals by hit count (stable on the
 //            ascending diagonal order) and their windows, written as jobs
-//   segment  one thread per job, jobs of one query share its profile staged in
-//            shared memory: kadane_segment (score, first best start and end)
+//   score    one job per lane with refill, jobs of one query share its profile
+//            staged in shared memory: kadane_score over the window
 //   chain    one thread per group: best segment, best chain, gate, region,
-//            candidate slot + flag
+//            candidate slot + flag; kadane_segment positions only for the jobs
+//            a chain test or a region reads (the reference's lazy pos_of)
 //   compact  candidates in (query, target) order (CUB select)
 //   rank     stable radix sort by (query, 2^31 - 1 - score) keeps target order
 //            inside equal scores; per-query cut to max_candidates; gather
@@ -271,18 +272,29 @@ struct GateSegParams {
   const uint32_t* n_groups;
   const uint32_t* joff;  // total jobs at joff[n_groups]
   int32_t* score;
-  int32_t* qs;
-  int32_t* qe;
   uint32_t max_m_pad;
 };
 
-// kadane_segment (src/ungapped.rs:69-88) of each job: best score, start of the
-// run that first reaches it and its end (0, 0 when the best is 0).  Target
-// residues are read as 16-byte vectors; cells outside [lo, hi) score 0, which
-// changes neither the best nor where it is first reached.
-__global__ void __launch_bounds__(256) gate_segment_kernel(const GateSegParams prm) {
+// Byte mask of a 16-byte vector: 0xFF for the bytes i with lo <= i < hi.
+__device__ __forceinline__ void gate_window_mask(int32_t lo, int32_t hi, uint32_t m[4]) {
+  const uint32_t bits = ((1u << hi) - 1u) & ~((1u << lo) - 1u);  // 0 <= lo < hi <= 16
+#pragma unroll
+  for (int j = 0; j < 4; ++j) m[j] = (((bits >> (4 * j)) & 0xFu) * 0x00204081u & 0x01010101u) * 0xFFu;
+}
+
+// kadane_score (src/ungapped.rs:53-62) of each job over its window.  A CTA
+// takes a chunk of jobs; per run of one query inside it the query's int8
+// profile is staged in shared memory and every thread keeps one job in flight,
+// one 16-byte target vector per step, taking the run's next job (shared
+// counter) as soon as its own is done, so lanes stay busy whatever the window
+// lengths.  The first and last vectors of a window have their bytes outside
+// the window replaced by the sentinel code, whose profile row is zero: zero
+// cells at the ends of a window change no Kadane maximum, so the cell loop has
+// no window test.  Profiles outside int8 read int32 rows from global memory
+// with an explicit test.
+__global__ void __launch_bounds__(256) gate_score_kernel(const GateSegParams prm) {
   extern __shared__ __align__(16) int8_t smem[];
-  __shared__ uint32_t s_run_end;
+  __shared__ uint32_t s_run_end, s_next;
   const uint32_t n = prm.joff[*prm.n_groups];
   const uint32_t stride = prm.max_m_pad;
   int8_t* base = smem + 16;
@@ -304,7 +316,10 @@ __global__ void __launch_bounds__(256) gate_segment_kernel(const GateSegParams p
         }
         e += 32;
       }
-      if (threadIdx.x == 0) s_run_end = e;
+      if (threadIdx.x == 0) {
+        s_run_end = e;
+        s_next = a + blockDim.x;
+      }
     }
     const uint32_t pstride = prm.prof.stride8[q];
     const int8_t* src = prm.prof.p8[q];
@@ -322,49 +337,116 @@ __global__ void __launch_bounds__(256) gate_segment_kernel(const GateSegParams p
     const int32_t* p32 = prm.prof.p32[q];
     const int32_t s32 = static_cast<int32_t>(prm.prof.stride32[q]);
     const int32_t last_row = static_cast<int32_t>(prm.prof.qlen[q]) - 1;
-    for (uint32_t k = a + threadIdx.x; k < b; k += blockDim.x) {
-      const GateJob jb = prm.jobs[k];
-      int32_t best = 0, cur = 0, bs = 0, be = 0, cs = 0;
-      if (jb.hi > jb.lo) {
-        const uint8_t* tp = prm.db.arena + prm.db.offset[jb.target];
-        const int32_t d = jb.diag;
-        const int32_t p0 = static_cast<int32_t>(jb.lo) + d, p1 = static_cast<int32_t>(jb.hi) + d;
-        for (int32_t pa = p0 & ~15; pa < p1; pa += 16) {
+    // per lane: job k, target base, diagonal, window [p0, p1) in target positions, next vector pa
+    uint32_t k = a + threadIdx.x;
+    const uint8_t* tp = nullptr;
+    int32_t d = 0, p0 = 0, p1 = 0, pa = 0, cur = 0, best = 0;
+    bool live = false;
+    auto take = [&](uint32_t j) {
+      k = j;
+      live = j < b;
+      if (live) {
+        const GateJob jb = prm.jobs[j];
+        tp = prm.db.arena + prm.db.offset[jb.target];
+        d = jb.diag;
+        p0 = static_cast<int32_t>(jb.lo) + d;
+        p1 = static_cast<int32_t>(jb.hi) + d;
+        pa = jb.hi > jb.lo ? (p0 & ~15) : p1;  // an empty window is done at once (p0 may be negative)
+        cur = 0;
+        best = 0;
+      }
+    };
+    take(k);
+    while (__any_sync(0xFFFFFFFFu, live)) {
+      if (live) {
+        if (pa < p1) {
           const uint4 v = *reinterpret_cast<const uint4*>(tp + pa);
-          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+          uint32_t w[4] = {v.x, v.y, v.z, v.w};
           const int32_t qa = pa - d;
-          const int8_t* rowbase = base + qa;
+          if (narrow) {
+            if (pa < p0 || pa + 16 > p1) {  // a window end inside this vector
+              uint32_t m[4];
+              gate_window_mask(max(p0 - pa, 0), min(p1 - pa, 16), m);
 #pragma unroll
-          for (int bb = 0; bb < 16; ++bb) {
-            const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
-            const int32_t p = pa + bb;
-            const bool in = (p >= p0) && (p < p1);
-            int32_t sc;
-            if (narrow) {
-              sc = rowbase[static_cast<int32_t>(r * stride) + bb];
-            } else {
-              const int32_t row = min(max(qa + bb, 0), last_row);
-              sc = __ldg(p32 + static_cast<int32_t>(r) * s32 + row);
+              for (int j = 0; j < 4; ++j) w[j] = (w[j] & m[j]) | (0x15151515u & ~m[j]);
             }
-            const int32_t s = in ? sc : 0;
-            const int32_t qp = qa + bb;
-            cs = cur <= 0 ? qp : cs;
-            cur = wadd(max(cur, 0), s);
-            if (cur > best) {
-              best = cur;
-              bs = cs;
-              be = qp;
+            const int8_t* rowbase = base + qa;
+#pragma unroll
+            for (int bb = 0; bb < 16; ++bb) {
+              const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+              cur = wadd(max(cur, 0), static_cast<int32_t>(rowbase[static_cast<int32_t>(r * stride) + bb]));
+              best = max(best, cur);
+            }
+          } else {
+#pragma unroll
+            for (int bb = 0; bb < 16; ++bb) {
+              const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+              const int32_t p = pa + bb;
+              const int32_t row = min(max(qa + bb, 0), last_row);
+              const int32_t sc = (p >= p0 && p < p1) ? __ldg(p32 + static_cast<int32_t>(r) * s32 + row) : 0;
+              cur = wadd(max(cur, 0), sc);
+              best = max(best, cur);
             }
           }
+          pa += 16;
+        }
+        if (pa >= p1) {  // done (or an empty window)
+          prm.score[k] = best;
+          take(atomicAdd(&s_next, 1u));
         }
       }
-      prm.score[k] = best;
-      prm.qs[k] = bs;
-      prm.qe[k] = be;
     }
     __syncthreads();
     a = b;
   }
+}
+
+// kadane_segment (src/ungapped.rs:69-88) of one job from the profile in global
+// memory: best score, start of the run that first reaches it and its end
+// (0, 0 when the best is 0).  Used only for the jobs whose positions decide a
+// chain or a region.  Target residues come as 16-byte vectors and the 16
+// profile loads of a vector are independent of each other; cells outside the
+// window score 0, which moves neither the best nor where it is first reached.
+__device__ int32_t gate_kadane_segment(const DeviceProfiles& prof, const DeviceDb& db, const GateJob& jb, int32_t& qs,
+                                       int32_t& qe) {
+  int32_t best = 0, cur = 0, bs = 0, be = 0, cs = 0;
+  if (jb.hi > jb.lo) {
+    const uint8_t* t = db.arena + db.offset[jb.target];
+    const bool narrow = prof.fits8[jb.query] != 0;
+    const int8_t* p8 = prof.p8[jb.query];
+    const int32_t* p32 = prof.p32[jb.query];
+    const int32_t s8 = static_cast<int32_t>(prof.stride8[jb.query]), s32 = static_cast<int32_t>(prof.stride32[jb.query]);
+    const int32_t d = jb.diag, lo = static_cast<int32_t>(jb.lo), hi = static_cast<int32_t>(jb.hi);
+    const int32_t p0 = lo + d, p1 = hi + d;
+    for (int32_t pa = p0 & ~15; pa < p1; pa += 16) {
+      const uint4 v = *reinterpret_cast<const uint4*>(t + pa);
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int bb = 0; bb < 16; ++bb) {
+        const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+        const int32_t q = pa + bb - d;
+        const bool in = q >= lo && q < hi;
+        const int32_t qc = min(max(q, lo), hi - 1);
+        const int32_t sv = narrow ? static_cast<int32_t>(p8[static_cast<int32_t>(r) * s8 + qc])
+                                  : p32[static_cast<int32_t>(r) * s32 + qc];
+        const int32_t s = in ? sv : 0;
+        if (cur <= 0) {
+          cur = s;
+          cs = q;
+        } else {
+          cur = wadd(cur, s);
+        }
+        if (cur > best) {
+          best = cur;
+          bs = cs;
+          be = q;
+        }
+      }
+    }
+  }
+  qs = bs;
+  qe = be;
+  return best;
 }
 
 __device__ __forceinline__ int32_t gate_gap_cost(int32_t open, int32_t ext, uint32_t len) {
@@ -374,10 +456,10 @@ __device__ __forceinline__ int32_t gate_gap_cost(int32_t open, int32_t ext, uint
 // Best single segment (first maximum in job order) or best chain x -> y of two
 // co-linear segments (first maximum in (x, y) order), the gate and the region
 // (src/prefilter.rs:1577-1657, region :1269-1278).
-__global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf g, const uint32_t* joff,
-                                                         const GateJob* jobs, const int32_t* score,
-                                                         const int32_t* qs, const int32_t* qe, GateCandidate* cand,
-                                                         uint8_t* flag, GateStats* st) {
+__global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf g, DeviceDb db, DeviceProfiles prof,
+                                                         const uint32_t* joff, const GateJob* jobs,
+                                                         const int32_t* score, GateCandidate* cand, uint8_t* flag,
+                                                         GateStats* st) {
   const uint32_t ng = *G.n_groups;
   unsigned long long n_chained = 0;
   for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ng; gi += gridDim.x * blockDim.x) {
@@ -393,13 +475,22 @@ __global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf 
           bi = k;
         }
       }
+      // segment positions, computed where a chain or a region needs them (as the reference's pos_of)
+      int32_t pqs[kGateMaxDiags], pqe[kGateMaxDiags];
+      uint32_t have = 0;
+      auto pos_of = [&](uint32_t x) {
+        if (!(have & (1u << x))) {
+          gate_kadane_segment(prof, db, jobs[j0 + x], pqs[x], pqe[x]);
+          have |= 1u << x;
+        }
+      };
       int32_t chain = INT32_MIN;
       uint32_t cx = 0, cy = 0;
       if (nsg > 1) {
         for (uint32_t x = 0; x < nsg; ++x) {
           const int32_t sx = score[j0 + x];
           if (sx <= 0) continue;
-          const int32_t dx = jobs[j0 + x].diag, qex = qe[j0 + x];
+          const int32_t dx = jobs[j0 + x].diag;
           for (uint32_t y = 0; y < nsg; ++y) {
             if (x == y) continue;
             const int32_t sy = score[j0 + y], dy = jobs[j0 + y].diag;
@@ -407,7 +498,9 @@ __global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf 
             const uint32_t len = static_cast<uint32_t>(dy > dx ? dy - dx : dx - dy);
             const int32_t c = wsub(wadd(sx, sy), gate_gap_cost(g.open, g.ext, len));
             if (c <= best || c <= chain) continue;
-            const int32_t qsy = qs[j0 + y];
+            pos_of(x);
+            pos_of(y);
+            const int32_t qex = pqe[x], qsy = pqs[y];
             if (qex < qsy && static_cast<int64_t>(qex) + dx < static_cast<int64_t>(qsy) + dy) {
               chain = c;
               cx = x;
@@ -433,9 +526,11 @@ __global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf 
         gate_group_range(G, gi, ng, s, e);
         uint32_t rlo = 0, rhi = 0xFFFFFFFFu;
         if (g.regions) {
+          pos_of(u0);
+          pos_of(u1);
           const int64_t d0 = jobs[j0 + u0].diag, d1 = jobs[j0 + u1].diag;
-          const int64_t a0 = i64max(qs[j0 + u0] + d0, 0), b0 = i64max(qe[j0 + u0] + d0, 0);
-          const int64_t a1 = i64max(qs[j0 + u1] + d1, 0), b1 = i64max(qe[j0 + u1] + d1, 0);
+          const int64_t a0 = i64max(pqs[u0] + d0, 0), b0 = i64max(pqe[u0] + d0, 0);
+          const int64_t a1 = i64max(pqs[u1] + d1, 0), b1 = i64max(pqe[u1] + d1, 0);
           rlo = static_cast<uint32_t>(i64min(a0, a1));
           rhi = static_cast<uint32_t>(i64max(b0, b1));
         }

@@ -490,9 +490,9 @@ static int set_smem_limits(int device) {
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
   cudaFuncAttributes fa_g;
-  ST_CUDA(cudaFuncGetAttributes(&fa_g, reinterpret_cast<const void*>(gate_segment_kernel)));
+  ST_CUDA(cudaFuncGetAttributes(&fa_g, reinterpret_cast<const void*>(gate_score_kernel)));
   g_gate_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(fa_g.sharedSizeBytes));
-  ST_CUDA(cudaFuncSetAttribute(gate_segment_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_gate_smem));
+  ST_CUDA(cudaFuncSetAttribute(gate_score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_gate_smem));
   return ST_OK;
 }
 
@@ -2727,6 +2727,42 @@ static int run_pairs_device(st_ctx* c, const st_hit* d_hits, uint64_t n, const i
   return ST_OK;
 }
 
+// Host -> device copy on stream s.  Pinned memory is copied directly; pageable
+// memory goes through the two pinned staging blocks in turn (filled by all
+// host threads, each uploaded on the copy stream while the next one fills),
+// which runs at host memcpy speed instead of the driver's pageable path.
+static int upload_host(st_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return ST_OK;
+  if (host_pinned(src)) {
+    ST_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    return ST_OK;
+  }
+  constexpr size_t kChunk = 32ull << 20, kPiece = 1ull << 20;
+  if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+  ST_CUDA(cudaEventRecord(c->copy_ev, s));  // the destination's earlier users come first
+  ST_CUDA(cudaStreamWaitEvent(c->copy, c->copy_ev, 0));
+  int slot = 0;
+  for (size_t o = 0; o < bytes; o += kChunk) {
+    const size_t len = std::min(kChunk, bytes - o);
+    Pinned& st = c->prof_stage[slot];
+    if (!c->prof_stage_ev[slot]) ST_CUDA(cudaEventCreateWithFlags(&c->prof_stage_ev[slot], cudaEventDisableTiming));
+    if (c->prof_stage_used[slot]) ST_CUDA(cudaEventSynchronize(c->prof_stage_ev[slot]));
+    ST_TRY(st.reserve(kChunk));
+    char* h = st.as<char>();
+    const char* from = static_cast<const char*>(src) + o;
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < static_cast<int64_t>((len + kPiece - 1) / kPiece); ++k)
+      memcpy(h + k * kPiece, from + k * kPiece, std::min(kPiece, len - k * kPiece));
+    ST_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + o, h, len, cudaMemcpyHostToDevice, c->copy));
+    ST_CUDA(cudaEventRecord(c->prof_stage_ev[slot], c->copy));
+    c->prof_stage_used[slot] = true;
+    slot ^= 1;
+  }
+  ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
+  ST_CUDA(cudaStreamWaitEvent(s, c->copy_ev, 0));
+  return ST_OK;
+}
+
 static int check_hits_device(st_ctx* c) {
   if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
   return sync_profiles(c);
@@ -2775,7 +2811,7 @@ extern "C" int st_ungapped_hits(st_ctx* c, const st_hit* hits, uint64_t n, int32
     ~Back() { pool_put_after(c, std::move(*m), c->stream); }
   } back{c, &buf};
   char* d = buf.as<char>();
-  ST_CUDA(cudaMemcpyAsync(d, hits, n * sizeof(st_hit), cudaMemcpyHostToDevice, c->stream));
+  ST_TRY(upload_host(c, d, hits, n * sizeof(st_hit), c->stream));
   int32_t* d_out = reinterpret_cast<int32_t*>(d + hb);
   ST_TRY(launch_ungapped(c, true, d, n, d_out));
   if (want_pairs) {
@@ -2850,8 +2886,7 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   };
   const size_t o_k0 = take(8ull * n), o_k1 = take(8ull * n), o_v0 = take(4ull * n), o_v1 = take(4ull * n);
   const size_t o_start = take(4ull * n), o_ng = take(4), o_ns = take(4ull * (n + 1)), o_joff = take(4ull * (n + 1));
-  const size_t o_jobs = take(sizeof(GateJob) * n), o_sc = take(4ull * n), o_qs = take(4ull * n),
-               o_qe = take(4ull * n);
+  const size_t o_jobs = take(sizeof(GateJob) * n), o_sc = take(4ull * n);
   const size_t o_cand = take(sizeof(GateCandidate) * n), o_flag = take(n), o_sel = take(4ull * n), o_nc = take(4);
   const size_t o_stats = take(sizeof(GateStats)), o_nout = take(8);
   const size_t o_qf = take(4 * P), o_qend = take(4 * P), o_kept = take(4 * P), o_koff = take(4 * P);
@@ -2896,8 +2931,6 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   uint32_t* joff = static_cast<uint32_t*>(at(o_joff));
   GateJob* jobs = static_cast<GateJob*>(at(o_jobs));
   int32_t* sc = static_cast<int32_t*>(at(o_sc));
-  int32_t* qs = static_cast<int32_t*>(at(o_qs));
-  int32_t* qe = static_cast<int32_t*>(at(o_qe));
   GateCandidate* cand = static_cast<GateCandidate*>(at(o_cand));
   uint8_t* flag = static_cast<uint8_t*>(at(o_flag));
   uint32_t* sel = static_cast<uint32_t*>(at(o_sel));
@@ -2910,9 +2943,10 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   uint32_t* koff = static_cast<uint32_t*>(at(o_koff));
   void* tmp = at(o_tmp);
   cudaStream_t s = c->stream;
-  const uint32_t cap_grid = static_cast<uint32_t>(c->sms) * 8;
+  // enough blocks for every SM to hold its full 2048 threads several times over
   auto grid_for = [&](uint64_t items, uint32_t block) {
-    return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>((items + block - 1) / block, cap_grid)));
+    const uint64_t cap = static_cast<uint64_t>(c->sms) * (2048 / block) * 4;
+    return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>((items + block - 1) / block, cap)));
   };
   ST_CUDA(cudaMemsetAsync(st, 0, sizeof(GateStats), s));
   // keys, sort, groups
@@ -2939,14 +2973,14 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
     gate_emit_kernel<4><<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv.qlen, ns, joff, jobs);
   else
     gate_emit_kernel<kGateMaxDiags><<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv.qlen, ns, joff, jobs);
-  // segments
-  GateSegParams sp{db, pv, jobs, ng, joff, sc, qs, qe, ung_stride(c)};
+  // window scores
+  GateSegParams sp{db, pv, jobs, ng, joff, sc, ung_stride(c)};
   const size_t smem = 16 + static_cast<size_t>(kProfRows) * sp.max_m_pad + 16;
-  gate_segment_kernel<<<static_cast<uint32_t>((static_cast<uint64_t>(n) + kGateChunk - 1) / kGateChunk), 256, smem,
-                        s>>>(sp);
+  gate_score_kernel<<<static_cast<uint32_t>((static_cast<uint64_t>(n) + kGateChunk - 1) / kGateChunk), 256, smem, s>>>(
+      sp);
   // chain, gate, compaction
   ST_CUDA(cudaMemsetAsync(flag, 0, n, s));
-  gate_chain_kernel<<<grid_for(n, 128), 128, 0, s>>>(G, g, joff, jobs, sc, qs, qe, cand, flag, st);
+  gate_chain_kernel<<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv, joff, jobs, sc, cand, flag, st);
   {
     cub::CountingInputIterator<uint32_t> it(0);
     t = t_max;
@@ -3041,7 +3075,7 @@ extern "C" int st_prefilter_gate(st_ctx* c, const st_seed_hit* hits, uint64_t n,
       ~Back() { pool_put_after(c, std::move(*m), c->stream); }
     } back{c, &buf};
     char* d = buf.as<char>();
-    ST_CUDA(cudaMemcpyAsync(d, hits, n * sizeof(st_seed_hit), cudaMemcpyHostToDevice, c->stream));
+    ST_TRY(upload_host(c, d, hits, n * sizeof(st_seed_hit), c->stream));
     GateCandidate* d_out = reinterpret_cast<GateCandidate*>(d + hb);
     ST_TRY(gate_pipeline(c, reinterpret_cast<const GateSeedHit*>(d), static_cast<uint32_t>(n), g, qbits, d_out,
                          n_out, &st));
