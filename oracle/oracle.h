@@ -137,6 +137,50 @@ int or_calibrate_profile(const int32_t* rows, uint32_t m, const uint32_t* length
                          uint32_t samples, uint64_t seed, const double* p_back20, int32_t open, int32_t ext,
                          int32_t* scores, double* lambda, double* k, double* mu, int nthreads);
 
+/* ---- seed hits (seeds.c) ---------------------------------------------------------
+ * The seed stage of prefilter_query (src/prefilter.rs:816-995) over a CPU seed
+ * index of the targets (window_ok, src/index.rs:1059-1074). */
+typedef struct {
+  uint64_t code;
+  uint32_t tid;
+  uint32_t tpos;
+} or_posting;
+
+typedef struct {
+  int32_t kmer_score;
+  uint32_t max_kmers_per_pos;
+  uint32_t exact_seeds;
+  uint32_t max_seed_occ; /* 0 = never skip */
+} or_seed_params;
+
+typedef struct {
+  uint64_t windows;
+  uint64_t windows_skipped;
+  uint64_t kmers_generated;
+  uint64_t windows_at_cap;
+  uint64_t exact_seeds_added;
+  uint64_t seeds;
+  uint64_t postings_visited;
+  uint64_t seeds_over_occ_cap;
+  uint64_t postings_skipped_occ;
+} or_seed_stats;
+
+/* top_kmers_heap (src/prefilter.rs:624-690): rows = w x 21 score rows of the
+ * window's care positions; codes/scores in canonical order (room for cap);
+ * returns 1 when more than cap k-mers reach thr. */
+int or_top_kmers(const int32_t* rows, int w, int32_t thr, uint32_t cap, uint64_t* codes, int32_t* scores,
+                 uint32_t* n_out);
+uint64_t or_index_count(const uint8_t* tgt_arena, const uint64_t* tgt_off, uint32_t n_targets, const uint32_t* offs,
+                        uint32_t w, uint32_t span);
+/* out: room for or_index_count entries; sorted by (code, target, position) */
+void or_index_build(const uint8_t* tgt_arena, const uint64_t* tgt_off, uint32_t n_targets, const uint32_t* offs,
+                    uint32_t w, uint32_t span, or_posting* out);
+/* one query's hits (target, diag, qpos), at most cap_hits written; returns the total.
+ * residues may be NULL (profile queries: no skipped windows, no exact seeds). */
+uint64_t or_seed_hits(const int32_t* rows, const uint8_t* residues, uint32_t m, const uint32_t* offs, uint32_t w,
+                      uint32_t span, const or_seed_params* p, const or_posting* idx, uint64_t n_post, uint32_t query,
+                      uint32_t* ht, int32_t* hd, uint32_t* hqpos, uint64_t cap_hits, or_seed_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

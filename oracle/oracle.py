@@ -50,6 +50,13 @@ def _load():
     lib.or_fit_gumbel_ml.argtypes = [P, u64, P, P]
     lib.or_calibrate_profile.restype = C.c_int
     lib.or_calibrate_profile.argtypes = [P, u32, P, u32, u32, u64, P, i32, i32, P, P, P, P, C.c_int]
+    lib.or_top_kmers.restype = C.c_int
+    lib.or_top_kmers.argtypes = [P, C.c_int, i32, u32, P, P, P]
+    lib.or_index_count.restype = u64
+    lib.or_index_count.argtypes = [P, P, u32, P, u32, u32]
+    lib.or_index_build.argtypes = [P, P, u32, P, u32, u32, P]
+    lib.or_seed_hits.restype = u64
+    lib.or_seed_hits.argtypes = [P, P, u32, P, u32, u32, P, P, u64, u32, P, P, P, u64, P]
     return lib
 
 
@@ -257,3 +264,58 @@ def calibrate_profile(rows, lengths, samples, seed, p_back20, open_, ext, thread
     ok = lib.or_calibrate_profile(_p(r), r.shape[0], _p(lengths), len(lengths), samples, seed, _p(p), open_, ext,
                                   _p(scores), C.byref(lam), C.byref(k), C.byref(mu), threads or os.cpu_count() or 1)
     return ((lam.value, k.value, mu.value) if ok else None), scores[:samples].copy()
+
+
+# ---- seed hits (seeds.c) -----------------------------------------------------------
+SEED_STATS_FIELDS = ("windows", "windows_skipped", "kmers_generated", "windows_at_cap", "exact_seeds_added", "seeds",
+                     "postings_visited", "seeds_over_occ_cap", "postings_skipped_occ")
+_POSTING_DTYPE = np.dtype([("code", "<u8"), ("tid", "<u4"), ("tpos", "<u4")])
+_SEED_PARAM_DTYPE = np.dtype([("kmer_score", "<i4"), ("max_kmers_per_pos", "<u4"), ("exact_seeds", "<u4"),
+                              ("max_seed_occ", "<u4")])
+
+
+def pattern_offsets(mask):
+    """SeedPattern::from_mask (src/prefilter.rs:101-124): care offsets and span."""
+    offs = [i for i, c in enumerate(mask) if c == "1"]
+    return np.array(offs, dtype=np.uint32), len(mask)
+
+
+def top_kmers(rows_w, thr, cap):
+    """(codes, scores, capped): the first cap k-mers >= thr in canonical order."""
+    r = _rows(rows_w)
+    codes = np.zeros(max(cap, 1), dtype=np.uint64)
+    scores = np.zeros(max(cap, 1), dtype=np.int32)
+    n = C.c_uint32()
+    capped = lib.or_top_kmers(_p(r), r.shape[0], thr, cap, _p(codes), _p(scores), C.byref(n))
+    return codes[:n.value].copy(), scores[:n.value].copy(), bool(capped)
+
+
+class SeedIndex:
+    """The CPU seed index of a target list (window_ok, src/index.rs:1059-1074)."""
+
+    def __init__(self, arena: Arena, mask):
+        self.offs, self.span = pattern_offsets(mask)
+        self.w = len(self.offs)
+        nt = len(arena.tgt_off) - 1
+        n = lib.or_index_count(_p(arena.tgt), _p(arena.tgt_off), nt, _p(self.offs), self.w, self.span)
+        self.post = np.zeros(max(int(n), 1), dtype=_POSTING_DTYPE)
+        lib.or_index_build(_p(arena.tgt), _p(arena.tgt_off), nt, _p(self.offs), self.w, self.span, _p(self.post))
+        self.n = int(n)
+
+
+def seed_hits(rows, residues, index: SeedIndex, kmer_score, max_kmers_per_pos=512, exact_seeds=True,
+              max_seed_occ=0):
+    """One query's seed hits: (target, diag, qpos) arrays and the seed counters."""
+    r = _rows(rows)
+    res = None if residues is None else np.ascontiguousarray(residues, dtype=np.uint8)
+    prm = np.zeros(1, dtype=_SEED_PARAM_DTYPE)
+    prm["kmer_score"], prm["max_kmers_per_pos"] = kmer_score, max_kmers_per_pos
+    prm["exact_seeds"], prm["max_seed_occ"] = int(bool(exact_seeds)), max_seed_occ
+    st = np.zeros(len(SEED_STATS_FIELDS), dtype=np.uint64)
+    args = (_p(r), _p(res), r.shape[0], _p(index.offs), index.w, index.span, _p(prm), _p(index.post), index.n, 0)
+    n = int(lib.or_seed_hits(*args, None, None, None, 0, _p(st)))
+    ht = np.zeros(max(n, 1), dtype=np.uint32)
+    hd = np.zeros(max(n, 1), dtype=np.int32)
+    hq = np.zeros(max(n, 1), dtype=np.uint32)
+    lib.or_seed_hits(*args, _p(ht), _p(hd), _p(hq), n, _p(st))
+    return ht[:n], hd[:n], hq[:n], {f: int(v) for f, v in zip(SEED_STATS_FIELDS, st)}

@@ -22,9 +22,11 @@
 //            ascending diagonal order) and their windows, written as jobs
 //   score    one job per lane with refill, jobs of one query share its profile
 //            staged in shared memory: kadane_score over the window
-//   chain    one thread per group: best segment, best chain, gate, region,
-//            candidate slot + flag; kadane_segment positions only for the jobs
-//            a chain test or a region reads (the reference's lazy pos_of)
+//   screen   groups that may pass (several diagonals, or one at the gate) to a
+//            work list
+//   chain    one thread per listed group: best segment, best chain, gate,
+//            region, candidate slot + flag; kadane_segment positions only for
+//            the jobs a chain test or a region reads (the reference's pos_of)
 //   compact  candidates in (query, target) order (CUB select)
 //   rank     stable radix sort by (query, 2^31 - 1 - score) keeps target order
 //            inside equal scores; per-query cut to max_candidates; gather
@@ -453,92 +455,103 @@ __device__ __forceinline__ int32_t gate_gap_cost(int32_t open, int32_t ext, uint
   return len == 0 ? 0 : wadd(open, static_cast<int32_t>((len - 1u) * static_cast<uint32_t>(ext)));
 }
 
-// Best single segment (first maximum in job order) or best chain x -> y of two
-// co-linear segments (first maximum in (x, y) order), the gate and the region
-// (src/prefilter.rs:1577-1657, region :1269-1278).
-__global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf g, DeviceDb db, DeviceProfiles prof,
-                                                         const uint32_t* joff, const GateJob* jobs,
-                                                         const int32_t* score, GateCandidate* cand, uint8_t* flag,
-                                                         GateStats* st) {
+// Groups that may pass the gate: every group with more than one diagonal or
+// with its one diagonal at or above the gate goes to a work list (the order of
+// the list does not matter: each group writes its own slot).  Groups left out
+// keep the zero flag written before.
+__global__ void __launch_bounds__(256) gate_screen_kernel(GateGroups G, GateConf g, const uint32_t* joff,
+                                                          const int32_t* score, uint32_t* work, uint32_t* n_work) {
   const uint32_t ng = *G.n_groups;
-  unsigned long long n_chained = 0;
   for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ng; gi += gridDim.x * blockDim.x) {
     const uint32_t j0 = joff[gi], nsg = joff[gi + 1] - j0;
-    uint8_t keep = 0;
-    if (nsg > 0 && !(nsg == 1 && score[j0] < g.min_score)) {
-      int32_t best = 0;
-      uint32_t bi = 0;
-      for (uint32_t k = 0; k < nsg; ++k) {
-        const int32_t sk = score[j0 + k];
-        if (sk > best) {
-          best = sk;
-          bi = k;
-        }
+    if (nsg > 0 && !(nsg == 1 && score[j0] < g.min_score)) work[atomicAdd(n_work, 1u)] = gi;
+  }
+}
+
+// Best single segment (first maximum in job order) or best chain x -> y of two
+// co-linear segments (first maximum in (x, y) order), the gate and the region
+// (src/prefilter.rs:1577-1657, region :1269-1278), one thread per listed group.
+__global__ void __launch_bounds__(128) gate_chain_kernel(GateGroups G, GateConf g, DeviceDb db, DeviceProfiles prof,
+                                                         const uint32_t* joff, const GateJob* jobs,
+                                                         const int32_t* score, const uint32_t* work,
+                                                         const uint32_t* n_work, GateCandidate* cand, uint8_t* flag,
+                                                         GateStats* st) {
+  const uint32_t ng = *G.n_groups;
+  const uint32_t nw = *n_work;
+  unsigned long long n_chained = 0;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
+    const uint32_t gi = work[w];
+    const uint32_t j0 = joff[gi], nsg = joff[gi + 1] - j0;
+    int32_t best = 0;
+    uint32_t bi = 0;
+    for (uint32_t k = 0; k < nsg; ++k) {
+      const int32_t sk = score[j0 + k];
+      if (sk > best) {
+        best = sk;
+        bi = k;
       }
-      // segment positions, computed where a chain or a region needs them (as the reference's pos_of)
-      int32_t pqs[kGateMaxDiags], pqe[kGateMaxDiags];
-      uint32_t have = 0;
-      auto pos_of = [&](uint32_t x) {
-        if (!(have & (1u << x))) {
-          gate_kadane_segment(prof, db, jobs[j0 + x], pqs[x], pqe[x]);
-          have |= 1u << x;
-        }
-      };
-      int32_t chain = INT32_MIN;
-      uint32_t cx = 0, cy = 0;
-      if (nsg > 1) {
-        for (uint32_t x = 0; x < nsg; ++x) {
-          const int32_t sx = score[j0 + x];
-          if (sx <= 0) continue;
-          const int32_t dx = jobs[j0 + x].diag;
-          for (uint32_t y = 0; y < nsg; ++y) {
-            if (x == y) continue;
-            const int32_t sy = score[j0 + y], dy = jobs[j0 + y].diag;
-            if (sy <= 0 || dx == dy) continue;
-            const uint32_t len = static_cast<uint32_t>(dy > dx ? dy - dx : dx - dy);
-            const int32_t c = wsub(wadd(sx, sy), gate_gap_cost(g.open, g.ext, len));
-            if (c <= best || c <= chain) continue;
-            pos_of(x);
-            pos_of(y);
-            const int32_t qex = pqe[x], qsy = pqs[y];
-            if (qex < qsy && static_cast<int64_t>(qex) + dx < static_cast<int64_t>(qsy) + dy) {
-              chain = c;
-              cx = x;
-              cy = y;
-            }
+    }
+    // segment positions, computed where a chain or a region needs them (as the reference's pos_of)
+    int32_t pqs[kGateMaxDiags], pqe[kGateMaxDiags];
+    uint32_t have = 0;
+    auto pos_of = [&](uint32_t x) {
+      if (!(have & (1u << x))) {
+        gate_kadane_segment(prof, db, jobs[j0 + x], pqs[x], pqe[x]);
+        have |= 1u << x;
+      }
+    };
+    int32_t chain = INT32_MIN;
+    uint32_t cx = 0, cy = 0;
+    if (nsg > 1) {
+      for (uint32_t x = 0; x < nsg; ++x) {
+        const int32_t sx = score[j0 + x];
+        if (sx <= 0) continue;
+        const int32_t dx = jobs[j0 + x].diag;
+        for (uint32_t y = 0; y < nsg; ++y) {
+          if (x == y) continue;
+          const int32_t sy = score[j0 + y], dy = jobs[j0 + y].diag;
+          if (sy <= 0 || dx == dy) continue;
+          const uint32_t len = static_cast<uint32_t>(dy > dx ? dy - dx : dx - dy);
+          const int32_t c = wsub(wadd(sx, sy), gate_gap_cost(g.open, g.ext, len));
+          if (c <= best || c <= chain) continue;
+          pos_of(x);
+          pos_of(y);
+          const int32_t qex = pqe[x], qsy = pqs[y];
+          if (qex < qsy && static_cast<int64_t>(qex) + dx < static_cast<int64_t>(qsy) + dy) {
+            chain = c;
+            cx = x;
+            cy = y;
           }
         }
       }
-      int32_t total;
-      uint32_t u0, u1;
-      if (chain > best) {
-        ++n_chained;
-        total = chain;
-        u0 = cx;
-        u1 = cy;
-      } else {
-        total = best;
-        u0 = u1 = bi;
-      }
-      if (total >= g.min_score) {
-        keep = 1;
-        uint32_t s, e;
-        gate_group_range(G, gi, ng, s, e);
-        uint32_t rlo = 0, rhi = 0xFFFFFFFFu;
-        if (g.regions) {
-          pos_of(u0);
-          pos_of(u1);
-          const int64_t d0 = jobs[j0 + u0].diag, d1 = jobs[j0 + u1].diag;
-          const int64_t a0 = i64max(pqs[u0] + d0, 0), b0 = i64max(pqe[u0] + d0, 0);
-          const int64_t a1 = i64max(pqs[u1] + d1, 0), b1 = i64max(pqe[u1] + d1, 0);
-          rlo = static_cast<uint32_t>(i64min(a0, a1));
-          rhi = static_cast<uint32_t>(i64max(b0, b1));
-        }
-        const GateJob jb = jobs[j0];
-        cand[gi] = GateCandidate{jb.query, jb.target, e - s, total, static_cast<int64_t>(jobs[j0 + bi].diag), rlo, rhi};
-      }
     }
-    flag[gi] = keep;
+    int32_t total;
+    uint32_t u0, u1;
+    if (chain > best) {
+      ++n_chained;
+      total = chain;
+      u0 = cx;
+      u1 = cy;
+    } else {
+      total = best;
+      u0 = u1 = bi;
+    }
+    if (total < g.min_score) continue;
+    uint32_t s, e;
+    gate_group_range(G, gi, ng, s, e);
+    uint32_t rlo = 0, rhi = 0xFFFFFFFFu;
+    if (g.regions) {
+      pos_of(u0);
+      pos_of(u1);
+      const int64_t d0 = jobs[j0 + u0].diag, d1 = jobs[j0 + u1].diag;
+      const int64_t a0 = i64max(pqs[u0] + d0, 0), b0 = i64max(pqe[u0] + d0, 0);
+      const int64_t a1 = i64max(pqs[u1] + d1, 0), b1 = i64max(pqe[u1] + d1, 0);
+      rlo = static_cast<uint32_t>(i64min(a0, a1));
+      rhi = static_cast<uint32_t>(i64max(b0, b1));
+    }
+    const GateJob jb = jobs[j0];
+    cand[gi] = GateCandidate{jb.query, jb.target, e - s, total, static_cast<int64_t>(jobs[j0 + bi].diag), rlo, rhi};
+    flag[gi] = 1;
   }
   gate_flush(&st->chains_used, n_chained);
 }

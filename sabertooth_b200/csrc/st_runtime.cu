@@ -2888,6 +2888,7 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   const size_t o_start = take(4ull * n), o_ng = take(4), o_ns = take(4ull * (n + 1)), o_joff = take(4ull * (n + 1));
   const size_t o_jobs = take(sizeof(GateJob) * n), o_sc = take(4ull * n);
   const size_t o_cand = take(sizeof(GateCandidate) * n), o_flag = take(n), o_sel = take(4ull * n), o_nc = take(4);
+  const size_t o_work = take(4ull * n), o_nw = take(4);
   const size_t o_stats = take(sizeof(GateStats)), o_nout = take(8);
   const size_t o_qf = take(4 * P), o_qend = take(4 * P), o_kept = take(4 * P), o_koff = take(4 * P);
   // CUB scratch, sized for the largest input of each call
@@ -2935,6 +2936,8 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   uint8_t* flag = static_cast<uint8_t*>(at(o_flag));
   uint32_t* sel = static_cast<uint32_t*>(at(o_sel));
   uint32_t* nc = static_cast<uint32_t*>(at(o_nc));
+  uint32_t* work = static_cast<uint32_t*>(at(o_work));
+  uint32_t* n_work = static_cast<uint32_t*>(at(o_nw));
   GateStats* st = static_cast<GateStats*>(at(o_stats));
   unsigned long long* nout = static_cast<unsigned long long*>(at(o_nout));
   uint32_t* qf = static_cast<uint32_t*>(at(o_qf));
@@ -2980,13 +2983,15 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
       sp);
   // chain, gate, compaction
   ST_CUDA(cudaMemsetAsync(flag, 0, n, s));
-  gate_chain_kernel<<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv, joff, jobs, sc, cand, flag, st);
+  ST_CUDA(cudaMemsetAsync(n_work, 0, 4, s));
+  gate_screen_kernel<<<grid_for(n, 256), 256, 0, s>>>(G, g, joff, sc, work, n_work);
+  gate_chain_kernel<<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv, joff, jobs, sc, work, n_work, cand, flag, st);
   {
     cub::CountingInputIterator<uint32_t> it(0);
     t = t_max;
     ST_CUDA(cub::DeviceSelect::Flagged(tmp, t, it, flag, sel, nc, n, s));
   }
-  c->launches += 7;
+  c->launches += 8;
   ST_CUDA(cudaGetLastError());
   ST_TRY(c->pin.reserve(64));
   uint32_t* h_nc = c->pin.as<uint32_t>();
