@@ -271,6 +271,61 @@ int st_prefilter_gate(st_ctx* ctx, const st_seed_hit* hits, uint64_t n, const st
 int st_prefilter_gate_device(st_ctx* ctx, const st_seed_hit* d_hits, uint64_t n, const st_prefilter_params* params,
                              st_candidate* d_out, uint64_t* n_out, st_prefilter_stats* stats);
 
+/* ---- seed hits ---------------------------------------------------------------
+ * The seed stage of prefilter_query (src/prefilter.rs:816-995) on the device.
+ * st_seed_index_build indexes the uploaded database for a seed pattern given
+ * as a 0/1 mask that starts and ends with '1' (SeedPattern::from_mask,
+ * src/prefilter.rs:101-124; weight 2..7 here): every window whose care
+ * residues are all standard (codes < 20), keyed by those residues in base 20
+ * (the seeding pass of src/index.rs:1059-1074).  An upload of a new database
+ * drops the index. */
+int st_seed_index_build(st_ctx* ctx, const char* seed_mask);
+
+/* The similar-k-mer fields of PrefilterParams (src/prefilter.rs:262-303). */
+typedef struct {
+  int32_t kmer_score;          /* threshold of a similar k-mer's summed score */
+  uint32_t max_kmers_per_pos;  /* >= 1: the first this many k-mers of the canonical order per window */
+  uint32_t exact_seeds;        /* add the query's own k-mer (sequence queries) */
+  uint32_t max_seed_occ;       /* skip k-mers with more postings (0 = never) */
+} st_seed_params;
+
+/* The seed counters of PrefilterStats, summed over the call's queries. */
+typedef struct {
+  uint64_t windows;
+  uint64_t windows_skipped;
+  uint64_t kmers_generated;
+  uint64_t windows_at_cap;
+  uint64_t exact_seeds_added;
+  uint64_t seeds;
+  uint64_t postings_visited;
+  uint64_t seeds_over_occ_cap;
+  uint64_t postings_skipped_occ;
+} st_seed_stats;
+
+/* Seed hits of n_queries queries (profile ids; seed rows = the profiles' rows).
+ * residues (optional) holds each sequence query's residue codes,
+ * residues[residue_offsets[i] .. residue_offsets[i+1]) with one code per
+ * profile row: windows with a care residue >= 20 are skipped and, with
+ * exact_seeds, the query's own k-mer is added; NULL for profile (PSSM) queries.
+ * Per window (every start in [0, m - span]): the first max_kmers_per_pos
+ * k-mers scoring >= kmer_score in the canonical order (score descending, then
+ * the rank vector ascending: top_kmers, src/prefilter.rs:457-568), then one hit
+ * per posting.  *n_out receives the hit count; the first min(cap, count) hits
+ * are written, in no particular order.  Windows whose rows span more than 1,024
+ * score values above the threshold are rejected (ST_EINVAL). */
+int st_seed_hits(st_ctx* ctx, const uint32_t* profiles, uint32_t n_queries, const uint8_t* residues,
+                 const uint64_t* residue_offsets, const st_seed_params* params, st_seed_hit* out, uint64_t cap,
+                 uint64_t* n_out, st_seed_stats* stats);
+
+/* The whole prefilter of prefilter_query for a batch of queries on the device:
+ * seed hits (as st_seed_hits) -> evidence, chains and gate -> ranked
+ * candidates (as st_prefilter_gate; params->span is taken from the index's
+ * pattern).  Host buffers; stats and seed_stats may be NULL. */
+int st_prefilter_queries(st_ctx* ctx, const uint32_t* profiles, uint32_t n_queries, const uint8_t* residues,
+                         const uint64_t* residue_offsets, const st_seed_params* seed_params,
+                         const st_prefilter_params* params, st_candidate* out, uint64_t cap, uint64_t* n_out,
+                         st_prefilter_stats* stats, st_seed_stats* seed_stats);
+
 /* ---- per-profile calibration ----------------------------------------------
  * calibrate_profile (src/evalue.rs:714-748) for many profiles at once: sample i
  * (0 <= i < samples) is a background target drawn from the SplitMix64 stream

@@ -16,7 +16,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libsabertooth_b200.so")
 
 SOURCES = ["st_runtime.cu", "st_noalloc.cu", "st_host.cpp", "st_server.cpp"]
-HEADERS = ["st_common.cuh", "st_sw16.cuh", "st_sw32.cuh", "st_ungapped.cuh", "st_tuning.h", "st_dplan.cuh", "st_gate.cuh", "st_calib.cuh"]
+HEADERS = ["st_common.cuh", "st_sw16.cuh", "st_sw32.cuh", "st_ungapped.cuh", "st_tuning.h", "st_dplan.cuh", "st_gate.cuh", "st_calib.cuh", "st_seed.cuh"]
 INCLUDES = [os.path.join(ROOT, "include", h) for h in ("sabertooth_b200.h", "sabertooth_b200_host.h")]
 
 

@@ -58,6 +58,19 @@ class CalibrationC(C.Structure):
                 ("ok", C.c_int32)]
 
 
+class SeedParamsC(C.Structure):
+    _fields_ = [("kmer_score", C.c_int32), ("max_kmers_per_pos", C.c_uint32), ("exact_seeds", C.c_uint32),
+                ("max_seed_occ", C.c_uint32)]
+
+
+SEED_STATS_FIELDS = ("windows", "windows_skipped", "kmers_generated", "windows_at_cap", "exact_seeds_added", "seeds",
+                     "postings_visited", "seeds_over_occ_cap", "postings_skipped_occ")
+
+
+class SeedStatsC(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in SEED_STATS_FIELDS]
+
+
 class PrefilterStatsC(C.Structure):
     _fields_ = [(f, C.c_uint64) for f in PREFILTER_STATS_FIELDS]
 
@@ -103,6 +116,9 @@ SIGNATURES = {
     "st_prefilter_gate": (C.c_int, [_P, _P, _u64, _P, _P, _u64, _P, _P]),
     "st_prefilter_gate_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P]),
     "st_calibrate_profiles": (C.c_int, [_P, _P, _u32, _P, _u32, _u32, _u64, _P, _i32, _i32, _P, _P]),
+    "st_seed_index_build": (C.c_int, [_P, C.c_char_p]),
+    "st_seed_hits": (C.c_int, [_P, _P, _u32, _P, _P, _P, _P, _u64, _P, _P]),
+    "st_prefilter_queries": (C.c_int, [_P, _P, _u32, _P, _P, _P, _P, _P, _u64, _P, _P, _P]),
     "st_tune_num_classes": (C.c_int, []),
     "st_tune_class_shape": (C.c_int, [C.c_int, _P, _P, _P]),
     "st_tune_get": (C.c_int, [_P, _P]),

@@ -43,10 +43,11 @@ class GapCosts:
 
 @dataclass(frozen=True)
 class PrefilterParams:
-    """The segment-evidence fields of the reference's PrefilterParams
-    (src/prefilter.rs:262-303; defaults sequence_default :309-331 and
-    profile_default :333-341), plus span: the seed pattern's span (k for a
-    contiguous seed), which widens each diagonal's window past its last hit."""
+    """The reference's PrefilterParams (src/prefilter.rs:262-303; defaults
+    sequence_default :309-331 and profile_default :333-341): the segment-evidence
+    fields, the similar-k-mer fields, and span: the seed pattern's span (k for a
+    contiguous seed), which widens each diagonal's window past its last hit (taken
+    from the seed index when the seeds are generated on the device)."""
 
     min_hits: int = 1
     min_diag_score: int = 42
@@ -56,6 +57,10 @@ class PrefilterParams:
     regions: bool = False
     diag_window: int = 48
     span: int = 6
+    kmer_score: int = 22
+    max_kmers_per_pos: int = 512
+    exact_seeds: bool = True
+    max_seed_occ: int = 0
 
     @staticmethod
     def sequence_default():
@@ -63,7 +68,11 @@ class PrefilterParams:
 
     @staticmethod
     def profile_default():
-        return PrefilterParams(min_diag_score=30, span=5)
+        return PrefilterParams(min_diag_score=30, span=5, kmer_score=40, exact_seeds=False)
+
+    def seed_c(self):
+        return _lib.SeedParamsC(self.kmer_score, self.max_kmers_per_pos, 1 if self.exact_seeds else 0,
+                                self.max_seed_occ)
 
     def to_c(self, gaps: GapCosts):
         return _lib.PrefilterParamsC(self.min_hits, self.diag_hits, self.max_diagonals, self.diag_window, self.span,
@@ -276,6 +285,61 @@ class Context:
         check(lib.st_prefilter_gate(self._h, ptr(hits), n, C.byref(prm), ptr(out), n, C.byref(n_out),
                                     C.byref(st)))
         return out[:n_out.value].copy(), {f: getattr(st, f) for f in PREFILTER_STATS_FIELDS}
+
+    def seed_index_build(self, seed_mask="111001101"):
+        """Indexes the device database for a seed pattern (0/1 mask; the reference's
+        sequence default 111001101, profile default 11111)."""
+        check(lib.st_seed_index_build(self._h, seed_mask.encode()))
+
+    @staticmethod
+    def _queries(profile_ids, residues):
+        ids = np.ascontiguousarray(profile_ids, dtype=np.uint32)
+        if residues is None:
+            return ids, None, None
+        offs = np.zeros(len(residues) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([len(r) for r in residues])
+        res = np.concatenate([np.asarray(r, dtype=np.uint8) for r in residues]) if len(residues) else \
+            np.zeros(1, np.uint8)
+        return ids, np.ascontiguousarray(res), offs
+
+    def seed_hits(self, profile_ids, residues=None, params: PrefilterParams = None):
+        """Seed hits (SEED_HIT_DTYPE, unordered) of the queries and the seed counters;
+        residues: per query its residue codes (sequence queries) or None (profiles)."""
+        params = params or PrefilterParams.sequence_default()
+        ids, res, offs = self._queries(profile_ids, residues)
+        sp = params.seed_c()
+        st = _lib.SeedStatsC()
+        n = C.c_uint64()
+        args = (self._h, ptr(ids), len(ids), ptr(res) if res is not None else None,
+                ptr(offs) if offs is not None else None, C.byref(sp))
+        check(lib.st_seed_hits(*args, None, 0, C.byref(n), C.byref(st)))
+        out = np.zeros(max(n.value, 1), dtype=SEED_HIT_DTYPE)
+        check(lib.st_seed_hits(*args, ptr(out), n.value, C.byref(n), C.byref(st)))
+        return out[:n.value].copy(), {f: getattr(st, f) for f in _lib.SEED_STATS_FIELDS}
+
+    def prefilter_queries(self, profile_ids, residues=None, params: PrefilterParams = None, gaps: GapCosts = None):
+        """The whole prefilter of the queries on the device (seed hits -> evidence ->
+        chains -> gate -> ranking): candidates (CANDIDATE_DTYPE), evidence counters,
+        seed counters."""
+        params = params or PrefilterParams.sequence_default()
+        gaps = gaps or GapCosts.sequence_default()
+        ids, res, offs = self._queries(profile_ids, residues)
+        sp = params.seed_c()
+        gp = params.to_c(gaps)
+        st = _lib.PrefilterStatsC()
+        sst = _lib.SeedStatsC()
+        n = C.c_uint64()
+        args = (self._h, ptr(ids), len(ids), ptr(res) if res is not None else None,
+                ptr(offs) if offs is not None else None, C.byref(sp), C.byref(gp))
+        cap = 1 << 16
+        while True:
+            out = np.zeros(cap, dtype=CANDIDATE_DTYPE)
+            check(lib.st_prefilter_queries(*args, ptr(out), cap, C.byref(n), C.byref(st), C.byref(sst)))
+            if n.value <= cap:
+                break
+            cap = int(n.value)
+        return (out[:n.value].copy(), {f: getattr(st, f) for f in PREFILTER_STATS_FIELDS},
+                {f: getattr(sst, f) for f in _lib.SEED_STATS_FIELDS})
 
     def prefilter_gate_device(self, d_hits_ptr, n, d_out_ptr, params: PrefilterParams = None,
                               gaps: GapCosts = None):

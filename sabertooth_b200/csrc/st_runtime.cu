@@ -25,6 +25,7 @@
 #include "st_dplan.cuh"
 #include "st_gate.cuh"
 #include "st_calib.cuh"
+#include "st_seed.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
@@ -291,6 +292,11 @@ struct st_ctx {
   DevMem stage;
   DevMem scratch_small;
   Tuning tuning;
+  // seed index over the database (st_seed_index_build): offsets of the 20^w codes, postings
+  DevMem seed_off, seed_post;
+  SeedPat seed_pat{};
+  uint64_t seed_n_post = 0;
+  bool has_seed_index = false;
   // device arenas of finished work, reused by later work; an arena with an
   // event is reusable once the event has completed (work queued before it done)
   struct PoolEntry {
@@ -653,6 +659,7 @@ extern "C" int st_db_upload(st_ctx* c, const uint8_t* residues, const uint64_t* 
   c->n_seqs = n_seqs;
   c->n_res = offsets[n_seqs] - offsets[0];
   c->has_db = true;
+  c->has_seed_index = false;  // an index describes the previous database
   return ST_OK;
 }
 
@@ -3090,6 +3097,264 @@ extern "C" int st_prefilter_gate(st_ctx* c, const st_seed_hit* hits, uint64_t n,
       ST_CUDA(cudaStreamSynchronize(c->stream));
     }
   }
+  return gate_result(st, stats);
+}
+
+// ---------------------------------------------------------------------------
+// seed index and seed hits (st_seed.cuh)
+// ---------------------------------------------------------------------------
+static_assert(sizeof(st_seed_stats) == 9 * 8, "seed stats layout");
+
+extern "C" int st_seed_index_build(st_ctx* c, const char* mask) {
+  CTX_GUARD(c);
+  if (!mask) return fail(ST_EINVAL, "st_seed_index_build: null seed mask");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  // SeedPattern::from_mask (src/prefilter.rs:101-124)
+  SeedPat p{};
+  const size_t len = strlen(mask);
+  for (size_t i = 0; i < len; ++i) {
+    if (mask[i] != '0' && mask[i] != '1') return fail(ST_EINVAL, "seed mask must be 0/1, got '%c'", mask[i]);
+    if (mask[i] == '1') {
+      if (p.w >= static_cast<uint32_t>(kSeedMaxW))
+        return fail(ST_EINVAL, "seed weight above %d is not supported by the device index", kSeedMaxW);
+      p.offs[p.w++] = static_cast<uint32_t>(i);
+    }
+  }
+  if (len == 0 || p.w == 0) return fail(ST_EINVAL, "seed mask has no care ('1') positions");
+  if (mask[0] != '1' || mask[len - 1] != '1') return fail(ST_EINVAL, "seed mask must start and end with '1'");
+  if (p.w < 2) return fail(ST_EINVAL, "seed weight below 2 is not supported");
+  p.span = static_cast<uint32_t>(len);
+  uint64_t n_codes = 1;
+  for (uint32_t i = 0; i < p.w; ++i) n_codes *= kSeedAA;
+  c->has_seed_index = false;
+  ST_TRY(dev_alloc(&c->mt, c->seed_off, (n_codes + 1) * 4));
+  size_t t_scan = 0;
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t_scan, static_cast<uint32_t*>(nullptr),
+                                        static_cast<uint32_t*>(nullptr), n_codes + 1, c->stream));
+  DevMem tmp;
+  ST_TRY(pool_get(c, up256((n_codes + 1) * 4) + t_scan, tmp));
+  uint32_t* cnt = tmp.as<uint32_t>();
+  void* cub_tmp = tmp.as<char>() + up256((n_codes + 1) * 4);
+  ST_CUDA(cudaMemsetAsync(cnt, 0, (n_codes + 1) * 4, c->stream));
+  const DeviceDb db = db_view(c);
+  const uint32_t blocks = static_cast<uint32_t>(
+      std::max<uint64_t>(1, std::min<uint64_t>((c->n_seqs + 7) / 8, static_cast<uint64_t>(c->sms) * 32)));
+  seed_index_kernel<false><<<blocks, 256, 0, c->stream>>>(db, p, cnt, nullptr);
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, t_scan, cnt, c->seed_off.as<uint32_t>(), n_codes + 1, c->stream));
+  // postings: the scan's last entry, read back once
+  ST_TRY(c->pin.reserve(64));
+  uint32_t* h_total = c->pin.as<uint32_t>();
+  ST_CUDA(cudaMemcpyAsync(h_total, c->seed_off.as<uint32_t>() + n_codes, 4, cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  const uint64_t n_post = *h_total;
+  // every window of the database is counted at most once; 32-bit offsets hold it below 2^32
+  if (c->n_res >= 0xFFFFFFFFull) return fail(ST_EINVAL, "database too large for 32-bit seed-index offsets");
+  ST_TRY(dev_alloc(&c->mt, c->seed_post, std::max<uint64_t>(n_post, 1) * sizeof(SeedPost)));
+  ST_CUDA(cudaMemcpyAsync(cnt, c->seed_off.p, n_codes * 4, cudaMemcpyDeviceToDevice, c->stream));
+  seed_index_kernel<true><<<blocks, 256, 0, c->stream>>>(db, p, cnt, c->seed_post.as<SeedPost>());
+  c->launches += 4;
+  ST_CUDA(cudaGetLastError());
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  pool_put(c, std::move(tmp));
+  c->seed_pat = p;
+  c->seed_n_post = n_post;
+  c->has_seed_index = true;
+  return ST_OK;
+}
+
+// The seed stage for a batch of queries: hits (device, pooled in `hits`), their
+// count and the counters.  Two host synchronisations (seed slots, hits) size
+// the buffers.
+static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const uint8_t* residues,
+                      const uint64_t* res_off, const st_seed_params* sp, DevMem& hits, uint32_t* n_hits,
+                      st_seed_stats* stats) {
+  if (!sp) return fail(ST_EINVAL, "null seed parameters");
+  if (sp->max_kmers_per_pos == 0) return fail(ST_EINVAL, "max_kmers_per_pos must be at least 1");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  if (!c->has_seed_index) return fail(ST_ESTATE, "no seed index for the current database (st_seed_index_build)");
+  if (n_q && !profiles) return fail(ST_EINVAL, "null profile ids");
+  if (residues && !res_off) return fail(ST_EINVAL, "residues without offsets");
+  const SeedPat& P = c->seed_pat;
+  std::vector<uint32_t> woff(static_cast<size_t>(n_q) + 1), row0(static_cast<size_t>(n_q) + 1);
+  uint64_t nw = 0, nr = 0;
+  for (uint32_t i = 0; i < n_q; ++i) {
+    ST_TRY(check_profile(c, profiles[i]));
+    const uint64_t m = c->profs[profiles[i]].m;
+    if (residues && res_off[i + 1] - res_off[i] != m)
+      return fail(ST_EINVAL, "query %u: %llu residues for a profile of %llu rows", i,
+                  static_cast<unsigned long long>(res_off[i + 1] - res_off[i]), static_cast<unsigned long long>(m));
+    woff[i] = static_cast<uint32_t>(nw);
+    row0[i] = static_cast<uint32_t>(nr);
+    nw += m >= P.span ? m - P.span + 1 : 0;
+    nr += m;
+    if (nw >= 0x7FFFFFFFull || nr >= 0x7FFFFFFFull) return fail(ST_EINVAL, "too many query positions in one call");
+  }
+  woff[n_q] = static_cast<uint32_t>(nw);
+  row0[n_q] = static_cast<uint32_t>(nr);
+  memset(stats, 0, sizeof *stats);
+  stats->windows = nw;
+  *n_hits = 0;
+  if (nw == 0) return ST_OK;
+  ST_TRY(sync_profiles(c));
+  cudaStream_t s = c->stream;
+  // windows: sorted rows, counts, slots
+  size_t t_scan = 0;
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t_scan, static_cast<uint32_t*>(nullptr),
+                                        static_cast<uint32_t*>(nullptr), nw + 1, s));
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t r = o;
+    o += up256(std::max<size_t>(bytes, 1));
+    return r;
+  };
+  const size_t o_q = take(4ull * n_q), o_wo = take(4ull * (n_q + 1)), o_r0 = take(4ull * (n_q + 1));
+  const size_t o_res = take(residues ? nr : 0), o_rows = take(sizeof(SeedRow) * nr);
+  const size_t o_slots = take(4 * (nw + 1)), o_soff = take(4 * (nw + 1)), o_win = take(sizeof(SeedWin) * nw);
+  const size_t o_st = take(sizeof(SeedStatsDev)), o_tmp = take(t_scan);
+  DevMem wm;
+  ST_TRY(pool_get(c, o, wm));
+  struct Back {
+    st_ctx* c;
+    DevMem* m;
+    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
+  } back_w{c, &wm};
+  char* b = wm.as<char>();
+  ST_CUDA(cudaMemcpyAsync(b + o_q, profiles, 4ull * n_q, cudaMemcpyHostToDevice, s));
+  ST_CUDA(cudaMemcpyAsync(b + o_wo, woff.data(), 4ull * (n_q + 1), cudaMemcpyHostToDevice, s));
+  ST_CUDA(cudaMemcpyAsync(b + o_r0, row0.data(), 4ull * (n_q + 1), cudaMemcpyHostToDevice, s));
+  if (residues) ST_TRY(upload_host(c, b + o_res, residues + res_off[0], nr, s));
+  SeedStatsDev* st = reinterpret_cast<SeedStatsDev*>(b + o_st);
+  ST_CUDA(cudaMemsetAsync(st, 0, sizeof(SeedStatsDev), s));
+  SeedQ Q;
+  Q.qids = reinterpret_cast<const uint32_t*>(b + o_q);
+  Q.woff = reinterpret_cast<const uint32_t*>(b + o_wo);
+  Q.row0 = reinterpret_cast<const uint32_t*>(b + o_r0);
+  Q.res = residues ? reinterpret_cast<const uint8_t*>(b + o_res) : nullptr;
+  Q.rows = reinterpret_cast<const SeedRow*>(b + o_rows);
+  Q.n_q = n_q;
+  Q.n_win = static_cast<uint32_t>(nw);
+  Q.thr = sp->kmer_score;
+  Q.cap = sp->max_kmers_per_pos;
+  Q.exact = (residues && sp->exact_seeds) ? 1u : 0u;
+  uint32_t* slots = reinterpret_cast<uint32_t*>(b + o_slots);
+  uint32_t* soff = reinterpret_cast<uint32_t*>(b + o_soff);
+  SeedWin* win = reinterpret_cast<SeedWin*>(b + o_win);
+  auto grid_for = [&](uint64_t items, uint32_t block) {
+    const uint64_t cap = static_cast<uint64_t>(c->sms) * (2048 / block) * 4;
+    return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>((items + block - 1) / block, cap)));
+  };
+  seed_sort_rows_kernel<<<n_q, 128, 0, s>>>(prof_view(c), Q.qids, Q.row0, const_cast<SeedRow*>(Q.rows));
+  seed_count_kernel<<<grid_for(nw + 1, 128), 128, 0, s>>>(Q, P, slots, win, st);
+  size_t t = t_scan;
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(b + o_tmp, t, slots, soff, nw + 1, s));
+  c->launches += 3;
+  ST_CUDA(cudaGetLastError());
+  ST_TRY(c->pin.reserve(64));
+  uint32_t* h = c->pin.as<uint32_t>();
+  ST_CUDA(cudaMemcpyAsync(h, soff + nw, 4, cudaMemcpyDeviceToHost, s));
+  ST_CUDA(cudaStreamSynchronize(s));
+  const uint64_t ns = *h;
+  // seeds: k-mers, posting counts, hit offsets
+  size_t t_scan2 = 0;
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t_scan2, static_cast<uint32_t*>(nullptr),
+                                        static_cast<uint32_t*>(nullptr), ns + 1, s));
+  o = 0;
+  const size_t o_seeds = take(sizeof(SeedSeed) * ns), o_cnt = take(4 * (ns + 1)), o_hoff = take(4 * (ns + 1));
+  const size_t o_tmp2 = take(t_scan2);
+  DevMem sm;
+  ST_TRY(pool_get(c, o, sm));
+  struct Back back_s{c, &sm};
+  char* b2 = sm.as<char>();
+  SeedSeed* seeds = reinterpret_cast<SeedSeed*>(b2 + o_seeds);
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(b2 + o_cnt);
+  uint32_t* hoff = reinterpret_cast<uint32_t*>(b2 + o_hoff);
+  if (ns) seed_emit_kernel<<<grid_for(nw, 128), 128, 0, s>>>(Q, P, soff, win, seeds, st);
+  seed_post_count_kernel<<<grid_for(ns + 1, 256), 256, 0, s>>>(seeds, static_cast<uint32_t>(ns),
+                                                               c->seed_off.as<uint32_t>(),
+                                                               sp->max_seed_occ, cnt, st);
+  t = t_scan2;
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(b2 + o_tmp2, t, cnt, hoff, ns + 1, s));
+  c->launches += 3;
+  ST_CUDA(cudaGetLastError());
+  ST_TRY(c->pin.reserve(sizeof(SeedStatsDev) + 64));
+  SeedStatsDev* hst = reinterpret_cast<SeedStatsDev*>(c->pin.as<char>());
+  uint32_t* h_hits = reinterpret_cast<uint32_t*>(c->pin.as<char>() + sizeof(SeedStatsDev));
+  ST_CUDA(cudaMemcpyAsync(hst, st, sizeof(SeedStatsDev), cudaMemcpyDeviceToHost, s));
+  ST_CUDA(cudaMemcpyAsync(h_hits, hoff + ns, 4, cudaMemcpyDeviceToHost, s));
+  ST_CUDA(cudaStreamSynchronize(s));
+  const SeedStatsDev sd = *hst;
+  const uint64_t nh = *h_hits;
+  stats->windows_skipped = sd.windows_skipped;
+  stats->kmers_generated = sd.kmers_generated;
+  stats->windows_at_cap = sd.windows_at_cap;
+  stats->exact_seeds_added = sd.exact_seeds_added;
+  stats->seeds = sd.seeds;
+  stats->postings_visited = sd.postings_visited;
+  stats->seeds_over_occ_cap = sd.seeds_over_occ_cap;
+  stats->postings_skipped_occ = sd.postings_skipped_occ;
+  if (sd.errors)
+    return fail(ST_EINVAL, "%llu windows have a score range above %d histogram bins (rows too wide for the "
+                "device seed generator)", sd.errors, kSeedMaxBins);
+  if (sd.postings_visited >= 0x7FFFFFFFull) return fail(ST_EINVAL, "too many seed hits in one call");
+  ST_TRY(pool_get(c, std::max<uint64_t>(nh, 1) * sizeof(GateSeedHit), hits));
+  if (nh) {
+    seed_hits_kernel<<<grid_for(ns, 256), 256, 0, s>>>(Q, seeds, static_cast<uint32_t>(ns), cnt, hoff,
+                                                       c->seed_off.as<uint32_t>(), c->seed_post.as<SeedPost>(),
+                                                       hits.as<GateSeedHit>());
+    ++c->launches;
+    ST_CUDA(cudaGetLastError());
+  }
+  *n_hits = static_cast<uint32_t>(nh);
+  return ST_OK;
+}
+
+extern "C" int st_seed_hits(st_ctx* c, const uint32_t* profiles, uint32_t n_queries, const uint8_t* residues,
+                            const uint64_t* residue_offsets, const st_seed_params* params, st_seed_hit* out,
+                            uint64_t cap, uint64_t* n_out, st_seed_stats* stats) {
+  CTX_GUARD(c);
+  if (!n_out || (cap && !out)) return fail(ST_EINVAL, "st_seed_hits: null argument");
+  DevMem hits;
+  uint32_t nh = 0;
+  st_seed_stats st{};
+  *n_out = 0;
+  ST_TRY(seed_stage(c, profiles, n_queries, residues, residue_offsets, params, hits, &nh, &st));
+  if (stats) *stats = st;
+  *n_out = nh;
+  const uint64_t k = std::min<uint64_t>(cap, nh);
+  if (k) ST_CUDA(cudaMemcpyAsync(out, hits.p, k * sizeof(st_seed_hit), cudaMemcpyDeviceToHost, c->stream));
+  ST_CUDA(cudaStreamSynchronize(c->stream));
+  pool_put(c, std::move(hits));
+  return ST_OK;
+}
+
+extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_t n_queries, const uint8_t* residues,
+                                    const uint64_t* residue_offsets, const st_seed_params* seed_params,
+                                    const st_prefilter_params* params, st_candidate* out, uint64_t cap,
+                                    uint64_t* n_out, st_prefilter_stats* stats, st_seed_stats* seed_stats) {
+  CTX_GUARD(c);
+  if (!n_out || (cap && !out) || !params) return fail(ST_EINVAL, "st_prefilter_queries: null argument");
+  *n_out = 0;
+  st_prefilter_params gp = *params;
+  if (c->has_seed_index) gp.span = c->seed_pat.span;  // the index's seed pattern sets the window span
+  GateConf g;
+  int qbits = 0;
+  ST_TRY(gate_conf(c, &gp, g, qbits));
+  DevMem hits;
+  uint32_t nh = 0;
+  st_seed_stats sst{};
+  ST_TRY(seed_stage(c, profiles, n_queries, residues, residue_offsets, seed_params, hits, &nh, &sst));
+  if (seed_stats) *seed_stats = sst;
+  GateStats st{};
+  if (nh) {
+    DevMem cm;
+    ST_TRY(pool_get(c, static_cast<size_t>(nh) * sizeof(GateCandidate), cm));
+    ST_TRY(gate_pipeline(c, hits.as<GateSeedHit>(), nh, g, qbits, cm.as<GateCandidate>(), n_out, &st));
+    const uint64_t k = std::min<uint64_t>(cap, *n_out);
+    if (k) ST_CUDA(cudaMemcpyAsync(out, cm.p, k * sizeof(st_candidate), cudaMemcpyDeviceToHost, c->stream));
+    ST_CUDA(cudaStreamSynchronize(c->stream));
+    pool_put(c, std::move(cm));
+  }
+  pool_put(c, std::move(hits));
   return gate_result(st, stats);
 }
 
