@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--serving-seconds", type=float, default=2.0, help="arrival window per swept rate")
     ap.add_argument("--calib-profiles", type=int, default=1000,
                     help="config-3 profiles for the per-profile calibration measurement (0: skip)")
+    ap.add_argument("--search-queries", type=int, default=1000,
+                    help="config-5 queries for the whole-search measurement (0: skip)")
+    ap.add_argument("--search-targets", type=int, default=1_000_000, help="config-5 database sequences")
     ap.add_argument("--gate-hits", type=int, default=20_000_000,
                     help="seed hits for the evidence / chain / gate measurement (0: skip)")
     return ap.parse_args()
@@ -441,6 +444,8 @@ def main():
         result["ungapped"] = ungapped_measure(ctx, args)
     if result is not None and args.gate_hits > 0:
         result["gate"] = gate_measure(ctx, args)
+    if result is not None and args.search_queries > 0:
+        result["search"] = search_measure(ctx, args)
     if result is not None and args.serving_pairs > 0:
         result["serving"] = serving_measure(ctx, args)
     if world > 1:
@@ -526,6 +531,102 @@ def ungapped_measure(ctx, args):
                                                        "reference's AVX2 batched Kadane (biased u8 tables, 32 lanes, "
                                                        "window-start order, exact rescore) restated in C, queries in "
                                                        "parallel over all host threads"},
+            "setup_s": round(t_gen, 1)}
+
+
+def search_measure(ctx, args):
+    """Config 5 as whole searches: a 10^6-sequence database (~265 M residues) and 1,000 sequence queries, each
+    with 5 planted homologs; the reference's sequence defaults (spaced seed 111001101, k-mer score 22, 512 k-mers
+    per window, exact seeds, 4 diagonals, window 48) with the gate moved to the database size
+    (size_adjusted_gate, src/prefilter.rs:253-257); gaps 11/1.  One step = st_prefilter_queries for the whole
+    batch (host residues in, ranked candidates out: seeds -> hits -> evidence -> chains -> gate) then
+    st_sw_score_pairs over every candidate (host pairs in, scores out)."""
+    from oracle import oracle as O
+    from sabertooth_b200 import GapCosts, PrefilterParams
+    from sabertooth_b200._lib import PAIR_DTYPE
+    from sabertooth_b200 import workloads as W
+    t0 = time.perf_counter()
+    w = W.config5(seed=args.seed, n_queries=args.search_queries, n_targets=args.search_targets)
+    t_gen = time.perf_counter() - t0
+    n_res = int(w.db_offsets[-1])
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    t0 = time.perf_counter()
+    ctx.seed_index_build("111001101")
+    t_index = time.perf_counter() - t0
+    ids = ctx.create_profiles(w.rows)
+    gate = W.size_adjusted_gate(42, n_res)
+    params = PrefilterParams(min_diag_score=gate, span=9)
+    gaps = GapCosts.sequence_default()
+    ctx.prefilter_queries(ids[:16], w.queries[:16], params, gaps)  # warm-up
+    qlen = np.array([len(q) for q in w.queries], dtype=np.int64)
+    tlen = np.diff(w.db_offsets.astype(np.int64))
+    runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        cands, st, sst = ctx.prefilter_queries(ids, w.queries, params, gaps)
+        t1 = time.perf_counter()
+        pairs = np.zeros(len(cands), dtype=PAIR_DTYPE)
+        pairs["profile"] = cands["query"]
+        pairs["target"] = cands["target"]
+        pairs["band_radius"] = -1
+        scores = ctx.sw_score_pairs(pairs, gaps)
+        t2 = time.perf_counter()
+        runs.append((t1 - t0, t2 - t1))
+    t_pre = float(np.median([r[0] for r in runs]))
+    t_sw = float(np.median([r[1] for r in runs]))
+    inv = np.zeros(int(ids.max()) + 1, dtype=np.int64)
+    inv[ids] = np.arange(len(ids))
+    cq = inv[cands["query"]]
+    cells = int((qlen[cq] * tlen[cands["target"]]).sum())
+    # CPU baseline: the restated seed stage (best-first similar k-mers over a direct-table index) + evidence +
+    # gate, then the reference's AVX2 striped SW over the candidates, for a sample of queries on all host threads
+    t0 = time.perf_counter()
+    di = O.DirectSeedIndex(w.db_residues, w.db_offsets, "111001101")
+    t_cpu_index = time.perf_counter() - t0
+    k = min(48, len(ids))
+    sp = {"kmer_score": params.kmer_score, "max_kmers_per_pos": params.max_kmers_per_pos, "exact_seeds": 1,
+          "max_seed_occ": 0}
+    gp = {"min_hits": params.min_hits, "diag_hits": params.diag_hits, "max_diagonals": params.max_diagonals,
+          "diag_window": params.diag_window, "span": 9, "min_diag_score": gate, "gap_open": gaps.open,
+          "gap_ext": gaps.extend, "max_candidates": params.max_candidates, "regions": 0}
+    t0 = time.perf_counter()
+    cc, nc, nh = O.prefilter_search(w.rows[:k], w.queries[:k], di, sp, gp, cap_per_query=1 << 15)
+    t_cpu_pre = time.perf_counter() - t0
+    same = True
+    for q in range(k):
+        g = cands[cq == q].copy()
+        g["query"] = q
+        same &= bool(np.array_equal(g, cc[q]))
+    sample = np.concatenate([cc[q] for q in range(k)]) if k else np.zeros(0, dtype=O.CANDIDATE_DTYPE)
+    targets_s = np.unique(sample["target"]) if len(sample) else np.zeros(0, np.uint32)
+    remap = {int(t): i for i, t in enumerate(targets_s)}
+    arena = O.Arena(w.rows[:k], [w.db_residues[int(w.db_offsets[t]):int(w.db_offsets[t + 1])] for t in targets_s])
+    t0 = time.perf_counter()
+    cpu_scores = O.striped_pairs(arena, sample["query"], np.array([remap[int(t)] for t in sample["target"]],
+                                                                  dtype=np.uint32), gaps.open, gaps.extend)
+    t_cpu_sw = time.perf_counter() - t0
+    gpu_s = np.concatenate([scores[cq == q] for q in range(k)]) if k else np.zeros(0, np.int32)
+    same_scores = bool(same and np.array_equal(cpu_scores, gpu_s))
+    ctx.free_profiles(ids)
+    nq = len(ids)
+    return {"workload": f"config 5 searches: {nq} sequence queries against {len(tlen)} targets ({n_res / 1e6:.0f} M "
+                        f"residues), 5 planted homologs per query; seed 111001101, k-mer score 22, cap 512, exact "
+                        f"seeds, gate {gate} (size-adjusted 42), gaps 11/1",
+            "index_build_s": round(t_index, 3),
+            "prefilter_ms": round(t_pre * 1e3, 1), "sw_ms": round(t_sw * 1e3, 1),
+            "queries_per_s": round(nq / (t_pre + t_sw), 1), "prefilter_queries_per_s": round(nq / t_pre, 1),
+            "hits": int(sst["postings_visited"]), "ghits_per_s": round(sst["postings_visited"] / t_pre / 1e9, 2),
+            "candidates": int(len(cands)), "sw_cells": cells, "sw_gcups": round(cells / t_sw / 1e9, 1),
+            "seed_stats": {k_: int(v) for k_, v in sst.items()},
+            "gate_stats": {k_: int(v) for k_, v in st.items()},
+            "matches_cpu_baseline": same, "sw_scores_match_cpu_baseline": same_scores,
+            "cpu_baseline": {"value": round(k / (t_cpu_pre + t_cpu_sw), 2), "unit": "queries/s",
+                             "cores": os.cpu_count(), "kind": "port",
+                             "prefilter_s": round(t_cpu_pre, 2), "sw_s": round(t_cpu_sw, 2),
+                             "index_build_s": round(t_cpu_index, 1),
+                             "sample": f"{k} queries on the whole database: the restated seed stage (best-first "
+                                       "similar k-mers, direct-table index), evidence and gate, then the reference's "
+                                       "AVX2 striped SW over their candidates, all host threads"},
             "setup_s": round(t_gen, 1)}
 
 

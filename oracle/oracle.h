@@ -180,6 +180,19 @@ void or_index_build(const uint8_t* tgt_arena, const uint64_t* tgt_off, uint32_t 
 uint64_t or_seed_hits(const int32_t* rows, const uint8_t* residues, uint32_t m, const uint32_t* offs, uint32_t w,
                       uint32_t span, const or_seed_params* p, const or_posting* idx, uint64_t n_post, uint32_t query,
                       uint32_t* ht, int32_t* hd, uint32_t* hqpos, uint64_t cap_hits, or_seed_stats* st);
+/* Direct-table index: count_only = 1 fills off (20^w + 1 entries, prefix sums:
+ * off[c] = first posting of code c) and returns the postings; count_only = 0
+ * fills post_t/post_p and advances off[c] to the end of each code (shift it back
+ * by one entry, off[c] = old off[c-1], before lookups). */
+uint64_t or_index_direct_build(const uint8_t* tgt_arena, const uint64_t* tgt_off, uint32_t n_targets,
+                               const uint32_t* offs, uint32_t w, uint32_t span, uint64_t* off, uint32_t* post_t,
+                               uint32_t* post_p, int count_only);
+void or_prefilter_search(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
+                         const uint8_t* res_arena, uint32_t n_queries, const uint8_t* tgt_arena,
+                         const uint64_t* tgt_off, const uint32_t* offs, uint32_t w, uint32_t span,
+                         const uint64_t* off, const uint32_t* post_t, const uint32_t* post_p,
+                         const or_seed_params* sp, const or_prefilter_params* gp, or_candidate* out,
+                         uint64_t cap_per_query, uint64_t* n_cand, uint64_t* n_hits, int nthreads);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,9 @@ def _load():
     lib.or_index_count.restype = u64
     lib.or_index_count.argtypes = [P, P, u32, P, u32, u32]
     lib.or_index_build.argtypes = [P, P, u32, P, u32, u32, P]
+    lib.or_index_direct_build.restype = u64
+    lib.or_index_direct_build.argtypes = [P, P, u32, P, u32, u32, P, P, P, C.c_int]
+    lib.or_prefilter_search.argtypes = [P, P, P, P, u32, P, P, P, u32, u32, P, P, P, P, P, P, u64, P, P, C.c_int]
     lib.or_seed_hits.restype = u64
     lib.or_seed_hits.argtypes = [P, P, u32, P, u32, u32, P, P, u64, u32, P, P, P, u64, P]
     return lib
@@ -319,3 +322,50 @@ def seed_hits(rows, residues, index: SeedIndex, kmer_score, max_kmers_per_pos=51
     hq = np.zeros(max(n, 1), dtype=np.uint32)
     lib.or_seed_hits(*args, _p(ht), _p(hd), _p(hq), n, _p(st))
     return ht[:n], hd[:n], hq[:n], {f: int(v) for f, v in zip(SEED_STATS_FIELDS, st)}
+
+
+class DirectSeedIndex:
+    """The CPU seed index as a direct table (counting sort over all windows)."""
+
+    def __init__(self, tgt_arena, tgt_off, mask):
+        self.offs, self.span = pattern_offsets(mask)
+        self.w = len(self.offs)
+        self.tgt = np.ascontiguousarray(tgt_arena, dtype=np.uint8)
+        self.tgt_off = np.ascontiguousarray(tgt_off, dtype=np.uint64)
+        nt = len(self.tgt_off) - 1
+        self.off = np.zeros(20 ** self.w + 1, dtype=np.uint64)
+        n = int(lib.or_index_direct_build(_p(self.tgt), _p(self.tgt_off), nt, _p(self.offs), self.w, self.span,
+                                          _p(self.off), None, None, 1))
+        self.post_t = np.zeros(max(n, 1), dtype=np.uint32)
+        self.post_p = np.zeros(max(n, 1), dtype=np.uint32)
+        lib.or_index_direct_build(_p(self.tgt), _p(self.tgt_off), nt, _p(self.offs), self.w, self.span,
+                                  _p(self.off), _p(self.post_t), _p(self.post_p), 0)
+        self.off[1:] = self.off[:-1].copy()
+        self.off[0] = 0
+        self.n = n
+
+
+def prefilter_search(rows_list, residues, index: DirectSeedIndex, seed_p: dict, gate_p: dict, cap_per_query=4096,
+                     threads=0):
+    """Seeds + evidence + gate for each query over a DirectSeedIndex, queries in parallel:
+    (candidates per query, truncated to cap_per_query; candidate counts; hit counts)."""
+    arena = Arena(rows_list, [])
+    nq = len(rows_list)
+    res = None
+    if residues is not None:
+        res = np.ascontiguousarray(np.concatenate([np.asarray(r, np.uint8) for r in residues]))
+    sp = np.zeros(1, dtype=_SEED_PARAM_DTYPE)
+    for f in _SEED_PARAM_DTYPE.names:
+        sp[f] = seed_p[f]
+    gp = np.zeros(1, dtype=_PARAM_DTYPE)
+    for f in PARAM_FIELDS:
+        gp[f] = gate_p[f]
+    out = np.zeros(nq * cap_per_query, dtype=CANDIDATE_DTYPE)
+    n_cand = np.zeros(nq, dtype=np.uint64)
+    n_hits = np.zeros(nq, dtype=np.uint64)
+    lib.or_prefilter_search(_p(arena.rows), _p(arena.row_off), _p(arena.qlen), _p(res), nq, _p(index.tgt),
+                            _p(index.tgt_off), _p(index.offs), index.w, index.span, _p(index.off), _p(index.post_t),
+                            _p(index.post_p), _p(sp), _p(gp), _p(out), cap_per_query, _p(n_cand), _p(n_hits),
+                            threads or os.cpu_count() or 1)
+    cands = [out[q * cap_per_query:q * cap_per_query + min(int(n_cand[q]), cap_per_query)] for q in range(nq)]
+    return cands, n_cand, n_hits

@@ -268,3 +268,123 @@ uint64_t or_seed_hits(const int32_t* rows, const uint8_t* residues, uint32_t m, 
   free(scores);
   return nh;
 }
+
+/* ---- direct-table index and batched queries (the CPU baseline of the search) ----
+ * The same index as or_index_build as a direct table: off[code] .. off[code+1]
+ * indexes post (target, position) pairs, built by a counting sort over all
+ * windows (20^w + 1 offsets, w <= 7). */
+uint64_t or_index_direct_build(const uint8_t* tgt_arena, const uint64_t* tgt_off, uint32_t n_targets,
+                               const uint32_t* offs, uint32_t w, uint32_t span, uint64_t* off, uint32_t* post_t,
+                               uint32_t* post_p, int count_only) {
+  uint64_t n_codes = 1;
+  for (uint32_t i = 0; i < w; ++i) n_codes *= AA;
+  if (count_only) memset(off, 0, (n_codes + 1) * sizeof(uint64_t));
+  for (uint32_t t = 0; t < n_targets; ++t) {
+    const uint8_t* s = tgt_arena + tgt_off[t];
+    const uint64_t len = tgt_off[t + 1] - tgt_off[t];
+    if (len < span) continue;
+    for (uint64_t st = 0; st + span <= len; ++st) {
+      uint64_t code = 0;
+      int ok = 1;
+      for (uint32_t i = 0; i < w; ++i) {
+        const uint8_t r = s[st + offs[i]];
+        if (r >= AA) ok = 0;
+        code = code * AA + r;
+      }
+      if (!ok) continue;
+      if (count_only) {
+        off[code + 1]++;
+      } else {
+        const uint64_t k = off[code]++;
+        post_t[k] = t;
+        post_p[k] = (uint32_t)st;
+      }
+    }
+  }
+  if (count_only)
+    for (uint64_t c = 0; c < n_codes; ++c) off[c + 1] += off[c];
+  return off[n_codes];
+}
+
+/* Queries in parallel over the direct index (off already shifted back: off[c] is
+ * the start of code c): seed hits as or_seed_hits, then the evidence stage of
+ * or_prefilter_query.  n_cand[q] receives each query's candidate count; at most
+ * cap_per_query candidates of query q are written at out + q * cap_per_query. */
+void or_prefilter_search(const int32_t* rows_arena, const uint64_t* row_off, const uint32_t* qlen,
+                         const uint8_t* res_arena, uint32_t n_queries, const uint8_t* tgt_arena,
+                         const uint64_t* tgt_off, const uint32_t* offs, uint32_t w, uint32_t span,
+                         const uint64_t* off, const uint32_t* post_t, const uint32_t* post_p,
+                         const or_seed_params* sp, const or_prefilter_params* gp, or_candidate* out,
+                         uint64_t cap_per_query, uint64_t* n_cand, uint64_t* n_hits, int nthreads) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int64_t q = 0; q < (int64_t)n_queries; ++q) {
+    const int32_t* rows = rows_arena + row_off[q] * OR_NPROF;
+    const uint32_t m = qlen[q];
+    const uint8_t* res = res_arena ? res_arena + row_off[q] : NULL;
+    n_cand[q] = 0;
+    n_hits[q] = 0;
+    if (m < span) continue;
+    srow* sr = (srow*)malloc((size_t)m * sizeof(srow));
+    for (uint32_t i = 0; i < m; ++i) sort_row(rows + (size_t)i * OR_NPROF, &sr[i]);
+    uint64_t* codes = (uint64_t*)malloc(((size_t)sp->max_kmers_per_pos + 1) * sizeof(uint64_t));
+    int32_t* scores = (int32_t*)malloc(((size_t)sp->max_kmers_per_pos + 1) * sizeof(int32_t));
+    uint64_t cap_h = 1 << 16, nh = 0;
+    uint32_t* ht = (uint32_t*)malloc(cap_h * 4);
+    int32_t* hd = (int32_t*)malloc(cap_h * 4);
+    uint32_t* hq = (uint32_t*)malloc(cap_h * 4);
+    for (uint32_t start = 0; start + span <= m; ++start) {
+      srow wr[MAXK];
+      uint64_t exact = 0;
+      int skip = 0;
+      for (uint32_t i = 0; i < w; ++i) {
+        const uint32_t c = start + offs[i];
+        if (res) {
+          if (res[c] >= AA) {
+            skip = 1;
+            break;
+          }
+          exact = exact * AA + res[c];
+        }
+        wr[i] = sr[c];
+      }
+      if (skip) continue;
+      uint32_t nk = 0;
+      top_kmers_sorted(wr, (int)w, sp->kmer_score, sp->max_kmers_per_pos, codes, scores, &nk);
+      int have = 0;
+      for (uint32_t k = 0; k < nk; ++k) have |= codes[k] == exact;
+      if (res && sp->exact_seeds && !have) codes[nk++] = exact;
+      for (uint32_t k = 0; k < nk; ++k) {
+        const uint64_t a = off[codes[k]], b = off[codes[k] + 1];
+        if (b <= a || (sp->max_seed_occ > 0 && b - a > sp->max_seed_occ)) continue;
+        if (nh + (b - a) > cap_h) {
+          while (nh + (b - a) > cap_h) cap_h *= 2;
+          ht = (uint32_t*)realloc(ht, cap_h * 4);
+          hd = (int32_t*)realloc(hd, cap_h * 4);
+          hq = (uint32_t*)realloc(hq, cap_h * 4);
+        }
+        for (uint64_t e = a; e < b; ++e) {
+          ht[nh] = post_t[e];
+          hd[nh] = (int32_t)post_p[e] - (int32_t)start;
+          hq[nh] = start;
+          ++nh;
+        }
+      }
+    }
+    n_hits[q] = nh;
+    if (nh) {
+      or_candidate* tmp = (or_candidate*)malloc(nh * sizeof(or_candidate));
+      or_prefilter_stats st;
+      const uint64_t nc =
+          or_prefilter_query(rows, m, (uint32_t)q, tgt_arena, tgt_off, ht, hd, hq, nh, gp, 1, tmp, &st);
+      n_cand[q] = nc;
+      memcpy(out + (size_t)q * cap_per_query, tmp, (nc < cap_per_query ? nc : cap_per_query) * sizeof(or_candidate));
+      free(tmp);
+    }
+    free(sr);
+    free(codes);
+    free(scores);
+    free(ht);
+    free(hd);
+    free(hq);
+  }
+}

@@ -3327,35 +3327,83 @@ extern "C" int st_seed_hits(st_ctx* c, const uint32_t* profiles, uint32_t n_quer
   return ST_OK;
 }
 
+// Queries are taken in chunks of at most this many seed windows (about 250
+// queries of 250 residues), which bounds the hits held on the device at once.
+constexpr uint64_t kSearchChunkWindows = 1ull << 16;
+
 extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_t n_queries, const uint8_t* residues,
                                     const uint64_t* residue_offsets, const st_seed_params* seed_params,
                                     const st_prefilter_params* params, st_candidate* out, uint64_t cap,
                                     uint64_t* n_out, st_prefilter_stats* stats, st_seed_stats* seed_stats) {
   CTX_GUARD(c);
-  if (!n_out || (cap && !out) || !params) return fail(ST_EINVAL, "st_prefilter_queries: null argument");
+  if (!n_out || (cap && !out) || !params || (n_queries && !profiles))
+    return fail(ST_EINVAL, "st_prefilter_queries: null argument");
+  if (residues && !residue_offsets) return fail(ST_EINVAL, "residues without offsets");
   *n_out = 0;
+  if (!c->has_seed_index) return fail(ST_ESTATE, "no seed index for the current database (st_seed_index_build)");
   st_prefilter_params gp = *params;
-  if (c->has_seed_index) gp.span = c->seed_pat.span;  // the index's seed pattern sets the window span
+  gp.span = c->seed_pat.span;  // the index's seed pattern sets the window span
   GateConf g;
   int qbits = 0;
   ST_TRY(gate_conf(c, &gp, g, qbits));
-  DevMem hits;
-  uint32_t nh = 0;
-  st_seed_stats sst{};
-  ST_TRY(seed_stage(c, profiles, n_queries, residues, residue_offsets, seed_params, hits, &nh, &sst));
-  if (seed_stats) *seed_stats = sst;
-  GateStats st{};
-  if (nh) {
-    DevMem cm;
-    ST_TRY(pool_get(c, static_cast<size_t>(nh) * sizeof(GateCandidate), cm));
-    ST_TRY(gate_pipeline(c, hits.as<GateSeedHit>(), nh, g, qbits, cm.as<GateCandidate>(), n_out, &st));
-    const uint64_t k = std::min<uint64_t>(cap, *n_out);
-    if (k) ST_CUDA(cudaMemcpyAsync(out, cm.p, k * sizeof(st_candidate), cudaMemcpyDeviceToHost, c->stream));
-    ST_CUDA(cudaStreamSynchronize(c->stream));
-    pool_put(c, std::move(cm));
+  for (uint32_t i = 0; i < n_queries; ++i) ST_TRY(check_profile(c, profiles[i]));
+  GateStats tot{};
+  st_seed_stats stot{};
+  std::vector<st_candidate> all;
+  uint32_t q0 = 0;
+  while (q0 < n_queries) {
+    uint32_t q1 = q0;
+    uint64_t wins = 0;
+    do {
+      const uint64_t m = c->profs[profiles[q1]].m;
+      wins += m >= c->seed_pat.span ? m - c->seed_pat.span + 1 : 0;
+      ++q1;
+    } while (q1 < n_queries && wins < kSearchChunkWindows);
+    DevMem hits;
+    uint32_t nh = 0;
+    st_seed_stats sst{};
+    ST_TRY(seed_stage(c, profiles + q0, q1 - q0, residues, residues ? residue_offsets + q0 : nullptr, seed_params,
+                      hits, &nh, &sst));
+    stot.windows += sst.windows;
+    stot.windows_skipped += sst.windows_skipped;
+    stot.kmers_generated += sst.kmers_generated;
+    stot.windows_at_cap += sst.windows_at_cap;
+    stot.exact_seeds_added += sst.exact_seeds_added;
+    stot.seeds += sst.seeds;
+    stot.postings_visited += sst.postings_visited;
+    stot.seeds_over_occ_cap += sst.seeds_over_occ_cap;
+    stot.postings_skipped_occ += sst.postings_skipped_occ;
+    if (nh) {
+      DevMem cm;
+      ST_TRY(pool_get(c, static_cast<size_t>(nh) * sizeof(GateCandidate), cm));
+      GateStats st{};
+      uint64_t nc = 0;
+      ST_TRY(gate_pipeline(c, hits.as<GateSeedHit>(), nh, g, qbits, cm.as<GateCandidate>(), &nc, &st));
+      const size_t at = all.size();
+      all.resize(at + nc);
+      if (nc) ST_CUDA(cudaMemcpyAsync(all.data() + at, cm.p, nc * sizeof(st_candidate), cudaMemcpyDeviceToHost,
+                                      c->stream));
+      ST_CUDA(cudaStreamSynchronize(c->stream));
+      pool_put(c, std::move(cm));
+      tot.targets_hit += st.targets_hit;
+      tot.targets_evaluated += st.targets_evaluated;
+      tot.diagonals_scored += st.diagonals_scored;
+      tot.chains_used += st.chains_used;
+      tot.candidates += st.candidates;
+      tot.candidates_capped += st.candidates_capped;
+      tot.hits_rejected += st.hits_rejected;
+    }
+    pool_put(c, std::move(hits));
+    q0 = q1;
   }
-  pool_put(c, std::move(hits));
-  return gate_result(st, stats);
+  // chunks are ranked by query id inside themselves; order the whole list by query id
+  std::stable_sort(all.begin(), all.end(),
+                   [](const st_candidate& x, const st_candidate& y) { return x.query < y.query; });
+  if (seed_stats) *seed_stats = stot;
+  *n_out = all.size();
+  const uint64_t k = std::min<uint64_t>(cap, all.size());
+  if (k) memcpy(out, all.data(), k * sizeof(st_candidate));
+  return gate_result(tot, stats);
 }
 
 // ---------------------------------------------------------------------------

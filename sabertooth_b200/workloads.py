@@ -501,3 +501,60 @@ def seed_hits(seed=0, n_queries=1000, n_targets=374_000, n_hits=20_000_000, homo
     return SeedHitWorkload("seed-hits-gate", [seq_rows(model, q) for q in queries], arena, offs, hits[perm],
                            info={"queries": n_queries, "targets": n_targets, "hits": int(hits.size),
                                  "db_residues": total, "homolog_targets": int(hom_t.size), "seed": seed})
+
+
+# ---- config 5: whole searches (seeds -> gate -> SW) ---------------------------
+@dataclass
+class SearchWorkload:
+    name: str
+    queries: list       # uint8 residue codes per query
+    rows: list          # int32 [m][21] BLOSUM62 rows per query
+    db_residues: np.ndarray
+    db_offsets: np.ndarray
+    info: dict = field(default_factory=dict)
+
+
+def size_adjusted_gate(gate, db_residues):
+    """size_adjusted_gate (src/prefilter.rs:253-257): the gate of a 10^8-residue
+    database moved by 2.5 (below) or 1.0 (above) per e-fold of database size,
+    rounded half away from zero and clamped to 20..60."""
+    x = np.log(max(db_residues, 1) / 1.0e8)
+    slope = 2.5 if x < 0 else 1.0
+    v = gate + slope * x
+    r = np.floor(abs(v) + 0.5) * np.sign(v)
+    return int(min(max(r, 20), 60))
+
+
+def config5(seed=0, n_queries=1000, n_targets=1_000_000, homologs_per_query=5, keep=0.5, model=None):
+    """Config 5's search workload: a database of n_targets sequences (lognormal
+    median 250, sigma 0.35, clipped 30-1,000: about 265 M residues for 10^6
+    targets) and sequence queries (lognormal median 250, sigma 0.5, clipped
+    30-5,000); each query has homologs_per_query mutated copies (BLOSUM62-
+    conditional substitutions keeping `keep` of the sites, indels at 2 % per site)
+    planted into random targets."""
+    model = model or Model()
+    rng = Rng(seed)
+    ql = lognormal_lengths(rng, n_queries, 250, 0.5, 30, 5000)
+    queries = [model.background(rng.child(i), int(l)) for i, l in enumerate(ql)]
+    tl = lognormal_lengths(rng, n_targets, 250, 0.35, 30, 1000)
+    offs = np.zeros(n_targets + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum(tl)
+    total = int(offs[-1])
+    arena = np.empty(total, dtype=np.uint8)
+    chunk = 1 << 24
+    for k, a in enumerate(range(0, total, chunk)):
+        b = min(total, a + chunk)
+        arena[a:b] = model.background(rng.child(10_000_000 + k), b - a)
+    hr = rng.child(98)
+    picks = hr.below(n_queries * homologs_per_query, n_targets)
+    for j, t in enumerate(picks):
+        q = queries[j // homologs_per_query]
+        h = model.mutate(hr, q, keep, indel_rate=0.02)
+        n = int(tl[t])
+        L = min(h.size, n)
+        s = int(hr.below(1, n - L + 1)[0])
+        u = int(hr.below(1, h.size - L + 1)[0])
+        arena[int(offs[t]) + s:int(offs[t]) + s + L] = h[u:u + L]
+    return SearchWorkload("config5-search", queries, [seq_rows(model, q) for q in queries], arena, offs,
+                          info={"queries": n_queries, "targets": n_targets, "db_residues": total,
+                                "homologs_per_query": homologs_per_query, "seed": seed})
