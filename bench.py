@@ -609,6 +609,8 @@ def search_measure(ctx, args):
     same_scores = bool(same and np.array_equal(cpu_scores, gpu_s))
     ctx.free_profiles(ids)
     nq = len(ids)
+    serving = search_serving(ctx, w, params, gaps, rates=(100, 500, 1000, 2000, 3000), seconds=args.serving_seconds,
+                             seed=args.seed, batched_qps=nq / (t_pre + t_sw))
     return {"workload": f"config 5 searches: {nq} sequence queries against {len(tlen)} targets ({n_res / 1e6:.0f} M "
                         f"residues), 5 planted homologs per query; seed 111001101, k-mer score 22, cap 512, exact "
                         f"seeds, gate {gate} (size-adjusted 42), gaps 11/1",
@@ -627,7 +629,49 @@ def search_measure(ctx, args):
                              "sample": f"{k} queries on the whole database: the restated seed stage (best-first "
                                        "similar k-mers, direct-table index), evidence and gate, then the reference's "
                                        "AVX2 striped SW over their candidates, all host threads"},
+            "serving": serving,
             "setup_s": round(t_gen, 1)}
+
+
+def search_serving(ctx, w, params, gaps, rates, seconds, seed, batched_qps):
+    """Config 5 serving: Poisson arrivals of bare queries into a SearchServer (whole searches per batch on the
+    device); latency from submit to completion as the server stamps it.  Then every query at once (the
+    saturated rate) against the batched figure."""
+    from sabertooth_b200 import SearchServer
+    srv = SearchServer(ctx, params, gaps)
+    rng = np.random.default_rng(seed)
+    nq = len(w.rows)
+    try:
+        warm = [srv.submit(w.rows[q], w.queries[q]) for q in range(min(32, nq))]
+        for r in warm:
+            srv.wait(r)
+        sweep = []
+        for rate in rates:
+            n = max(1, int(rate * seconds))
+            t_arr = np.cumsum(rng.exponential(1.0 / rate, n))
+            rids = []
+            t0 = time.perf_counter()
+            for k in range(n):
+                delay = t_arr[k] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                q = k % nq
+                rids.append(srv.submit(w.rows[q], w.queries[q]))
+            lats = np.array([srv.wait(r)[2] for r in rids])
+            t_end = time.perf_counter() - t0
+            sweep.append({"rate_qps": rate, "queries": n, "p50_ms": round(float(np.percentile(lats, 50)), 2),
+                          "p99_ms": round(float(np.percentile(lats, 99)), 2), "achieved_qps": round(n / t_end, 1)})
+        b0 = srv.stats()["batches"]
+        t0 = time.perf_counter()
+        rids = [srv.submit(w.rows[q], w.queries[q]) for q in range(nq)]
+        lats = np.array([srv.wait(r)[2] for r in rids])
+        t_sat = time.perf_counter() - t0
+        sat = {"queries": nq, "batches": srv.stats()["batches"] - b0, "qps": round(nq / t_sat, 1),
+               "of_batched": round(nq / t_sat / batched_qps, 3), "p50_ms": round(float(np.percentile(lats, 50)), 1),
+               "p99_ms": round(float(np.percentile(lats, 99)), 1)}
+    finally:
+        srv.close()
+    return {"sweep": sweep, "saturated": sat}
 
 
 def calibration_measure(ctx, args, w, ids, gaps):

@@ -326,6 +326,30 @@ int st_prefilter_queries(st_ctx* ctx, const uint32_t* profiles, uint32_t n_queri
                          const st_prefilter_params* params, st_candidate* out, uint64_t cap, uint64_t* n_out,
                          st_prefilter_stats* stats, st_seed_stats* seed_stats);
 
+/* ---- search serving ------------------------------------------------------------
+ * (No reference counterpart: the reference runs a search's queries in one rayon
+ * pass.)  A search server owns a worker thread on one context whose database
+ * has a seed index.  A request is one bare query — its int32 [m][21] rows and,
+ * for sequence queries (sequence_queries = 1), its m residue codes.  The worker
+ * takes every request that has arrived (up to max_batch_queries, 0 = 4,096)
+ * as one batch and runs the whole search for it: st_prefilter_queries, then
+ * the exact SW score of every candidate (gaps from params); requests that
+ * arrive meanwhile form the next batch.  Results equal those of the query
+ * searched alone.  wait returns the request's candidates (query field 0,
+ * ranked as by st_prefilter_queries) with their SW scores and its latency from
+ * submit to completion in milliseconds; with cap below the count it only sets
+ * *n_out and the request can be waited for again. */
+typedef struct st_search_server st_search_server;
+st_search_server* st_search_server_create(st_ctx* ctx, const st_seed_params* seed_params,
+                                          const st_prefilter_params* params, int sequence_queries,
+                                          uint32_t max_batch_queries);
+int st_search_server_submit(st_search_server* s, const int32_t* rows, uint32_t m, const uint8_t* residues,
+                            uint64_t* request_id);
+int st_search_server_wait(st_search_server* s, uint64_t request_id, st_candidate* candidates, int32_t* scores,
+                          uint64_t cap, uint64_t* n_out, double* latency_ms);
+int st_search_server_stats(st_search_server* s, uint64_t* batches, uint64_t* queries);
+void st_search_server_destroy(st_search_server* s);
+
 /* ---- per-profile calibration ----------------------------------------------
  * calibrate_profile (src/evalue.rs:714-748) for many profiles at once: sample i
  * (0 <= i < samples) is a background target drawn from the SplitMix64 stream

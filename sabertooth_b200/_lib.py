@@ -117,6 +117,11 @@ SIGNATURES = {
     "st_prefilter_gate_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P]),
     "st_calibrate_profiles": (C.c_int, [_P, _P, _u32, _P, _u32, _u32, _u64, _P, _i32, _i32, _P, _P]),
     "st_seed_index_build": (C.c_int, [_P, C.c_char_p]),
+    "st_search_server_create": (_P, [_P, _P, _P, C.c_int, _u32]),
+    "st_search_server_submit": (C.c_int, [_P, _P, _u32, _P, _P]),
+    "st_search_server_wait": (C.c_int, [_P, _u64, _P, _P, _u64, _P, _P]),
+    "st_search_server_stats": (C.c_int, [_P, _P, _P]),
+    "st_search_server_destroy": (None, [_P]),
     "st_seed_hits": (C.c_int, [_P, _P, _u32, _P, _P, _P, _P, _u64, _P, _P]),
     "st_prefilter_queries": (C.c_int, [_P, _P, _u32, _P, _P, _P, _P, _P, _u64, _P, _P, _P]),
     "st_tune_num_classes": (C.c_int, []),

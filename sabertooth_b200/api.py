@@ -537,6 +537,59 @@ class Server:
             pass
 
 
+class SearchServer:
+    """Whole searches as a service (st_search_server_*): submit(rows, residues) returns a request
+    id at once; wait(id) returns (candidates, SW scores, latency_ms). One worker thread runs the
+    requests that have arrived as one batch: seeds -> evidence -> gate -> SW on the device."""
+
+    def __init__(self, ctx: Context, params: "PrefilterParams" = None, gaps: GapCosts = None, sequence_queries=True,
+                 max_batch_queries=0):
+        params = params or PrefilterParams.sequence_default()
+        gaps = gaps or GapCosts.sequence_default()
+        self._ctx = ctx
+        self._sp = params.seed_c()
+        self._gp = params.to_c(gaps)
+        self._h = lib.st_search_server_create(ctx.handle, C.byref(self._sp), C.byref(self._gp),
+                                              1 if sequence_queries else 0, int(max_batch_queries))
+        if not self._h:
+            check(-1)
+
+    def submit(self, rows, residues=None):
+        rows = np.ascontiguousarray(rows, dtype=np.int32).reshape(-1, 21)
+        res = None if residues is None else np.ascontiguousarray(residues, dtype=np.uint8)
+        rid = C.c_uint64()
+        check(lib.st_search_server_submit(self._h, ptr(rows), rows.shape[0], ptr(res), C.byref(rid)))
+        return rid.value
+
+    def wait(self, rid):
+        n = C.c_uint64()
+        lat = C.c_double()
+        cap = 4096
+        while True:
+            out = np.zeros(cap, dtype=CANDIDATE_DTYPE)
+            sc = np.zeros(cap, dtype=np.int32)
+            check(lib.st_search_server_wait(self._h, int(rid), ptr(out), ptr(sc), cap, C.byref(n), C.byref(lat)))
+            if n.value <= cap:
+                return out[:n.value].copy(), sc[:n.value].copy(), lat.value
+            cap = int(n.value)
+
+    def stats(self):
+        b, q = C.c_uint64(), C.c_uint64()
+        check(lib.st_search_server_stats(self._h, C.byref(b), C.byref(q)))
+        return {"batches": b.value, "queries": q.value}
+
+    def close(self):
+        if self._h:
+            lib.st_search_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Plan:
     """A captured batch over device buffers (d_scores / d_kernels: device pointers as ints)."""
 

@@ -351,3 +351,220 @@ extern "C" void st_server_destroy(st_server* s) {
   if (s->arena) cudaFreeHost(s->arena);
   delete s;
 }
+
+// ---------------------------------------------------------------------------
+// Search serving: requests are bare queries; each batch runs the whole search
+// (profiles, seeds -> evidence -> chains -> gate on the device, then SW over
+// every candidate).  One batch at a time (the prefilter's sizing reads share
+// the context's stream with the scoring); requests that arrive during a batch
+// form the next one.  A request's candidates and scores equal those of the
+// query searched alone: every candidate depends only on its own query's hits.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SearchRequest {
+  uint64_t id = 0;
+  uint32_t m = 0;
+  std::vector<int32_t> rows;
+  std::vector<uint8_t> residues;  // empty: a profile query
+  std::vector<st_candidate> cands;
+  std::vector<int32_t> scores;
+  Clock::time_point t_submit, t_done;
+  bool done = false;
+  int status = ST_OK;
+  std::string error;
+};
+
+}  // namespace
+
+struct st_search_server {
+  st_ctx* ctx = nullptr;
+  st_seed_params sp{};
+  st_prefilter_params gp{};
+  uint32_t max_queries = 0;
+  bool sequence = true;  // queries carry residues
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::shared_ptr<SearchRequest>> pending;
+  std::unordered_map<uint64_t, std::shared_ptr<SearchRequest>> live;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  uint64_t batches = 0, queries = 0;
+  void run();
+  int search(std::vector<std::shared_ptr<SearchRequest>>& b);
+};
+
+int st_search_server::search(std::vector<std::shared_ptr<SearchRequest>>& b) {
+  const size_t n = b.size();
+  std::vector<uint64_t> offs(n + 1, 0);
+  for (size_t i = 0; i < n; ++i) offs[i + 1] = offs[i] + b[i]->m;
+  std::vector<int32_t> rows(std::max<uint64_t>(offs[n], 1) * 21);
+  std::vector<uint8_t> res(sequence ? std::max<uint64_t>(offs[n], 1) : 0);
+  for (size_t i = 0; i < n; ++i) {
+    if (b[i]->m) memcpy(rows.data() + offs[i] * 21, b[i]->rows.data(), b[i]->rows.size() * 4);
+    if (sequence && b[i]->m) memcpy(res.data() + offs[i], b[i]->residues.data(), b[i]->m);
+  }
+  std::vector<uint32_t> ids(n);
+  int rc = st_profiles_create(ctx, rows.data(), offs.data(), static_cast<uint32_t>(n), ids.data());
+  if (rc != ST_OK) return rc;
+  std::unordered_map<uint32_t, uint32_t> at;  // profile id -> request
+  for (size_t i = 0; i < n; ++i) at[ids[i]] = static_cast<uint32_t>(i);
+  // room for 1,024 candidates per query; a batch with more runs again with the exact room
+  std::vector<st_candidate> cands(std::max<size_t>(n * 1024, 65536));
+  uint64_t nc = 0;
+  rc = st_prefilter_queries(ctx, ids.data(), static_cast<uint32_t>(n), sequence ? res.data() : nullptr,
+                            sequence ? offs.data() : nullptr, &sp, &gp, cands.data(), cands.size(), &nc, nullptr,
+                            nullptr);
+  if (rc == ST_OK && nc > cands.size()) {
+    cands.resize(nc);
+    rc = st_prefilter_queries(ctx, ids.data(), static_cast<uint32_t>(n), sequence ? res.data() : nullptr,
+                              sequence ? offs.data() : nullptr, &sp, &gp, cands.data(), nc, &nc, nullptr, nullptr);
+  }
+  cands.resize(rc == ST_OK ? nc : 0);
+  std::vector<int32_t> scores(cands.size());
+  if (rc == ST_OK && !cands.empty()) {
+    std::vector<st_pair> pairs(cands.size());
+    for (size_t k = 0; k < cands.size(); ++k) pairs[k] = st_pair{cands[k].query, cands[k].target, 0, -1};
+    rc = st_sw_score_pairs(ctx, pairs.data(), pairs.size(), gp.gap_open, gp.gap_ext, scores.data(), nullptr);
+  }
+  st_profiles_free(ctx, ids.data(), static_cast<uint32_t>(n));
+  if (rc != ST_OK) return rc;
+  for (auto& r : b) {
+    r->cands.clear();
+    r->scores.clear();
+  }
+  for (size_t k = 0; k < cands.size(); ++k) {
+    auto& r = b[at[cands[k].query]];
+    st_candidate c = cands[k];
+    c.query = 0;
+    r->cands.push_back(c);
+    r->scores.push_back(scores[k]);
+  }
+  return ST_OK;
+}
+
+void st_search_server::run() {
+  for (;;) {
+    std::vector<std::shared_ptr<SearchRequest>> b;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv_work.wait(lk, [&] { return stop || !pending.empty(); });
+      if (stop && pending.empty()) return;
+      while (!pending.empty() && b.size() < max_queries) {
+        b.push_back(pending.front());
+        pending.pop_front();
+      }
+    }
+    const int rc = search(b);
+    const std::string err = rc == ST_OK ? std::string() : std::string(st_last_error());
+    const Clock::time_point now = Clock::now();
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& r : b) {
+      r->status = rc;
+      r->error = err;
+      r->t_done = now;
+      r->done = true;
+    }
+    ++batches;
+    queries += b.size();
+    cv_done.notify_all();
+  }
+}
+
+extern "C" st_search_server* st_search_server_create(st_ctx* ctx, const st_seed_params* seed_params,
+                                                     const st_prefilter_params* params, int sequence_queries,
+                                                     uint32_t max_batch_queries) {
+  if (!ctx || !seed_params || !params) {
+    st_internal_set_error("st_search_server_create: null argument");
+    return nullptr;
+  }
+  auto s = std::make_unique<st_search_server>();
+  s->ctx = ctx;
+  s->sp = *seed_params;
+  s->gp = *params;
+  s->sequence = sequence_queries != 0;
+  s->max_queries = max_batch_queries ? max_batch_queries : 4096;
+  st_search_server* p = s.get();
+  s->worker = std::thread([p] { p->run(); });
+  return s.release();
+}
+
+extern "C" int st_search_server_submit(st_search_server* s, const int32_t* rows, uint32_t m, const uint8_t* residues,
+                                       uint64_t* request_id) {
+  if (!s || !request_id || (m && !rows) || (s->sequence && m && !residues)) {
+    st_internal_set_error("st_search_server_submit: null argument");
+    return ST_EINVAL;
+  }
+  auto r = std::make_shared<SearchRequest>();
+  r->m = m;
+  r->rows.assign(rows, rows + static_cast<size_t>(m) * 21);
+  if (s->sequence) r->residues.assign(residues, residues + m);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) {
+    st_internal_set_error("st_search_server_submit: server is stopping");
+    return ST_ESTATE;
+  }
+  r->id = s->next_id++;
+  r->t_submit = Clock::now();
+  s->live[r->id] = r;
+  s->pending.push_back(r);
+  *request_id = r->id;
+  s->cv_work.notify_one();
+  return ST_OK;
+}
+
+extern "C" int st_search_server_wait(st_search_server* s, uint64_t request_id, st_candidate* cands, int32_t* scores,
+                                     uint64_t cap, uint64_t* n_out, double* latency_ms) {
+  if (!s || !n_out) {
+    st_internal_set_error("st_search_server_wait: null argument");
+    return ST_EINVAL;
+  }
+  std::shared_ptr<SearchRequest> r;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->live.find(request_id);
+    if (it == s->live.end()) {
+      st_internal_set_error("st_search_server_wait: unknown request id");
+      return ST_EINVAL;
+    }
+    r = it->second;
+    s->cv_done.wait(lk, [&] { return r->done; });
+  }
+  if (r->status != ST_OK) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->live.erase(request_id);
+    st_internal_set_error(r->error.c_str());
+    return r->status;
+  }
+  *n_out = r->cands.size();
+  if (cap < r->cands.size()) return ST_OK;  // call again with room for *n_out (the request stays)
+  if (cands) memcpy(cands, r->cands.data(), r->cands.size() * sizeof(st_candidate));
+  if (scores) memcpy(scores, r->scores.data(), r->scores.size() * 4);
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->live.erase(request_id);
+  return ST_OK;
+}
+
+extern "C" int st_search_server_stats(st_search_server* s, uint64_t* batches, uint64_t* queries) {
+  if (!s) {
+    st_internal_set_error("st_search_server_stats: null server");
+    return ST_EINVAL;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (batches) *batches = s->batches;
+  if (queries) *queries = s->queries;
+  return ST_OK;
+}
+
+extern "C" void st_search_server_destroy(st_search_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  delete s;
+}
