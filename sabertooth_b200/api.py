@@ -331,7 +331,7 @@ class Context:
         n = C.c_uint64()
         args = (self._h, ptr(ids), len(ids), ptr(res) if res is not None else None,
                 ptr(offs) if offs is not None else None, C.byref(sp), C.byref(gp))
-        cap = 1 << 16
+        cap = max(1 << 16, 1024 * len(ids))  # a batch with more candidates runs again with the exact room
         while True:
             out = np.zeros(cap, dtype=CANDIDATE_DTYPE)
             check(lib.st_prefilter_queries(*args, ptr(out), cap, C.byref(n), C.byref(st), C.byref(sst)))

@@ -91,6 +91,7 @@ struct GateConf {
   uint32_t dbits;
   uint32_t doff;
   uint32_t n_prof;  // query ids are < n_prof; n_prof marks rejected hits
+  uint32_t stride;  // staged profile row stride: >= every hit query's length rounded to 16, + 32
 };
 
 __device__ __forceinline__ uint32_t gate_key_query(uint64_t k, const GateConf& g) {

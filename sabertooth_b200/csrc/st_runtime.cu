@@ -2873,7 +2873,8 @@ static int gate_conf(st_ctx* c, const st_prefilter_params* p, GateConf& g, int& 
   if (qbits + static_cast<int>(g.tbits + g.dbits) > 64 || qbits > 32)
     return fail(ST_EINVAL, "seed-hit key needs %d bits (query %d, target %u, diagonal %u); at most 64",
                 qbits + static_cast<int>(g.tbits + g.dbits), qbits, g.tbits, g.dbits);
-  if (16 + static_cast<size_t>(kProfRows) * ung_stride(c) + 16 > static_cast<size_t>(g_gate_smem))
+  g.stride = ung_stride(c);
+  if (16 + static_cast<size_t>(kProfRows) * g.stride + 16 > static_cast<size_t>(g_gate_smem))
     return fail(ST_EINVAL, "query too long for the prefilter segment kernel (%u rows)", c->max_m);
   return ST_OK;
 }
@@ -2984,7 +2985,7 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   else
     gate_emit_kernel<kGateMaxDiags><<<grid_for(n, 128), 128, 0, s>>>(G, g, db, pv.qlen, ns, joff, jobs);
   // window scores
-  GateSegParams sp{db, pv, jobs, ng, joff, sc, ung_stride(c)};
+  GateSegParams sp{db, pv, jobs, ng, joff, sc, g.stride};
   const size_t smem = 16 + static_cast<size_t>(kProfRows) * sp.max_m_pad + 16;
   gate_score_kernel<<<static_cast<uint32_t>((static_cast<uint64_t>(n) + kGateChunk - 1) / kGateChunk), 256, smem, s>>>(
       sp);
@@ -3346,24 +3347,48 @@ extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_
   GateConf g;
   int qbits = 0;
   ST_TRY(gate_conf(c, &gp, g, qbits));
-  for (uint32_t i = 0; i < n_queries; ++i) ST_TRY(check_profile(c, profiles[i]));
+  for (uint32_t i = 0; i < n_queries; ++i) {
+    ST_TRY(check_profile(c, profiles[i]));
+    if (residues && (residue_offsets[i + 1] < residue_offsets[i] ||
+                     residue_offsets[i + 1] - residue_offsets[i] != c->profs[profiles[i]].m))
+      return fail(ST_EINVAL, "query %u: residue count differs from its profile's rows", i);
+  }
   GateStats tot{};
   st_seed_stats stot{};
   std::vector<st_candidate> all;
+  // queries in order of length, so that a chunk's staged profile rows (sized by its longest query) stay short
+  std::vector<uint32_t> order(n_queries);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    return c->profs[profiles[a]].m < c->profs[profiles[b]].m;
+  });
   uint32_t q0 = 0;
   while (q0 < n_queries) {
     uint32_t q1 = q0;
     uint64_t wins = 0;
+    uint32_t max_m = 0;
+    std::vector<uint32_t> cp;
+    std::vector<uint8_t> cres;
+    std::vector<uint64_t> coff(1, 0);
     do {
-      const uint64_t m = c->profs[profiles[q1]].m;
+      const uint32_t qi = order[q1];
+      const uint64_t m = c->profs[profiles[qi]].m;
       wins += m >= c->seed_pat.span ? m - c->seed_pat.span + 1 : 0;
+      max_m = std::max<uint32_t>(max_m, static_cast<uint32_t>(m));
+      cp.push_back(profiles[qi]);
+      if (residues) {
+        cres.insert(cres.end(), residues + residue_offsets[qi], residues + residue_offsets[qi + 1]);
+        coff.push_back(cres.size());
+      }
       ++q1;
     } while (q1 < n_queries && wins < kSearchChunkWindows);
+    GateConf gc = g;
+    gc.stride = static_cast<uint32_t>(up16(max_m) + 32);
     DevMem hits;
     uint32_t nh = 0;
     st_seed_stats sst{};
-    ST_TRY(seed_stage(c, profiles + q0, q1 - q0, residues, residues ? residue_offsets + q0 : nullptr, seed_params,
-                      hits, &nh, &sst));
+    ST_TRY(seed_stage(c, cp.data(), q1 - q0, residues ? cres.data() : nullptr, residues ? coff.data() : nullptr,
+                      seed_params, hits, &nh, &sst));
     stot.windows += sst.windows;
     stot.windows_skipped += sst.windows_skipped;
     stot.kmers_generated += sst.kmers_generated;
@@ -3378,7 +3403,7 @@ extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_
       ST_TRY(pool_get(c, static_cast<size_t>(nh) * sizeof(GateCandidate), cm));
       GateStats st{};
       uint64_t nc = 0;
-      ST_TRY(gate_pipeline(c, hits.as<GateSeedHit>(), nh, g, qbits, cm.as<GateCandidate>(), &nc, &st));
+      ST_TRY(gate_pipeline(c, hits.as<GateSeedHit>(), nh, gc, qbits, cm.as<GateCandidate>(), &nc, &st));
       const size_t at = all.size();
       all.resize(at + nc);
       if (nc) ST_CUDA(cudaMemcpyAsync(all.data() + at, cm.p, nc * sizeof(st_candidate), cudaMemcpyDeviceToHost,

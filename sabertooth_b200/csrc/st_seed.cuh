@@ -345,21 +345,52 @@ __global__ void __launch_bounds__(256) seed_post_count_kernel(const SeedSeed* se
   gate_flush(&st->postings_skipped_occ, n_skip);
 }
 
+// One hit per posting.  A warp takes 32 consecutive seeds, whose hits are one
+// contiguous range of the output; lane k writes output positions k, k + 32, ...
+// and finds the seed of each by a binary search over the 32 seeds' offsets held
+// in the lanes, so reads of the postings and writes of the hits are coalesced
+// whatever the list lengths.
 __global__ void __launch_bounds__(256) seed_hits_kernel(SeedQ Q, const SeedSeed* seeds, uint32_t n_seeds,
                                                         const uint32_t* cnt, const uint32_t* hoff, const uint32_t* off,
                                                         const SeedPost* post, GateSeedHit* hits) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_seeds; i += gridDim.x * blockDim.x) {
-    const uint32_t len = cnt[i];
-    if (!len) continue;
-    const SeedSeed sd = seeds[i];
-    uint32_t qi, start;
-    seed_window_of(Q, sd.window, qi, start);
-    const uint32_t q = Q.qids[qi];
-    const SeedPost* p = post + off[sd.code];
-    GateSeedHit* h = hits + hoff[i];
-    for (uint32_t e = 0; e < len; ++e) {
-      const SeedPost ps = p[e];
-      h[e] = GateSeedHit{q, ps.target, static_cast<int32_t>(ps.tpos) - static_cast<int32_t>(start), start};
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n_groups = (n_seeds + 31) / 32;
+  for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / 32; g < n_groups; g += (gridDim.x * blockDim.x) / 32) {
+    const uint32_t s = g * 32 + lane;
+    // this lane's seed: first output position, posting start, query and position
+    uint32_t o = 0, pstart = 0, q = 0, start = 0;
+    if (s < n_seeds) {
+      o = hoff[s];
+      if (cnt[s]) {
+        const SeedSeed sd = seeds[s];
+        uint32_t qi;
+        seed_window_of(Q, sd.window, qi, start);
+        q = Q.qids[qi];
+        pstart = off[sd.code];
+      }
+    }
+    const uint32_t last = min(n_seeds, g * 32 + 32);
+    const uint32_t o_begin = __shfl_sync(0xFFFFFFFFu, o, 0);
+    const uint32_t o_end = hoff[last];
+    for (uint32_t base = o_begin; base < o_end; base += 32) {  // every lane runs every round (shuffles)
+      const uint32_t k = base + lane;
+      const bool live = k < o_end;
+      // last lane j with offset <= k (lanes past the group's seeds are never chosen)
+      uint32_t j = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t cand = j + step;
+        const uint32_t oc = __shfl_sync(0xFFFFFFFFu, o, cand & 31);
+        if (cand < last - g * 32 && oc <= k) j = cand;
+      }
+      const uint32_t oj = __shfl_sync(0xFFFFFFFFu, o, j);
+      const uint32_t pj = __shfl_sync(0xFFFFFFFFu, pstart, j);
+      const uint32_t qj = __shfl_sync(0xFFFFFFFFu, q, j);
+      const uint32_t sj = __shfl_sync(0xFFFFFFFFu, start, j);
+      if (live) {
+        const SeedPost ps = post[pj + (k - oj)];
+        hits[k] = GateSeedHit{qj, ps.target, static_cast<int32_t>(ps.tpos) - static_cast<int32_t>(sj), sj};
+      }
     }
   }
 }
