@@ -333,7 +333,7 @@ class Context:
                 ptr(offs) if offs is not None else None, C.byref(sp), C.byref(gp))
         cap = max(1 << 16, 1024 * len(ids))  # a batch with more candidates runs again with the exact room
         while True:
-            out = np.zeros(cap, dtype=CANDIDATE_DTYPE)
+            out = np.empty(cap, dtype=CANDIDATE_DTYPE)
             check(lib.st_prefilter_queries(*args, ptr(out), cap, C.byref(n), C.byref(st), C.byref(sst)))
             if n.value <= cap:
                 break

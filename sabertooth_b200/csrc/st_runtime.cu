@@ -3421,13 +3421,23 @@ extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_
     pool_put(c, std::move(hits));
     q0 = q1;
   }
-  // chunks are ranked by query id inside themselves; order the whole list by query id
-  std::stable_sort(all.begin(), all.end(),
-                   [](const st_candidate& x, const st_candidate& y) { return x.query < y.query; });
+  // chunks are ranked by query id inside themselves; a counting sort by query id (stable) orders the whole
+  // list, straight into the caller's buffer
   if (seed_stats) *seed_stats = stot;
   *n_out = all.size();
-  const uint64_t k = std::min<uint64_t>(cap, all.size());
-  if (k) memcpy(out, all.data(), k * sizeof(st_candidate));
+  if (cap && !all.empty()) {
+    std::vector<st_candidate> tmp;
+    st_candidate* dst = out;
+    if (cap < all.size()) {  // only the first cap are wanted
+      tmp.resize(all.size());
+      dst = tmp.data();
+    }
+    std::vector<uint64_t> at(c->profs.size() + 1, 0);
+    for (const st_candidate& x : all) ++at[x.query + 1];
+    for (size_t i = 1; i < at.size(); ++i) at[i] += at[i - 1];
+    for (const st_candidate& x : all) dst[at[x.query]++] = x;
+    if (dst != out) memcpy(out, dst, cap * sizeof(st_candidate));
+  }
   return gate_result(tot, stats);
 }
 
