@@ -495,6 +495,10 @@ static int set_smem_limits(int device) {
   g_ung_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(std::max(fa_t.sharedSizeBytes, fa_f.sharedSizeBytes)));
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
   ST_CUDA(cudaFuncSetAttribute(ungapped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
+  cudaFuncAttributes fa_r;
+  ST_CUDA(cudaFuncGetAttributes(&fa_r, reinterpret_cast<const void*>(ungapped_hits_refill_kernel)));
+  g_ung_smem = std::min<int>(g_ung_smem, optin - static_cast<int>(fa_r.sharedSizeBytes));
+  ST_CUDA(cudaFuncSetAttribute(ungapped_hits_refill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
   cudaFuncAttributes fa_g;
   ST_CUDA(cudaFuncGetAttributes(&fa_g, reinterpret_cast<const void*>(gate_score_kernel)));
   g_gate_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(fa_g.sharedSizeBytes));
@@ -2640,7 +2644,7 @@ static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n,
   const uint64_t grid = (n + kUngChunk - 1) / kUngChunk;
   if (grid > 0x7FFFFFFFull) return fail(ST_EINVAL, "too many ungapped jobs");
   if (hits)
-    ungapped_kernel<true><<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
+    ungapped_hits_refill_kernel<<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
   else
     ungapped_kernel<false><<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
   ++c->launches;

@@ -183,4 +183,121 @@ __global__ void __launch_bounds__(256) ungapped_kernel(const UngappedParams prm)
   }
 }
 
+// Hits (whole-diagonal windows, diag_range) with one hit per lane: per run of
+// one query inside the CTA's chunk the profile is staged as above, then every
+// lane keeps a hit in flight, one 16-byte target vector per step, and takes the
+// run's next hit from a shared counter as soon as its own is done, so lanes
+// stay busy whatever the diagonal lengths.  On int8 profiles no cell needs a
+// test (the argument of the whole-diagonal path of ungapped_kernel); rows
+// outside int8 read the int32 profile with an explicit window test.
+__global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const UngappedParams prm) {
+  extern __shared__ __align__(16) int8_t smem[];
+  __shared__ unsigned long long s_run_end, s_next;
+  const HitRec* hits = reinterpret_cast<const HitRec*>(prm.jobs);
+  const uint32_t stride = prm.max_m_pad;
+  int8_t* base = smem + 16;
+  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kUngChunk;
+  if (c0 >= prm.n) return;
+  const uint64_t c1 = u64min(prm.n, c0 + kUngChunk);
+  uint64_t a = c0;
+  while (a < c1) {
+    const uint32_t q = hits[a].query;
+    if (threadIdx.x < 32) {
+      uint64_t e = a;
+      for (;;) {
+        const uint64_t k = e + threadIdx.x;
+        const bool same = (k < c1) && (hits[k].query == q);
+        const uint32_t ball = __ballot_sync(0xFFFFFFFFu, same);
+        if (ball != 0xFFFFFFFFu) {
+          e += __ffs(~ball) - 1;
+          break;
+        }
+        e += 32;
+      }
+      if (threadIdx.x == 0) {
+        s_run_end = e;
+        s_next = a + blockDim.x;
+      }
+    }
+    const uint32_t m = prm.prof.qlen[q];
+    const uint32_t pstride = prm.prof.stride8[q];
+    const int8_t* src = prm.prof.p8[q];
+    for (uint32_t idx = threadIdx.x; idx < kProfRows * (stride / 16); idx += blockDim.x) {
+      const uint32_t r = idx / (stride / 16);
+      const uint32_t i = (idx - r * (stride / 16)) * 16;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (i < pstride) v = *reinterpret_cast<const uint4*>(src + static_cast<size_t>(r) * pstride + i);
+      *reinterpret_cast<uint4*>(base + static_cast<size_t>(r) * stride + i) = v;
+    }
+    if (threadIdx.x < 16) smem[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t b = s_run_end;
+    const bool narrow = prm.prof.fits8[q] != 0;
+    const int32_t* p32 = prm.prof.p32[q];
+    const int32_t s32 = static_cast<int32_t>(prm.prof.stride32[q]);
+    const int32_t last_row = static_cast<int32_t>(m) - 1;
+    uint64_t k = a + threadIdx.x;
+    const uint8_t* tp = nullptr;
+    int32_t d = 0, p0 = 0, p1 = 0, pa = 0, cur = 0, best = 0;
+    bool live = false;
+    auto take = [&](uint64_t j) {
+      k = j;
+      live = j < b;
+      if (live) {
+        const HitRec h = hits[j];
+        const int64_t n = prm.db.length[h.target];
+        d = h.diag;
+        // diag_range, src/ungapped.rs:38-46
+        const int64_t lo = i64max(-static_cast<int64_t>(d), 0), hi = i64min(m, n - d);
+        tp = prm.db.arena + prm.db.offset[h.target];
+        if (hi > lo) {
+          p0 = static_cast<int32_t>(lo) + d;
+          p1 = static_cast<int32_t>(hi) + d;
+          pa = p0 & ~15;
+        } else {
+          p0 = p1 = pa = 0;  // empty: done at once
+        }
+        cur = 0;
+        best = 0;
+      }
+    };
+    take(k);
+    while (__any_sync(0xFFFFFFFFu, live)) {
+      if (live) {
+        if (pa < p1) {
+          const uint4 v = *reinterpret_cast<const uint4*>(tp + pa);
+          const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+          const int32_t qa = pa - d;
+          if (narrow) {
+            const int8_t* rowbase = base + qa;
+#pragma unroll
+            for (int bb = 0; bb < 16; ++bb) {
+              const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+              cur = wadd(max(cur, 0), static_cast<int32_t>(rowbase[static_cast<int32_t>(r * stride) + bb]));
+              best = max(best, cur);
+            }
+          } else {
+#pragma unroll
+            for (int bb = 0; bb < 16; ++bb) {
+              const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+              const int32_t p = pa + bb;
+              const int32_t row = min(max(qa + bb, 0), last_row);
+              const int32_t sc = (p >= p0 && p < p1) ? __ldg(p32 + static_cast<int32_t>(r) * s32 + row) : 0;
+              cur = wadd(max(cur, 0), sc);
+              best = max(best, cur);
+            }
+          }
+          pa += 16;
+        }
+        if (pa >= p1) {
+          prm.out[k] = best;
+          take(atomicAdd(&s_next, 1ull));
+        }
+      }
+    }
+    __syncthreads();
+    a = b;
+  }
+}
+
 }  // namespace st
