@@ -356,7 +356,18 @@ static int pool_get(st_ctx* c, size_t bytes, DevMem& out) {
     c->pool.erase(c->pool.begin() + best);
     return ST_OK;
   }
-  return dev_alloc(&c->mt, out, bytes + bytes / 8);
+  // new arenas come in a few size classes (2^k times 1, 1.25, 1.5 or 1.75), so that later requests of a
+  // similar size find one to reuse instead of allocating (a large cudaMalloc or cudaFree costs milliseconds)
+  size_t cls = 1 << 20;
+  while (cls < bytes) cls <<= 1;
+  size_t q = cls / 8;  // quarter steps between cls / 2 and cls
+  size_t want = cls;
+  for (size_t k = 5; k <= 8; ++k)
+    if (q * k >= bytes) {
+      want = q * k;
+      break;
+    }
+  return dev_alloc(&c->mt, out, std::max(want, bytes));
 }
 
 static void pool_trim(st_ctx* c) {
@@ -2925,8 +2936,10 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
     t_max = std::max(t_max, t);
   }
   const size_t o_tmp = take(t_max);
+  TraceClock tc("gate");
   DevMem mem;
   ST_TRY(pool_get(c, o, mem));
+  tc.lap("scratch");
   struct Back {
     st_ctx* c;
     DevMem* m;
@@ -3007,9 +3020,11 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   ST_CUDA(cudaGetLastError());
   ST_TRY(c->pin.reserve(64));
   uint32_t* h_nc = c->pin.as<uint32_t>();
+  tc.lap("enqueue");
   ST_CUDA(cudaMemcpyAsync(h_nc, nc, 4, cudaMemcpyDeviceToHost, s));
   ST_CUDA(cudaStreamSynchronize(s));
   const uint32_t n_cand = *h_nc;
+  tc.lap("device");
   // ranking: the sort keys reuse the hit-key buffers (free after the jobs are emitted)
   if (n_cand) {
     gate_rank_keys_kernel<<<grid_for(n_cand, 256), 256, 0, s>>>(cand, sel, nc, k0, v0);
@@ -3038,6 +3053,7 @@ static int gate_pipeline(st_ctx* c, const GateSeedHit* d_hits, uint32_t n, const
   ST_CUDA(cudaStreamSynchronize(s));
   *h_stats = *h_st;
   *n_out = h_st->candidates;
+  tc.lap("rank (enqueue + device)");
   return ST_OK;
 }
 
@@ -3200,6 +3216,7 @@ static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const u
   stats->windows = nw;
   *n_hits = 0;
   if (nw == 0) return ST_OK;
+  TraceClock tc("seeds");
   ST_TRY(sync_profiles(c));
   cudaStream_t s = c->stream;
   // windows: sorted rows, counts, slots
@@ -3216,8 +3233,10 @@ static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const u
   const size_t o_res = take(residues ? nr : 0), o_rows = take(sizeof(SeedRow) * nr);
   const size_t o_slots = take(4 * (nw + 1)), o_soff = take(4 * (nw + 1)), o_win = take(sizeof(SeedWin) * nw);
   const size_t o_st = take(sizeof(SeedStatsDev)), o_tmp = take(t_scan);
+  tc.lap("windows (prep)");
   DevMem wm;
   ST_TRY(pool_get(c, o, wm));
+  tc.lap("windows (scratch)");
   struct Back {
     st_ctx* c;
     DevMem* m;
@@ -3228,6 +3247,7 @@ static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const u
   ST_CUDA(cudaMemcpyAsync(b + o_wo, woff.data(), 4ull * (n_q + 1), cudaMemcpyHostToDevice, s));
   ST_CUDA(cudaMemcpyAsync(b + o_r0, row0.data(), 4ull * (n_q + 1), cudaMemcpyHostToDevice, s));
   if (residues) ST_TRY(upload_host(c, b + o_res, residues + res_off[0], nr, s));
+  tc.lap("windows (uploads)");
   SeedStatsDev* st = reinterpret_cast<SeedStatsDev*>(b + o_st);
   ST_CUDA(cudaMemsetAsync(st, 0, sizeof(SeedStatsDev), s));
   SeedQ Q;
@@ -3256,9 +3276,11 @@ static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const u
   ST_CUDA(cudaGetLastError());
   ST_TRY(c->pin.reserve(64));
   uint32_t* h = c->pin.as<uint32_t>();
+  tc.lap("windows (enqueue)");
   ST_CUDA(cudaMemcpyAsync(h, soff + nw, 4, cudaMemcpyDeviceToHost, s));
   ST_CUDA(cudaStreamSynchronize(s));
   const uint64_t ns = *h;
+  tc.lap("windows (device)");
   // seeds: k-mers, posting counts, hit offsets
   size_t t_scan2 = 0;
   ST_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t_scan2, static_cast<uint32_t*>(nullptr),
@@ -3285,8 +3307,10 @@ static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const u
   SeedStatsDev* hst = reinterpret_cast<SeedStatsDev*>(c->pin.as<char>());
   uint32_t* h_hits = reinterpret_cast<uint32_t*>(c->pin.as<char>() + sizeof(SeedStatsDev));
   ST_CUDA(cudaMemcpyAsync(hst, st, sizeof(SeedStatsDev), cudaMemcpyDeviceToHost, s));
+  tc.lap("k-mers (enqueue)");
   ST_CUDA(cudaMemcpyAsync(h_hits, hoff + ns, 4, cudaMemcpyDeviceToHost, s));
   ST_CUDA(cudaStreamSynchronize(s));
+  tc.lap("k-mers (device)");
   const SeedStatsDev sd = *hst;
   const uint64_t nh = *h_hits;
   stats->windows_skipped = sd.windows_skipped;
@@ -3310,6 +3334,7 @@ static int seed_stage(st_ctx* c, const uint32_t* profiles, uint32_t n_q, const u
     ST_CUDA(cudaGetLastError());
   }
   *n_hits = static_cast<uint32_t>(nh);
+  tc.lap("hits (enqueue)");
   return ST_OK;
 }
 
@@ -3402,18 +3427,22 @@ extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_
     stot.postings_visited += sst.postings_visited;
     stot.seeds_over_occ_cap += sst.seeds_over_occ_cap;
     stot.postings_skipped_occ += sst.postings_skipped_occ;
+    TraceClock tc("search chunk");
     if (nh) {
       DevMem cm;
       ST_TRY(pool_get(c, static_cast<size_t>(nh) * sizeof(GateCandidate), cm));
+      tc.lap("candidate buffer");
       GateStats st{};
       uint64_t nc = 0;
       ST_TRY(gate_pipeline(c, hits.as<GateSeedHit>(), nh, gc, qbits, cm.as<GateCandidate>(), &nc, &st));
+      tc.lap("gate");
       const size_t at = all.size();
       all.resize(at + nc);
       if (nc) ST_CUDA(cudaMemcpyAsync(all.data() + at, cm.p, nc * sizeof(st_candidate), cudaMemcpyDeviceToHost,
                                       c->stream));
       ST_CUDA(cudaStreamSynchronize(c->stream));
       pool_put(c, std::move(cm));
+      tc.lap("candidates to host");
       tot.targets_hit += st.targets_hit;
       tot.targets_evaluated += st.targets_evaluated;
       tot.diagonals_scored += st.diagonals_scored;
