@@ -320,7 +320,8 @@ int st_seed_hits(st_ctx* ctx, const uint32_t* profiles, uint32_t n_queries, cons
 /* The whole prefilter of prefilter_query for a batch of queries on the device:
  * seed hits (as st_seed_hits) -> evidence, chains and gate -> ranked
  * candidates (as st_prefilter_gate; params->span is taken from the index's
- * pattern).  Host buffers; stats and seed_stats may be NULL. */
+ * pattern).  The profile ids of one call must be distinct.  Host buffers; stats
+ * and seed_stats may be NULL. */
 int st_prefilter_queries(st_ctx* ctx, const uint32_t* profiles, uint32_t n_queries, const uint8_t* residues,
                          const uint64_t* residue_offsets, const st_seed_params* seed_params,
                          const st_prefilter_params* params, st_candidate* out, uint64_t cap, uint64_t* n_out,

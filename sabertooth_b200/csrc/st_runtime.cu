@@ -3376,8 +3376,11 @@ extern "C" int st_prefilter_queries(st_ctx* c, const uint32_t* profiles, uint32_
   GateConf g;
   int qbits = 0;
   ST_TRY(gate_conf(c, &gp, g, qbits));
+  std::vector<uint8_t> seen(c->profs.size(), 0);
   for (uint32_t i = 0; i < n_queries; ++i) {
     ST_TRY(check_profile(c, profiles[i]));
+    if (seen[profiles[i]]++)  // the evidence stage groups hits by profile id
+      return fail(ST_EINVAL, "profile id %u appears twice in one call", profiles[i]);
     if (residues && (residue_offsets[i + 1] < residue_offsets[i] ||
                      residue_offsets[i + 1] - residue_offsets[i] != c->profs[profiles[i]].m))
       return fail(ST_EINVAL, "query %u: residue count differs from its profile's rows", i);

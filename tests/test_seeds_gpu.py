@@ -103,6 +103,8 @@ def test_errors(ctx):
             ctx.seed_hits(ids, params=PrefilterParams(max_kmers_per_pos=0))
         hits, st = ctx.seed_hits(ids, [encode("MKVLLACDEFGH")])
         assert len(hits) > 0 and st["windows"] == 12 - 6 + 1
+        with pytest.raises(StError):  # the same profile twice in one prefilter call
+            ctx.prefilter_queries(np.concatenate([ids, ids]), [encode("MKVLLACDEFGH")] * 2)
     finally:
         ctx.free_profiles(ids)
 
