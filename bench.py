@@ -438,15 +438,17 @@ def main():
             "step_ms_min_max": [round(min(step_ms), 3), round(max(step_ms), 3)],
         }
     plan.close()
-    if result is not None and args.calib_profiles > 0:
+    # the other rows are single-GPU measurements: taken on one GPU runs only (the other ranks would wait)
+    extra = result is not None and world == 1
+    if extra and args.calib_profiles > 0:
         result["calibration"] = calibration_measure(ctx, args, w, ids, gaps)
-    if result is not None and args.ungapped_hits > 0:
+    if extra and args.ungapped_hits > 0:
         result["ungapped"] = ungapped_measure(ctx, args)
-    if result is not None and args.gate_hits > 0:
+    if extra and args.gate_hits > 0:
         result["gate"] = gate_measure(ctx, args)
-    if result is not None and args.search_queries > 0:
+    if extra and args.search_queries > 0:
         result["search"] = search_measure(ctx, args)
-    if result is not None and args.serving_pairs > 0:
+    if extra and args.serving_pairs > 0:
         result["serving"] = serving_measure(ctx, args)
     if world > 1:
         torch.distributed.barrier()
