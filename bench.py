@@ -14,6 +14,12 @@ reference's gapped_cells) / step time.
 Under torchrun (N > 1) every rank scores its own instance of the workload
 (seed + rank): weak scaling with no collective on the data path; the step
 time is the max over ranks.  Rank 0 prints one JSON line.
+
+On one GPU the line also carries the other rows, each with its own CPU
+baseline and parity check: `calibration` (per-profile calibration of config-3
+PSSMs), `ungapped` (config 2, 2x10^7 hits), `gate` (evidence / chain / gate on
+2x10^7 seed hits), `search` (config 5 whole searches and their serving sweep)
+and `serving` (config-4 scoring requests).  Each has a flag to skip it.
 """
 import argparse
 import json
