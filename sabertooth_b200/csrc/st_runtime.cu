@@ -3630,8 +3630,50 @@ extern "C" int st_calibrate_profiles(st_ctx* c, const uint32_t* profiles, uint32
     for (uint32_t i = 0; i < samples; ++i) pairs.push_back(st_pair{profiles[p], i, 0, -1});
   }
   std::vector<int32_t> sc(pairs.size());
+  uint64_t lsum = 0;
+  for (uint32_t i = 0; i < n_lengths; ++i) lsum += lengths[i];
+  const double mean_len = static_cast<double>(lsum) / static_cast<double>(n_lengths);
+  // ML Gumbel fit per profile, K over the search space m * (N_t * mean length) (src/evalue.rs:739-747)
+  auto fit_rows = [&](size_t r0, size_t r1) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t r = static_cast<int64_t>(r0); r < static_cast<int64_t>(r1); ++r) {
+      std::vector<double> xs(samples);
+      for (uint32_t i = 0; i < samples; ++i) xs[i] = static_cast<double>(sc[static_cast<size_t>(r) * samples + i]);
+      double lambda = 0.0, mu = 0.0;
+      st_calibration& o = out[row[r]];
+      if (fit_gumbel_ml(xs, &lambda, &mu)) {
+        o.lambda = lambda;
+        o.mu = mu;
+        o.k = std::exp(lambda * (mu + 0.5)) / (static_cast<double>(m[row[r]]) * mean_len);
+        o.ok = 1;
+      }
+    }
+  };
+  // profiles in groups: group g + 1 is scored on the device while the host fits group g
+  const size_t n_rows = row.size();
+  const size_t per = std::max<size_t>(64, (n_rows + 3) / 4);
+  std::vector<size_t> gs;
+  for (size_t r = 0; r < n_rows; r += per) gs.push_back(r);
+  gs.push_back(n_rows);
+  const size_t ng = gs.size() - 1;
+  std::vector<st_batch*> handles(ng, nullptr);
+  auto launch = [&](size_t g) {
+    const size_t a = gs[g] * samples, b = gs[g + 1] * samples;
+    return st_sw_score_pairs_async(c, pairs.data() + a, b - a, open, ext, sc.data() + a, nullptr, &handles[g]);
+  };
   swap_db(c, cal);
-  const int rc = pairs.empty() ? ST_OK : st_sw_score_pairs(c, pairs.data(), pairs.size(), open, ext, sc.data(), nullptr);
+  int rc = ng ? launch(0) : ST_OK;
+  for (size_t g = 0; g < ng && rc == ST_OK; ++g) {
+    if (g + 1 < ng) {
+      rc = launch(g + 1);
+      if (rc != ST_OK) break;
+    }
+    rc = st_batch_wait(handles[g]);
+    handles[g] = nullptr;
+    if (rc == ST_OK) fit_rows(gs[g], gs[g + 1]);
+  }
+  for (st_batch* h : handles)  // after an error: the batches still in flight
+    if (h) st_batch_wait(h);
   swap_db(c, cal);
   ST_CUDA(cudaStreamSynchronize(c->stream));
   pool_put(c, std::move(st_dev));
@@ -3640,23 +3682,6 @@ extern "C" int st_calibrate_profiles(st_ctx* c, const uint32_t* profiles, uint32
     memset(scores, 0, static_cast<size_t>(n_profiles) * samples * 4);
     for (size_t r = 0; r < row.size(); ++r)
       memcpy(scores + static_cast<size_t>(row[r]) * samples, sc.data() + r * samples, static_cast<size_t>(samples) * 4);
-  }
-  // ML Gumbel fit per profile, K over the search space m * (N_t * mean length) (src/evalue.rs:739-747)
-  uint64_t lsum = 0;
-  for (uint32_t i = 0; i < n_lengths; ++i) lsum += lengths[i];
-  const double mean_len = static_cast<double>(lsum) / static_cast<double>(n_lengths);
-#pragma omp parallel for schedule(dynamic, 1)
-  for (int64_t r = 0; r < static_cast<int64_t>(row.size()); ++r) {
-    std::vector<double> xs(samples);
-    for (uint32_t i = 0; i < samples; ++i) xs[i] = static_cast<double>(sc[static_cast<size_t>(r) * samples + i]);
-    double lambda = 0.0, mu = 0.0;
-    st_calibration& o = out[row[r]];
-    if (fit_gumbel_ml(xs, &lambda, &mu)) {
-      o.lambda = lambda;
-      o.mu = mu;
-      o.k = std::exp(lambda * (mu + 0.5)) / (static_cast<double>(m[row[r]]) * mean_len);
-      o.ok = 1;
-    }
   }
   return ST_OK;
 }
