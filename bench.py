@@ -448,6 +448,8 @@ def main():
     extra = result is not None and world == 1
     if extra and args.calib_profiles > 0:
         result["calibration"] = calibration_measure(ctx, args, w, ids, gaps)
+    # the config-3 profiles are done with; kernels that stage a query's rows size them by the live profiles
+    ctx.free_profiles(ids)
     if extra and args.ungapped_hits > 0:
         result["ungapped"] = ungapped_measure(ctx, args)
     if extra and args.gate_hits > 0:

@@ -2640,7 +2640,9 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
 // ---------------------------------------------------------------------------
 static uint32_t ung_stride(st_ctx* c) { return static_cast<uint32_t>(up16(c->max_m) + 32); }
 
-static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n, int32_t* d_out) {
+// max_m: the longest query the jobs refer to (0: any live profile), which sizes
+// the staged profile rows and so the CTAs that fit on an SM.
+static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n, int32_t* d_out, uint32_t max_m = 0) {
   if (n == 0) return ST_OK;
   UngappedParams prm;
   prm.db = db_view(c);
@@ -2648,10 +2650,10 @@ static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n,
   prm.jobs = d_jobs;
   prm.n = n;
   prm.out = d_out;
-  prm.max_m_pad = ung_stride(c);
+  prm.max_m_pad = max_m ? static_cast<uint32_t>(up16(max_m) + 32) : ung_stride(c);
   const size_t smem = 16 + static_cast<size_t>(kProfRows) * prm.max_m_pad + 16;
   if (smem > static_cast<size_t>(g_ung_smem))
-    return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", c->max_m);
+    return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", max_m ? max_m : c->max_m);
   const uint64_t grid = (n + kUngChunk - 1) / kUngChunk;
   if (grid > 0x7FFFFFFFull) return fail(ST_EINVAL, "too many ungapped jobs");
   if (hits)
@@ -2695,7 +2697,7 @@ extern "C" int st_ungapped_score(st_ctx* c, uint32_t profile, const st_lane* lan
   char* d = c->stage.as<char>();
   ST_CUDA(cudaMemcpyAsync(d, h, static_cast<size_t>(n) * sizeof(UngappedJob), cudaMemcpyHostToDevice, c->stream));
   int32_t* d_out = reinterpret_cast<int32_t*>(d + jb);
-  ST_TRY(launch_ungapped(c, false, d, n, d_out));
+  ST_TRY(launch_ungapped(c, false, d, n, d_out, std::max<uint32_t>(m, 1)));
   ST_CUDA(cudaMemcpyAsync(out, d_out, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, c->stream));
   ST_CUDA(cudaStreamSynchronize(c->stream));
   return ST_OK;
@@ -2816,12 +2818,14 @@ extern "C" int st_ungapped_hits(st_ctx* c, const st_hit* hits, uint64_t n, int32
     if (n_pairs) *n_pairs = 0;
     return ST_OK;
   }
+  uint32_t max_m = 1;
   for (uint64_t i = 0; i < n; ++i) {
     if (hits[i].query >= c->profs.size() || !c->profs[hits[i].query].live)
       return fail(ST_EINVAL, "hit %llu: unknown profile id %u", static_cast<unsigned long long>(i), hits[i].query);
     if (hits[i].target >= c->n_seqs)
       return fail(ST_EINVAL, "hit %llu: target %u outside the database", static_cast<unsigned long long>(i),
                   hits[i].target);
+    max_m = std::max(max_m, c->profs[hits[i].query].m);
   }
   DevMem buf;
   const size_t hb = up16(n * sizeof(st_hit));
@@ -2835,7 +2839,7 @@ extern "C" int st_ungapped_hits(st_ctx* c, const st_hit* hits, uint64_t n, int32
   char* d = buf.as<char>();
   ST_TRY(upload_host(c, d, hits, n * sizeof(st_hit), c->stream));
   int32_t* d_out = reinterpret_cast<int32_t*>(d + hb);
-  ST_TRY(launch_ungapped(c, true, d, n, d_out));
+  ST_TRY(launch_ungapped(c, true, d, n, d_out, max_m));
   if (want_pairs) {
     int32_t* d_pb = reinterpret_cast<int32_t*>(d + hb + ob);
     uint32_t* d_pq = reinterpret_cast<uint32_t*>(d + hb + 2 * ob);
