@@ -186,3 +186,44 @@ def test_batch_of_homolog_queries(ctx):
         got = _check_prefilter(ctx, [m.sequence_rows(q) for q in qs], qs, targets, "111001101", p,
                                GapCosts.sequence_default())
         assert len(got) > 0
+
+
+def test_many_queries_in_several_chunks(ctx):
+    # more than 65,536 windows: the device prefilter takes the queries in length order in several chunks and
+    # must still return every query's candidates ranked, in query id order, and cut to a given capacity
+    model = W.Model()
+    rng = W.Rng(12)
+    m = blosum62()
+    lens = W.lognormal_lengths(rng, 320, 250, 0.6, 30, 1200)
+    qs = [model.background(rng.child(i), int(n)) for i, n in enumerate(lens)]
+    targets = []
+    for k in range(1500):
+        if k % 5 == 0:
+            targets.append(model.mutate(rng.child(5000 + k), qs[k % 320], 0.6, indel_rate=0.02))
+        else:
+            targets.append(model.background(rng.child(5000 + k), 80 + k % 300))
+    assert sum(max(int(n) - 8, 0) for n in lens) > 65536
+    got = _check_prefilter(ctx, [m.sequence_rows(q) for q in qs], qs, targets, "111001101",
+                           PrefilterParams(kmer_score=20), GapCosts.sequence_default())
+    assert len(got) > 0
+    # a capacity below the count writes the first candidates of the same order
+    ctx.upload_db_list(targets)
+    ctx.seed_index_build("111001101")
+    ids = ctx.create_profiles([m.sequence_rows(q) for q in qs])
+    try:
+        full, _, _ = ctx.prefilter_queries(ids, qs, PrefilterParams(kmer_score=20))
+        from sabertooth_b200._lib import CANDIDATE_DTYPE, check, lib, ptr
+        import ctypes as C
+        p = PrefilterParams(kmer_score=20)
+        sp, gp = p.seed_c(), p.to_c(GapCosts.sequence_default())
+        res = np.ascontiguousarray(np.concatenate(qs))
+        offs = np.zeros(len(qs) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([len(q) for q in qs])
+        k = len(full) // 3
+        out = np.zeros(k, dtype=CANDIDATE_DTYPE)
+        n = C.c_uint64()
+        check(lib.st_prefilter_queries(ctx.handle, ptr(ids), len(ids), ptr(res), ptr(offs), C.byref(sp), C.byref(gp),
+                                       ptr(out), k, C.byref(n), None, None))
+        assert n.value == len(full) and np.array_equal(out, full[:k])
+    finally:
+        ctx.free_profiles(ids)
