@@ -170,6 +170,10 @@ typedef struct {
  * returns 1 when more than cap k-mers reach thr. */
 int or_top_kmers(const int32_t* rows, int w, int32_t thr, uint32_t cap, uint64_t* codes, int32_t* scores,
                  uint32_t* n_out);
+/* top_kmers (src/prefilter.rs:470-568), the reference's default depth-first generator with
+ * cap_boundary: the same set as or_top_kmers in walk order; codes/scores need room for cap + 1. */
+int or_top_kmers_dfs(const int32_t* rows, int w, int32_t thr, uint32_t cap, uint64_t* codes, int32_t* scores,
+                     uint32_t* n_out);
 uint64_t or_index_count(const uint8_t* tgt_arena, const uint64_t* tgt_off, uint32_t n_targets, const uint32_t* offs,
                         uint32_t w, uint32_t span);
 /* out: room for or_index_count entries; sorted by (code, target, position) */

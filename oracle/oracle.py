@@ -52,6 +52,8 @@ def _load():
     lib.or_calibrate_profile.argtypes = [P, u32, P, u32, u32, u64, P, i32, i32, P, P, P, P, C.c_int]
     lib.or_top_kmers.restype = C.c_int
     lib.or_top_kmers.argtypes = [P, C.c_int, i32, u32, P, P, P]
+    lib.or_top_kmers_dfs.restype = C.c_int
+    lib.or_top_kmers_dfs.argtypes = [P, C.c_int, i32, u32, P, P, P]
     lib.or_index_count.restype = u64
     lib.or_index_count.argtypes = [P, P, u32, P, u32, u32]
     lib.or_index_build.argtypes = [P, P, u32, P, u32, u32, P]
@@ -290,6 +292,16 @@ def top_kmers(rows_w, thr, cap):
     scores = np.zeros(max(cap, 1), dtype=np.int32)
     n = C.c_uint32()
     capped = lib.or_top_kmers(_p(r), r.shape[0], thr, cap, _p(codes), _p(scores), C.byref(n))
+    return codes[:n.value].copy(), scores[:n.value].copy(), bool(capped)
+
+
+def top_kmers_dfs(rows_w, thr, cap):
+    """(codes, scores, capped) of the reference's default depth-first generator (walk order)."""
+    r = _rows(rows_w)
+    codes = np.zeros(cap + 2, dtype=np.uint64)
+    scores = np.zeros(cap + 2, dtype=np.int32)
+    n = C.c_uint32()
+    capped = lib.or_top_kmers_dfs(_p(r), r.shape[0], thr, cap, _p(codes), _p(scores), C.byref(n))
     return codes[:n.value].copy(), scores[:n.value].copy(), bool(capped)
 
 

@@ -131,6 +131,136 @@ static int top_kmers_sorted(const srow* rows, int w, int32_t thr, uint32_t cap, 
   return capped;
 }
 
+/* cap_boundary (src/prefilter.rs:571-609): the largest score t with at least cap
+ * k-mers >= t among those >= thr, and how many score above t. */
+static void cap_boundary(const srow* rows, int w, const int32_t* smax, int32_t thr, uint32_t cap, int32_t* t_out,
+                         uint64_t* above_out) {
+  /* histograms of partial sums pruned at the threshold (u64 counts) */
+  int32_t lo = 0, hi = 0;
+  size_t n = 1;
+  uint64_t* dist = (uint64_t*)calloc(1, sizeof(uint64_t));
+  dist[0] = 1;
+  for (int i = 0; i < w; ++i) {
+    const int32_t nhi = hi + rows[i].sc[0];
+    int32_t nlo = lo + rows[i].sc[AA - 1];
+    const int32_t need = thr - smax[i + 1];
+    if (need > nlo) nlo = need;
+    const size_t nn = (size_t)(nhi - nlo + 1);
+    uint64_t* tmp = (uint64_t*)calloc(nn, sizeof(uint64_t));
+    for (size_t off = 0; off < n; ++off) {
+      const uint64_t cnt = dist[off];
+      if (!cnt) continue;
+      const int32_t sv = lo + (int32_t)off;
+      for (int a = 0; a < AA; ++a) {
+        const int32_t t = sv + rows[i].sc[a];
+        if (t < nlo) break;
+        tmp[t - nlo] += cnt;
+      }
+    }
+    free(dist);
+    dist = tmp;
+    n = nn;
+    lo = nlo;
+    hi = nhi;
+  }
+  uint64_t above = 0;
+  int32_t t = hi;
+  for (;; --t) {
+    const uint64_t c = dist[t - lo];
+    if (above + c >= cap) break;
+    above += c;
+  }
+  free(dist);
+  *t_out = t;
+  *above_out = above;
+}
+
+/* top_kmers (src/prefilter.rs:470-568), the reference's default generator: a
+ * depth-first walk in rank-lexicographic order with suffix-maximum pruning;
+ * past the cap, the boundary score t* from cap_boundary, the list cut to the
+ * k-mers above t* plus the first ties, and only those accepted from then on.
+ * The returned set equals top_kmers_heap's; its order is the walk's. */
+static int top_kmers_dfs(const srow* rows, int w, int32_t thr, uint32_t cap, uint64_t* codes, int32_t* scores,
+                         uint32_t* n_out) {
+  *n_out = 0;
+  if (w == 0 || cap == 0) return 0;
+  int32_t smax[MAXK + 1];
+  smax[w] = 0;
+  for (int i = w - 1; i >= 0; --i) smax[i] = smax[i + 1] + rows[i].sc[0];
+  if (smax[0] < thr) return 0;
+  int32_t th = thr, tstar = INT32_MIN;
+  int capped = 0;
+  uint64_t ties_left = 0;
+  const int last = w - 1;
+  uint8_t rank[MAXK] = {0};
+  int32_t part[MAXK + 1] = {0};
+  uint64_t code[MAXK + 1] = {0};
+  uint32_t n = 0;
+  int d = 0;
+  for (;;) {
+    if (d == last) {
+      const int32_t bs = part[last];
+      const uint64_t bc = code[last] * AA;
+      for (int a = 0; a < AA; ++a) {
+        const int32_t ns = bs + rows[last].sc[a];
+        if (ns < th) break;
+        /* the buffer holds at most cap + 1 entries: cut as soon as it passes cap */
+        codes[n] = bc + rows[last].res[a];
+        scores[n] = ns;
+        ++n;
+        if (capped) {
+          if (ns == tstar && --ties_left == 0) th = tstar + 1;
+        } else if (n > cap) {
+          capped = 1;
+          uint64_t above;
+          cap_boundary(rows, w, smax, th, cap, &tstar, &above);
+          const uint64_t need = cap - above;
+          uint64_t kept = 0;
+          uint32_t k2 = 0;
+          for (uint32_t k = 0; k < n; ++k) {
+            if (scores[k] > tstar || (scores[k] == tstar && kept < need)) {
+              if (scores[k] == tstar) ++kept;
+              codes[k2] = codes[k];
+              scores[k2] = scores[k];
+              ++k2;
+            }
+          }
+          n = k2;
+          ties_left = need - kept;
+          th = ties_left == 0 ? tstar + 1 : tstar;
+        }
+      }
+      if (last == 0) break;
+      d = last - 1;
+      ++rank[d];
+      continue;
+    }
+    const int r = rank[d];
+    if (r < AA) {
+      const int32_t ns = part[d] + rows[d].sc[r];
+      if (ns + smax[d + 1] >= th) {
+        part[d + 1] = ns;
+        code[d + 1] = code[d] * AA + rows[d].res[r];
+        ++d;
+        rank[d] = 0;
+        continue;
+      }
+    }
+    if (d == 0) break;
+    --d;
+    ++rank[d];
+  }
+  *n_out = n;
+  return capped;
+}
+
+int or_top_kmers_dfs(const int32_t* rows, int w, int32_t thr, uint32_t cap, uint64_t* codes, int32_t* scores,
+                     uint32_t* n_out) {
+  srow sr[MAXK];
+  for (int i = 0; i < w && i < MAXK; ++i) sort_row(rows + (size_t)i * OR_NPROF, &sr[i]);
+  return top_kmers_dfs(sr, w, thr, cap, codes, scores, n_out);
+}
+
 int or_top_kmers(const int32_t* rows, int w, int32_t thr, uint32_t cap, uint64_t* codes, int32_t* scores,
                  uint32_t* n_out) {
   srow sr[MAXK];
@@ -326,8 +456,8 @@ void or_prefilter_search(const int32_t* rows_arena, const uint64_t* row_off, con
     if (m < span) continue;
     srow* sr = (srow*)malloc((size_t)m * sizeof(srow));
     for (uint32_t i = 0; i < m; ++i) sort_row(rows + (size_t)i * OR_NPROF, &sr[i]);
-    uint64_t* codes = (uint64_t*)malloc(((size_t)sp->max_kmers_per_pos + 1) * sizeof(uint64_t));
-    int32_t* scores = (int32_t*)malloc(((size_t)sp->max_kmers_per_pos + 1) * sizeof(int32_t));
+    uint64_t* codes = (uint64_t*)malloc(((size_t)sp->max_kmers_per_pos + 2) * sizeof(uint64_t));
+    int32_t* scores = (int32_t*)malloc(((size_t)sp->max_kmers_per_pos + 2) * sizeof(int32_t));
     uint64_t cap_h = 1 << 16, nh = 0;
     uint32_t* ht = (uint32_t*)malloc(cap_h * 4);
     int32_t* hd = (int32_t*)malloc(cap_h * 4);
@@ -349,7 +479,7 @@ void or_prefilter_search(const int32_t* rows_arena, const uint64_t* row_off, con
       }
       if (skip) continue;
       uint32_t nk = 0;
-      top_kmers_sorted(wr, (int)w, sp->kmer_score, sp->max_kmers_per_pos, codes, scores, &nk);
+      top_kmers_dfs(wr, (int)w, sp->kmer_score, sp->max_kmers_per_pos, codes, scores, &nk);
       int have = 0;
       for (uint32_t k = 0; k < nk; ++k) have |= codes[k] == exact;
       if (res && sp->exact_seeds && !have) codes[nk++] = exact;

@@ -2,7 +2,9 @@
 by the reference's own prefilter tests (src/prefilter.rs):
 
 * top_kmers_is_exact_global_order (:1754-1812): brute force over all 20^w
-  k-mers (w = 2..4, SplitMix64 seed 11, caps 1..100,000) in canonical order;
+  k-mers (w = 2..4, SplitMix64 seed 11, caps 1..100,000) in canonical order,
+  for the best-first restatement (that order) and the reference's default
+  depth-first generator with cap_boundary (the same set, in walk order);
 * old_dfs_generator_was_not_globally_ordered (:1839-1857): the global top-2;
 * exact_kmer_is_found, exact_seed_below_threshold_is_kept,
   similar_kmer_reaches_diverged_target, profile_prefilter_finds_target,
@@ -51,6 +53,13 @@ def test_top_kmers_is_exact_global_order():
                 assert list(zip(got_c.tolist(), got_s.tolist())) == want, (w, case, cap)
                 assert capped == (len(allk) > cap)
                 capped_cases += capped
+                # the reference's default depth-first generator: the same set, in walk order
+                d_c, d_s, d_capped = O.top_kmers_dfs(rows, thr, cap)
+                assert sorted(zip(d_c.tolist(), d_s.tolist())) == sorted(want), (w, case, cap)
+                assert d_capped == capped
+                if not capped:
+                    walk = sorted(range(len(keep)), key=lambda k: [int(cc[k]) for cc in cols])
+                    assert d_c.tolist() == [int(keep[k]) for k in walk]
     assert capped_cases > 100
 
 
