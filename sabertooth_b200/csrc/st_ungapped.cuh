@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(256) ungapped_kernel(const UngappedParams prm)
 // outside int8 read the int32 profile with an explicit window test.
 __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const UngappedParams prm) {
   extern __shared__ __align__(16) int8_t smem[];
-  __shared__ unsigned long long s_run_end, s_next;
+  __shared__ unsigned long long s_run_end;
+  __shared__ uint32_t s_next;
   const HitRec* hits = reinterpret_cast<const HitRec*>(prm.jobs);
   const uint32_t stride = prm.max_m_pad;
   int8_t* base = smem + 16;
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
       }
       if (threadIdx.x == 0) {
         s_run_end = e;
-        s_next = a + blockDim.x;
+        s_next = blockDim.x;
       }
     }
     const uint32_t m = prm.prof.qlen[q];
@@ -232,19 +233,21 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
     if (threadIdx.x < 16) smem[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t b = s_run_end;
+    const uint32_t nb = static_cast<uint32_t>(b - a);  // hits of the run, indexed from a
+    const HitRec* run = hits + a;
     const bool narrow = prm.prof.fits8[q] != 0;
     const int32_t* p32 = prm.prof.p32[q];
     const int32_t s32 = static_cast<int32_t>(prm.prof.stride32[q]);
     const int32_t last_row = static_cast<int32_t>(m) - 1;
-    uint64_t k = a + threadIdx.x;
+    uint32_t k = threadIdx.x;
     const uint8_t* tp = nullptr;
     int32_t d = 0, p0 = 0, p1 = 0, pa = 0, cur = 0, best = 0;
     bool live = false;
-    auto take = [&](uint64_t j) {
+    auto take = [&](uint32_t j) {
       k = j;
-      live = j < b;
+      live = j < nb;
       if (live) {
-        const HitRec h = hits[j];
+        const HitRec h = run[j];
         const int64_t n = prm.db.length[h.target];
         d = h.diag;
         // diag_range, src/ungapped.rs:38-46
@@ -269,12 +272,19 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
           const uint32_t w[4] = {v.x, v.y, v.z, v.w};
           const int32_t qa = pa - d;
           if (narrow) {
+            // u = max(cur, 0) carried instead of cur: u' = max(u + s, 0) is one DPX op, and
+            // max(best, cur) = max(best, u) since best >= 0; int8 scores over at most 2^20 rows
+            // cannot overflow, so the unwrapped add equals the reference's wrapping one
             const int8_t* rowbase = base + qa;
 #pragma unroll
-            for (int bb = 0; bb < 16; ++bb) {
-              const uint32_t r = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
-              cur = wadd(max(cur, 0), static_cast<int32_t>(rowbase[static_cast<int32_t>(r * stride) + bb]));
-              best = max(best, cur);
+            for (int bb = 0; bb < 16; bb += 2) {
+              const uint32_t r0 = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+              const uint32_t r1 = (w[bb >> 2] >> (((bb + 1) & 3) * 8)) & 0xFFu;
+              const int32_t u0 =
+                  __viaddmax_s32_relu(cur, static_cast<int32_t>(rowbase[static_cast<int32_t>(r0 * stride) + bb]), 0);
+              cur = __viaddmax_s32_relu(u0, static_cast<int32_t>(rowbase[static_cast<int32_t>(r1 * stride) + bb + 1]),
+                                        0);
+              best = __vimax3_s32(best, u0, cur);
             }
           } else {
 #pragma unroll
@@ -290,8 +300,8 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
           pa += 16;
         }
         if (pa >= p1) {
-          prm.out[k] = best;
-          take(atomicAdd(&s_next, 1ull));
+          prm.out[a + k] = best;
+          take(atomicAdd(&s_next, 1u));
         }
       }
     }
