@@ -257,6 +257,7 @@ struct st_ctx {
   cudaStream_t own = nullptr;     // the context's stream (also used for graph capture)
   cudaStream_t copy = nullptr;    // host->device uploads that may overlap queued kernels
   cudaStream_t stream = nullptr;  // where work is launched
+  cudaStream_t plan_s = nullptr;  // the device planner's first stage, beside kernels still queued
   std::recursive_mutex mu;
   uint64_t launches = 0;
   // database
@@ -267,6 +268,8 @@ struct st_ctx {
   uint32_t max_len = 0;  // longest sequence
   uint64_t n_res = 0;
   bool has_db = false;
+  cudaEvent_t db_ev = nullptr;  // after the last stream-ordered change of the database tables
+  bool db_ev_set = false;
   // profiles
   std::vector<ProfileMeta> profs;
   std::vector<std::unique_ptr<ProfileBlock>> blocks;
@@ -278,6 +281,7 @@ struct st_ctx {
   bool prof_ev_set = false;
   cudaEvent_t copy_ev = nullptr;   // uploads on the copy stream
   Pinned prof_desc;                // build descriptors on their way to the device
+  Pinned plan_meta;                // profile lengths and int8 flags for the device planner's first stage
   Pinned prof_stage[2];            // pageable rows staged on their way to the device
   cudaEvent_t prof_stage_ev[2] = {};
   bool prof_stage_used[2] = {};
@@ -587,6 +591,11 @@ extern "C" void st_shutdown(st_ctx* c) {
     cudaStreamSynchronize(c->copy);
     cudaStreamDestroy(c->copy);
   }
+  if (c->plan_s) {
+    cudaStreamSynchronize(c->plan_s);
+    cudaStreamDestroy(c->plan_s);
+  }
+  if (c->db_ev) cudaEventDestroy(c->db_ev);
   if (c->prof_ev) cudaEventDestroy(c->prof_ev);
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
   for (auto e : c->meta_ev)
@@ -1843,7 +1852,8 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
                o_qclass = carve(np1 * 4), o_nwt = carve(np1 * 4), o_ncta = carve(np1 * 4), o_qk0 = carve(np1 * 4),
                o_qk1 = carve(np1 * 4), o_qi0 = carve(np1 * 4), o_qi1 = carve(np1 * 4), o_as = carve(np1 * 4),
                o_aw = carve(np1 * 4), o_ac = carve(np1 * 4), o_os = carve(np1 * 4), o_ow = carve(np1 * 4),
-               o_oc = carve(np1 * 4), o_tot = carve(sizeof(DpTotals)), o_tmp = carve(t_tmp);
+               o_oc = carve(np1 * 4), o_tot = carve(sizeof(DpTotals)), o_sq = carve(np1 * 4),
+               o_sf = carve(np1), o_tmp = carve(t_tmp);
   ST_TRY(pool_get(c, off, work));
   char* b = work.as<char>();
   DpWork w{};
@@ -1878,40 +1888,64 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   void* tmp = b + o_tmp;
   in.pairs = reinterpret_cast<const st_pair*>(b + o_pairs);
 
-  // stage 1: pairs in, classify, sort, per-query class and CTA-task counts, class order
-  // the pairs go up on the copy stream, beside kernels still queued on the stream
+  // stage 1: pairs in, classify, sort, per-query class and CTA-task counts, class order.
+  // It runs on the planner's own stream, so its one wait (for the per-class
+  // totals) does not wait for kernels still queued on the stream, e.g. the
+  // previous batch. It reads the pairs and a snapshot of the profiles'
+  // lengths and int8 flags, both uploaded on the copy stream, and the
+  // database lengths (ordered after any stream-ordered database change).
   if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+  if (!c->plan_s) ST_CUDA(cudaStreamCreateWithFlags(&c->plan_s, cudaStreamNonBlocking));
+  cudaStream_t s1 = c->plan_s;
+  ST_TRY(c->plan_meta.reserve(np1 * 5));
+  {
+    uint32_t* hq = c->plan_meta.as<uint32_t>();
+    uint8_t* hf = c->plan_meta.as<uint8_t>(np1 * 4);
+    hq[n_prof] = 0;
+    hf[n_prof] = 0;
+    for (uint32_t k = 0; k < n_prof; ++k) {
+      const ProfileMeta& pm = c->profs[k];
+      hq[k] = pm.live ? pm.m : 0;
+      hf[k] = pm.live && pm.fits8 ? 1 : 0;
+    }
+  }
   ST_CUDA(cudaMemcpyAsync(b + o_pairs, pairs, n * 16, cudaMemcpyHostToDevice, c->copy));
+  ST_CUDA(cudaMemcpyAsync(b + o_sq, c->plan_meta.p, np1 * 4, cudaMemcpyHostToDevice, c->copy));
+  ST_CUDA(cudaMemcpyAsync(b + o_sf, c->plan_meta.as<uint8_t>(np1 * 4), np1, cudaMemcpyHostToDevice, c->copy));
   ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
-  ST_CUDA(cudaStreamWaitEvent(st, c->copy_ev, 0));
-  ST_CUDA(cudaMemsetAsync(cinit, 0, (kNumClasses + 2) * 4, st));
-  ST_CUDA(cudaMemsetAsync(w.qcnt, 0, np1 * 4, st));
-  ST_CUDA(cudaMemsetAsync(w.totals, 0, sizeof(DpTotals), st));
+  ST_CUDA(cudaStreamWaitEvent(s1, c->copy_ev, 0));
+  if (c->db_ev_set) ST_CUDA(cudaStreamWaitEvent(s1, c->db_ev, 0));
+  DpIn in1 = in;
+  in1.prof.qlen = reinterpret_cast<const uint32_t*>(b + o_sq);
+  in1.prof.fits8 = reinterpret_cast<const uint8_t*>(b + o_sf);
+  ST_CUDA(cudaMemsetAsync(cinit, 0, (kNumClasses + 2) * 4, s1));
+  ST_CUDA(cudaMemsetAsync(w.qcnt, 0, np1 * 4, s1));
+  ST_CUDA(cudaMemsetAsync(w.totals, 0, sizeof(DpTotals), s1));
   const uint32_t gb = static_cast<uint32_t>(std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(c->sms) * 8));
-  dp_classify_kernel<<<gb, 256, 0, st>>>(in, w);
+  dp_classify_kernel<<<gb, 256, 0, s1>>>(in1, w);
   cub::DoubleBuffer<ull> kb(w.keys, w.keys_alt);
   cub::DoubleBuffer<uint32_t> vb(w.vals, w.vals_alt);
-  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_sort, kb, vb, static_cast<int>(n), 0, key_bits, st));
+  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_sort, kb, vb, static_cast<int>(n), 0, key_bits, s1));
   w.vals_sorted = vb.Current();
-  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.qcnt, w.qstart, static_cast<int>(np1), st));
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.qcnt, w.qstart, static_cast<int>(np1), s1));
   const uint32_t gq32 = static_cast<uint32_t>((static_cast<uint64_t>(n_prof) * 32 + 255) / 256);
   const uint32_t gq = static_cast<uint32_t>((np1 + 255) / 256);
-  dp_pick_kernel<<<gq32, 256, 0, st>>>(in, w, cls);
-  dp_split_kernel<<<gq, 256, 0, st>>>(in, w, cls);
+  dp_pick_kernel<<<gq32, 256, 0, s1>>>(in1, w, cls);
+  dp_split_kernel<<<gq, 256, 0, s1>>>(in1, w, cls);
   cub::DoubleBuffer<uint32_t> qk(w.qkey, w.qkey_alt), qi(w.qid, w.qid_alt);
-  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_qsort, qk, qi, static_cast<int>(n_prof), 0, 6, st));
+  ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_qsort, qk, qi, static_cast<int>(n_prof), 0, 6, s1));
   w.qid_sorted = qi.Current();
-  dp_counts_kernel<<<gq, 256, 0, st>>>(in, w, cls);
-  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_slots, w.o_slots, static_cast<int>(np1), st));
-  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_wt, w.o_wt, static_cast<int>(np1), st));
-  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_cta, w.o_cta, static_cast<int>(np1), st));
+  dp_counts_kernel<<<gq, 256, 0, s1>>>(in1, w, cls);
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_slots, w.o_slots, static_cast<int>(np1), s1));
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_wt, w.o_wt, static_cast<int>(np1), s1));
+  ST_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t_scan, w.a_cta, w.o_cta, static_cast<int>(np1), s1));
   ST_CUDA(cudaGetLastError());
   c->launches += 5;
   DpTotals tot;
   uint32_t n_list32 = 0;  // pairs the classify stage sent to the 32-bit kernel
-  ST_CUDA(cudaMemcpyAsync(&tot, w.totals, sizeof(DpTotals), cudaMemcpyDeviceToHost, st));
-  ST_CUDA(cudaMemcpyAsync(&n_list32, w.list_count, 4, cudaMemcpyDeviceToHost, st));
-  ST_CUDA(cudaStreamSynchronize(st));
+  ST_CUDA(cudaMemcpyAsync(&tot, w.totals, sizeof(DpTotals), cudaMemcpyDeviceToHost, s1));
+  ST_CUDA(cudaMemcpyAsync(&n_list32, w.list_count, 4, cudaMemcpyDeviceToHost, s1));
+  ST_CUDA(cudaStreamSynchronize(s1));
   tc.lap("stage 1 (device)");
 
   // stage 2: sizes known; task arrays, scratch, emission, LPT order
@@ -3496,7 +3530,18 @@ struct DbState {
   bool has = false;
 };
 
+// The swapped-in tables may still be filling on the context's stream: the
+// event marks that point for work launched on other streams.
 static void swap_db(st_ctx* c, DbState& s) {
+  if (!c->db_ev && cudaEventCreateWithFlags(&c->db_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    c->db_ev = nullptr;
+    cudaStreamSynchronize(c->stream);  // no event: wait instead
+  }
+  if (c->db_ev) {
+    cudaEventRecord(c->db_ev, c->stream);
+    c->db_ev_set = true;
+  }
   std::swap(c->db_arena, s.arena);
   std::swap(c->db_off, s.off);
   std::swap(c->db_len, s.len);
