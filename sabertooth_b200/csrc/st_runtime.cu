@@ -269,6 +269,7 @@ struct st_ctx {
   uint64_t n_res = 0;
   bool has_db = false;
   cudaEvent_t db_ev = nullptr;  // after the last stream-ordered change of the database tables
+  cudaEvent_t trace_base = nullptr;  // with ST_TRACE: the origin of the batches' device timestamps
   bool db_ev_set = false;
   // profiles
   std::vector<ProfileMeta> profs;
@@ -596,6 +597,7 @@ extern "C" void st_shutdown(st_ctx* c) {
     cudaStreamDestroy(c->plan_s);
   }
   if (c->db_ev) cudaEventDestroy(c->db_ev);
+  if (c->trace_base) cudaEventDestroy(c->trace_base);
   if (c->prof_ev) cudaEventDestroy(c->prof_ev);
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
   for (auto e : c->meta_ev)
@@ -1895,7 +1897,13 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   // lengths and int8 flags, both uploaded on the copy stream, and the
   // database lengths (ordered after any stream-ordered database change).
   if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
-  if (!c->plan_s) ST_CUDA(cudaStreamCreateWithFlags(&c->plan_s, cudaStreamNonBlocking));
+  if (!c->plan_s) {
+    // the highest priority: its few short kernels take SMs as soon as CTAs of queued
+    // persistent grids retire, instead of after every CTA still waiting to start
+    int lo = 0, hi = 0;
+    ST_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    ST_CUDA(cudaStreamCreateWithPriority(&c->plan_s, cudaStreamNonBlocking, hi));
+  }
   cudaStream_t s1 = c->plan_s;
   ST_TRY(c->plan_meta.reserve(np1 * 5));
   {
@@ -2080,10 +2088,18 @@ struct st_batch {
   st_plan* plan = nullptr;
   std::unique_ptr<Pinned> stage;  // null when the caller's buffers are pinned
   cudaEvent_t done = nullptr;
+  // with ST_TRACE: the stream reaching the batch, the plan's launches starting and ending, the download done
+  cudaEvent_t tr[4] = {};
 };
 
 static void batch_release(st_batch* b) {
   st_ctx* c = b->c;
+  for (auto& e : b->tr)
+    if (e) {
+      cudaEventSynchronize(e);
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
   if (b->done) {
     cudaEventSynchronize(b->done);
     c->spare_events.push_back(b->done);
@@ -2108,6 +2124,11 @@ static int batch_begin(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   b->scores = scores;
   b->kernels = kernels;
   TraceClock tc("pairs");
+  if (trace_on() && n) {
+    if (!c->trace_base && cudaEventCreate(&c->trace_base) == cudaSuccess) cudaEventRecord(c->trace_base, c->stream);
+    for (auto& e : b->tr) cudaEventCreate(&e);
+    cudaEventRecord(b->tr[0], c->stream);
+  }
   if (n == 0) {  // nothing to score: a batch that is done when the stream gets there
     ST_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
     ST_CUDA(cudaEventRecord(b->done, c->stream));
@@ -2143,9 +2164,12 @@ static int batch_begin(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
     ST_TRY(plan_build(c, pairs, n, open, ext, d_scores, d_kern, &b->plan, false, c->stream, 0));
     tc.lap("plan");
   }
+  if (b->tr[1]) cudaEventRecord(b->tr[1], c->stream);
   ST_TRY(plan_run(b->plan));
+  if (b->tr[2]) cudaEventRecord(b->tr[2], c->stream);
   ST_CUDA(cudaMemcpyAsync(h_scores, d_scores, n * 4, cudaMemcpyDeviceToHost, c->stream));
   if (kernels) ST_CUDA(cudaMemcpyAsync(h_kern, d_kern, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (b->tr[3]) cudaEventRecord(b->tr[3], c->stream);
   if (!c->spare_events.empty()) {
     b->done = c->spare_events.back();
     c->spare_events.pop_back();
@@ -2162,6 +2186,12 @@ static int batch_finish(st_batch* b) {
   TraceClock tc("pairs");
   st_ctx* c = b->c;
   const cudaError_t e = cudaEventSynchronize(b->done);
+  if (e == cudaSuccess && b->tr[3] && c->trace_base) {
+    float t[4] = {};
+    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&t[i], c->trace_base, b->tr[i]);
+    fprintf(stderr, "[st] batch device: stream at %.3f, plan launches %.3f - %.3f, download done %.3f ms\n", t[0], t[1],
+            t[2], t[3]);
+  }
   if (e == cudaSuccess && b->stage) {
     const uint64_t n = b->n;
     const int32_t* hs = b->stage->as<int32_t>();
