@@ -163,12 +163,23 @@ struct Pinned {
   ~Pinned() {
     if (p) cudaFreeHost(p);
   }
+  // Grows by at least half the current size, to a size class (2^k times 1, 1.25,
+  // 1.5 or 1.75): freeing pinned memory waits for the whole device, so a buffer
+  // that follows slowly growing batches should reallocate rarely.
   int reserve(size_t n) {
     if (n <= bytes) return ST_OK;
+    const size_t target = std::max<size_t>(n, bytes + bytes / 2);
+    size_t cls = 1 << 20;
+    while (cls < target) cls <<= 1;
+    size_t want = cls;
+    for (size_t k = 5; k <= 8; ++k)
+      if (cls / 8 * k >= target) {
+        want = cls / 8 * k;
+        break;
+      }
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    size_t want = std::max<size_t>(n, 1 << 20);
     ST_CUDA(cudaMallocHost(&p, want));
     bytes = want;
     return ST_OK;
@@ -257,7 +268,8 @@ struct st_ctx {
   cudaStream_t own = nullptr;     // the context's stream (also used for graph capture)
   cudaStream_t copy = nullptr;    // host->device uploads that may overlap queued kernels
   cudaStream_t stream = nullptr;  // where work is launched
-  cudaStream_t plan_s = nullptr;  // the device planner's first stage, beside kernels still queued
+  cudaStream_t plan_s = nullptr;  // profile builds and the device planner, beside kernels still queued
+  cudaEvent_t plan_ev = nullptr;  // the end of a device plan's preparation on plan_s
   std::recursive_mutex mu;
   uint64_t launches = 0;
   // database
@@ -414,6 +426,21 @@ static DeviceDb db_view(st_ctx* c) {
   d.length = c->db_len.as<uint32_t>();
   d.n_seqs = c->n_seqs;
   return d;
+}
+
+// The context's side stream for short preparatory work (profile layout builds,
+// the device planner) that need not queue behind the kernels already on the
+// context's stream; at the highest priority, so its kernels take SMs as the
+// running grids retire.
+static int side_stream(st_ctx* c, cudaStream_t* out) {
+  if (!c->plan_s) {
+    int lo = 0, hi = 0;
+    ST_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    ST_CUDA(cudaStreamCreateWithPriority(&c->plan_s, cudaStreamNonBlocking, hi));
+  }
+  if (!c->plan_ev) ST_CUDA(cudaEventCreateWithFlags(&c->plan_ev, cudaEventDisableTiming));
+  *out = c->plan_s;
+  return ST_OK;
 }
 
 // Orders the context's stream after the last profile build and, when
@@ -597,6 +624,7 @@ extern "C" void st_shutdown(st_ctx* c) {
     cudaStreamDestroy(c->plan_s);
   }
   if (c->db_ev) cudaEventDestroy(c->db_ev);
+  if (c->plan_ev) cudaEventDestroy(c->plan_ev);
   if (c->trace_base) cudaEventDestroy(c->trace_base);
   if (c->prof_ev) cudaEventDestroy(c->prof_ev);
   if (c->copy_ev) cudaEventDestroy(c->copy_ev);
@@ -756,14 +784,19 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   const size_t rows_total = row_offsets[n_profiles] - row_offsets[0];
   const size_t src_bytes = rows_total * kAlpha * 4;
   const size_t desc_bytes = up16(n_profiles * sizeof(ProfBuildDesc));
+  // the layouts are built on the side stream, beside kernels already queued on the
+  // context's stream; work that reads profiles waits for prof_ev (sync_profiles)
+  cudaStream_t bs = nullptr;
+  ST_TRY(side_stream(c, &bs));
   DevMem blk_mem, tmp;  // tmp: uploaded rows and descriptors, back to the pool once the layouts are built
   ST_TRY(pool_get(c, bytes32 + bytes8, blk_mem));
   ST_TRY(pool_get(c, src_bytes + desc_bytes + 16, tmp));
   struct Back {
     st_ctx* c;
     DevMem* m;
-    ~Back() { pool_put_after(c, std::move(*m), c->stream); }
-  } back_tmp{c, &tmp};
+    cudaStream_t s;
+    ~Back() { pool_put_after(c, std::move(*m), s); }
+  } back_tmp{c, &tmp, bs};
   if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
   if (!c->prof_ev) ST_CUDA(cudaEventCreateWithFlags(&c->prof_ev, cudaEventDisableTiming));
   tc.lap("alloc");
@@ -771,8 +804,8 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   int32_t* d_src = tmp.as<int32_t>();
   ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + up16(src_bytes));
   // The rows travel on the copy stream (beside any kernels still queued) while
-  // the host computes their score ranges; the build runs on the context's
-  // stream after both. The call returns once the rows and descriptors are on
+  // the host computes their score ranges; the build runs on the side stream
+  // after both. The call returns once the rows and descriptors are on
   // the device (the caller may reuse them), not when the build is done: later
   // work on the profiles is ordered after it.
   // score range of profile k (residues >= 21 score 0); with dst, the rows are copied there in the same pass
@@ -827,11 +860,11 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   memcpy(c->prof_desc.p, desc.data(), n_profiles * sizeof(ProfBuildDesc));
   ST_CUDA(cudaMemcpyAsync(d_desc, c->prof_desc.p, n_profiles * sizeof(ProfBuildDesc), cudaMemcpyHostToDevice, c->copy));
   ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
-  ST_CUDA(cudaStreamWaitEvent(c->stream, c->copy_ev, 0));
-  build_profiles_kernel<<<n_profiles, 256, 0, c->stream>>>(d_src, d_desc, base);
+  ST_CUDA(cudaStreamWaitEvent(bs, c->copy_ev, 0));
+  build_profiles_kernel<<<n_profiles, 256, 0, bs>>>(d_src, d_desc, base);
   ++c->launches;
   ST_CUDA(cudaGetLastError());
-  ST_CUDA(cudaEventRecord(c->prof_ev, c->stream));
+  ST_CUDA(cudaEventRecord(c->prof_ev, bs));
   c->prof_ev_set = true;
   ST_CUDA(cudaEventSynchronize(c->copy_ev));
   tc.lap("upload");
@@ -887,7 +920,10 @@ static int profile_free(st_ctx* c, uint32_t id) {
   p.live = false;
   ProfileBlock* b = c->blocks[p.block].get();
   if (--b->live == 0) {
-    pool_put_after(c, std::move(b->mem), c->stream);  // reusable once work queued so far is done
+    // reusable once work queued so far is done, the block's layout build included
+    if (c->prof_ev_set && cudaStreamWaitEvent(c->stream, c->prof_ev, 0) != cudaSuccess)
+      return fail(ST_ECUDA, "cudaStreamWaitEvent failed");
+    pool_put_after(c, std::move(b->mem), c->stream);
     c->free_blocks.push_back(p.block);
   }
   p.block = -1;
@@ -1938,14 +1974,8 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   // lengths and int8 flags, both uploaded on the copy stream, and the
   // database lengths (ordered after any stream-ordered database change).
   if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
-  if (!c->plan_s) {
-    // the highest priority: its few short kernels take SMs as soon as CTAs of queued
-    // persistent grids retire, instead of after every CTA still waiting to start
-    int lo = 0, hi = 0;
-    ST_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-    ST_CUDA(cudaStreamCreateWithPriority(&c->plan_s, cudaStreamNonBlocking, hi));
-  }
-  cudaStream_t s1 = c->plan_s;
+  cudaStream_t s1 = nullptr;
+  ST_TRY(side_stream(c, &s1));
   ST_TRY(c->plan_meta.reserve(np1 * 5));
   {
     uint32_t* hq = c->plan_meta.as<uint32_t>();
@@ -2053,18 +2083,22 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   o.cta_idx = reinterpret_cast<uint32_t*>(a + p_ci0);
   o.cta_idx_alt = reinterpret_cast<uint32_t*>(a + p_ci1);
   o.n_cta = static_cast<uint32_t>(n_cta);
-  if (n_prof) dp_emit_kernel<<<gq32, 256, 0, st>>>(in, w, cls, o);
+  // the rest of the preparation stays on the planner's stream (it reads the same
+  // snapshot); the stream joins it before the plan's grids
+  if (n_prof) dp_emit_kernel<<<gq32, 256, 0, s1>>>(in1, w, cls, o);
   if (n_cta) {
     cub::DoubleBuffer<ull> ck(o.cta_key, o.cta_key_alt);
     cub::DoubleBuffer<uint32_t> ci(o.cta_idx, o.cta_idx_alt);
-    ST_CUDA(cub::DeviceRadixSort::SortPairs(a + p_tmp, t_lpt, ck, ci, static_cast<int>(n_cta), 0, 44 + 6, st));
+    ST_CUDA(cub::DeviceRadixSort::SortPairs(a + p_tmp, t_lpt, ck, ci, static_cast<int>(n_cta), 0, 44 + 6, s1));
     o.cta_idx_sorted = ci.Current();
-    dp_gather_cta_kernel<<<static_cast<uint32_t>((n_cta + 255) / 256), 256, 0, st>>>(o);
+    dp_gather_cta_kernel<<<static_cast<uint32_t>((n_cta + 255) / 256), 256, 0, s1>>>(o);
   }
   uint2* zline = reinterpret_cast<uint2*>(a + p_z);
-  dp_fill_zline_kernel<<<(zcols + 255) / 256, 256, 0, st>>>(zline, zcols, pk_splat(-open));
+  dp_fill_zline_kernel<<<(zcols + 255) / 256, 256, 0, s1>>>(zline, zcols, pk_splat(-open));
   ST_CUDA(cudaGetLastError());
   c->launches += 3;
+  ST_CUDA(cudaEventRecord(c->plan_ev, s1));
+  ST_CUDA(cudaStreamWaitEvent(st, c->plan_ev, 0));
 
   plan->counters = counters;
   plan->counters_init = cinit;

@@ -90,15 +90,18 @@ int st_server::launch(std::unique_ptr<Batch>& b) {
   for (size_t i = 0; i < b->reqs.size(); ++i) offs[i + 1] = offs[i] + b->reqs[i]->m;
   const size_t need = std::max<size_t>(static_cast<size_t>(offs.back()) * 21 * 4, 64);
   if (arena_bytes < need) {
+    // at least 16 MB, and at least double: freeing pinned memory waits for the
+    // batch in flight, so growth should be rare
+    const size_t want = std::max<size_t>({need + need / 4, 2 * arena_bytes, 16u << 20});
     if (arena) cudaFreeHost(arena);
     arena = nullptr;
     arena_bytes = 0;
-    if (cudaHostAlloc(reinterpret_cast<void**>(&arena), need + need / 4, cudaHostAllocPortable) != cudaSuccess) {
+    if (cudaHostAlloc(reinterpret_cast<void**>(&arena), want, cudaHostAllocPortable) != cudaSuccess) {
       cudaGetLastError();
       st_internal_set_error("serving: pinned host allocation failed");
       return ST_ENOMEM;
     }
-    arena_bytes = need + need / 4;
+    arena_bytes = want;
   }
   size_t n_pairs = 0;
   for (size_t i = 0; i < b->reqs.size(); ++i) n_pairs += b->reqs[i]->pairs.size();
