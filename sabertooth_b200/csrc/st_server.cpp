@@ -13,6 +13,8 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -31,6 +33,20 @@ __attribute__((visibility("hidden"))) void st_internal_set_error(const char* msg
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// With ST_TRACE set: worker steps slower than 5 ms go to stderr.
+bool server_trace() {
+  static const bool on = [] {
+    const char* e = std::getenv("ST_TRACE");
+    return e && *e && *e != '0';
+  }();
+  return on;
+}
+void trace_slow(const char* what, Clock::time_point t0, size_t reqs, size_t pairs) {
+  if (!server_trace()) return;
+  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+  if (ms > 5.0) fprintf(stderr, "[st] server %s %.3f ms (%zu requests, %zu pairs)\n", what, ms, reqs, pairs);
+}
 
 struct Request {
   uint64_t id = 0;
@@ -181,7 +197,9 @@ void st_server::run() {
       }
     }
     if (b) {
+      const Clock::time_point t0 = Clock::now();
       const int rc = launch(b);
+      trace_slow("launch", t0, b->reqs.size(), b->pairs.size());
       if (rc != ST_OK) {
         b->handle = nullptr;
         const std::string err = st_last_error();
@@ -203,7 +221,10 @@ void st_server::run() {
     }
     if (!inflight.empty()) {
       inflight_bytes -= inflight.front()->bytes;
+      const Clock::time_point t0 = Clock::now();
+      const size_t nr = inflight.front()->reqs.size(), np = inflight.front()->pairs.size();
       finish(inflight.front());
+      trace_slow("finish", t0, nr, np);
       inflight.pop_front();
     }
   }
