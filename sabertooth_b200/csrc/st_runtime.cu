@@ -1084,58 +1084,46 @@ static int plan_enqueue(st_plan* p, cudaStream_t st, st_ctx::ForkSet* fs, bool g
   const size_t nc = p->classes.size();
   if (!fs || nc <= 1) {
     for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, st>>>(cp.prm);
-  } else if (graph) {
-    // Captured into a graph, whose launch order of independent nodes is the
-    // runtime's: the forks first, the costliest class last on the launching
-    // stream measured fastest there (21.1 ms for the 1.2 M-pair PSSM batch,
-    // against 21.7 ms with the costliest class captured first, or with launch
-    // priorities by cost).
+  } else {
+    // The classes run side by side: the costliest on the launching stream, the
+    // others on forks joined before sw32. The launch order matters, as the block
+    // scheduler serves the grids in that order:
+    // * direct launches: the costliest first, the others by decreasing cost, so
+    //   the grids run longest first and the small classes fill the tails of the
+    //   large ones (21.3 ms for the 1.2 M-pair PSSM batch, against 22.3 ms with
+    //   the costliest launched last);
+    // * captured into a graph, whose launch order of independent nodes is the
+    //   runtime's: the forks in class order, the costliest last, measured fastest
+    //   there (21.1 ms, against 21.7 ms with the costliest captured first).
+    // Launch priorities by cost were tried: they also order one batch's classes,
+    // but a batch queued behind a running one then jumps ahead of its small
+    // classes and delays its completion.
+    size_t order[kNumClasses];
+    for (size_t i = 0; i < nc; ++i) order[i] = i;
     size_t big = 0;
     for (size_t i = 1; i < nc; ++i)
       if (p->classes[i].cells > p->classes[big].cells) big = i;
+    if (graph) {
+      std::stable_partition(order, order + nc, [&](size_t i) { return i != big; });
+    } else {
+      std::stable_sort(order, order + nc,
+                       [&](size_t a, size_t b) { return p->classes[a].cells > p->classes[b].cells; });
+      big = order[0];
+    }
     if (cudaEventRecord(fs->ev[0], st) != cudaSuccess) return ST_ECUDA;
     bool used[st_ctx::ForkSet::kForks] = {};
     int next = 0;
-    for (size_t i = 0; i < nc; ++i) {
-      if (i == big) continue;
-      const int j = next++ % st_ctx::ForkSet::kForks;
-      if (!used[j] && cudaStreamWaitEvent(fs->s[j], fs->ev[0], 0) != cudaSuccess) return ST_ECUDA;
-      used[j] = true;
-      const ClassPlan& cp = p->classes[i];
-      kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, fs->s[j]>>>(cp.prm);
-    }
-    const ClassPlan& cb = p->classes[big];
-    kClasses[cb.cls].fn<<<cb.grid, kClasses[cb.cls].W * 32, cb.smem, st>>>(cb.prm);
-    for (int j = 0; j < st_ctx::ForkSet::kForks; ++j) {
-      if (!used[j]) continue;
-      if (cudaEventRecord(fs->ev[1 + j], fs->s[j]) != cudaSuccess) return ST_ECUDA;
-      if (cudaStreamWaitEvent(st, fs->ev[1 + j], 0) != cudaSuccess) return ST_ECUDA;
-    }
-  } else {
-    // Direct launches: the block scheduler serves the grids in launch order, so the
-    // costliest class goes first (on the launching stream) and the others follow by
-    // decreasing cost on the forks: the grids run longest first and the small classes
-    // fill the tails of the large ones (21.3 ms for the 1.2 M-pair PSSM batch, against
-    // 22.3 ms with the costliest launched last). Launch priorities would also order
-    // one batch's classes, but a batch queued behind a running one would then jump
-    // ahead of its small classes and delay its completion.
-    size_t order[kNumClasses];
-    for (size_t i = 0; i < nc; ++i) order[i] = i;
-    std::stable_sort(order, order + nc,
-                     [&](size_t a, size_t b) { return p->classes[a].cells > p->classes[b].cells; });
-    auto launch = [&](const ClassPlan& cp, cudaStream_t s) {
+    for (size_t r = 0; r < nc; ++r) {
+      const ClassPlan& cp = p->classes[order[r]];
+      cudaStream_t s = st;
+      if (order[r] != big) {
+        const int j = next++ % st_ctx::ForkSet::kForks;
+        if (!used[j] && cudaStreamWaitEvent(fs->s[j], fs->ev[0], 0) != cudaSuccess) return ST_ECUDA;
+        used[j] = true;
+        s = fs->s[j];
+      }
       kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, s>>>(cp.prm);
-      return cudaGetLastError();
-    };
-    if (cudaEventRecord(fs->ev[0], st) != cudaSuccess) return ST_ECUDA;
-    if (launch(p->classes[order[0]], st) != cudaSuccess) return ST_ECUDA;
-    bool used[st_ctx::ForkSet::kForks] = {};
-    int next = 0;
-    for (size_t r = 1; r < nc; ++r) {
-      const int j = next++ % st_ctx::ForkSet::kForks;
-      if (!used[j] && cudaStreamWaitEvent(fs->s[j], fs->ev[0], 0) != cudaSuccess) return ST_ECUDA;
-      used[j] = true;
-      if (launch(p->classes[order[r]], fs->s[j]) != cudaSuccess) return ST_ECUDA;
+      if (cudaGetLastError() != cudaSuccess) return ST_ECUDA;
     }
     for (int j = 0; j < st_ctx::ForkSet::kForks; ++j) {
       if (!used[j]) continue;
