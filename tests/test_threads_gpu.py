@@ -1,0 +1,101 @@
+"""Calls from several host threads at once on one context.
+
+The reference calls its scoring functions from rayon workers concurrently
+(src/search.rs:553-556, src/prefilter.rs:1570), so the C ABI must give every
+thread the result it would get alone. Here six threads each build their own
+profiles and run, interleaved with the others: a batch large enough for the
+device planner, a small host-planned batch, an asynchronous batch, plain
+per-call scores and ungapped hits, then free their profiles. Every result must
+equal the same call made from one thread (whose parity with the oracle the
+other tests establish), and the context must stay usable afterwards.
+"""
+import ctypes as C
+import threading
+
+import numpy as np
+import pytest
+
+from sabertooth_b200 import GapCosts
+from sabertooth_b200 import workloads as W
+from sabertooth_b200._lib import HIT_DTYPE, PAIR_DTYPE, check, lib
+
+pytestmark = pytest.mark.gpu
+
+GAPS = GapCosts(44, 4)
+N_THREADS = 6
+
+
+def _pairs(ids, q, t):
+    p = np.zeros(len(q), dtype=PAIR_DTYPE)
+    p["profile"] = ids[q]
+    p["target"] = t
+    p["band_radius"] = -1
+    return p
+
+
+def _hits(ids, q, t, lens, rng):
+    h = np.zeros(len(q), dtype=HIT_DTYPE)
+    h["query"] = ids[q]
+    h["target"] = t
+    h["diag"] = rng.integers(-60, np.maximum(lens[t], 1)).astype(np.int32)
+    return h
+
+
+def _plain(ctx, pid, target):
+    """One st_sw_score call (the per-call drop-in) on a host target."""
+    t = np.ascontiguousarray(target, dtype=np.uint8)
+    s, k = C.c_int32(), C.c_uint32()
+    check(lib.st_sw_score(ctx.handle, pid, t.ctypes.data, t.size, GAPS.open, GAPS.extend, C.byref(s), C.byref(k)))
+    return s.value
+
+
+def _work(ctx, w, lens, seed):
+    """Everything one thread does; returns its results in a fixed order."""
+    rng = np.random.default_rng(seed)
+    ids = ctx.create_profiles(w.rows)
+    try:
+        big = _pairs(ids, w.pair_q, w.pair_t)  # >= 16 K pairs: the device planner
+        small = big[: 300].copy()              # the host planner
+        r_big = ctx.sw_score_pairs(big, GAPS)
+        batch = ctx.sw_score_pairs_async(small, GAPS)
+        targets = w.targets()
+        r_plain = [_plain(ctx, int(ids[w.pair_q[i]]), targets[int(w.pair_t[i])]) for i in range(8)]
+        hits = _hits(ids, w.pair_q[:2000], w.pair_t[:2000], lens, rng)
+        r_ung = ctx.ungapped_hits(hits, with_pairs=False)
+        r_small = batch.wait()
+        return r_big, r_small, np.array(r_plain), r_ung
+    finally:
+        ctx.free_profiles(ids)
+
+
+def test_concurrent_calls_equal_single_thread_results(ctx):
+    w = W.config3(seed=41, n_queries=40, db_residues=80_000, per_query=420)
+    assert w.n_pairs >= 16_384
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    lens = np.diff(w.db_offsets.astype(np.int64))
+    want = [_work(ctx, w, lens, seed=100 + k) for k in range(N_THREADS)]
+
+    got = [None] * N_THREADS
+    errors = []
+    start = threading.Barrier(N_THREADS)
+
+    def run(k):
+        try:
+            start.wait()
+            got[k] = _work(ctx, w, lens, seed=100 + k)
+        except Exception as e:  # reported below
+            errors.append(repr(e))
+
+    th = [threading.Thread(target=run, args=(k,)) for k in range(N_THREADS)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=300)
+    assert not errors, errors
+    for k in range(N_THREADS):
+        for a, b in zip(got[k], want[k]):
+            assert np.array_equal(a, b), k
+    # the context still works, and every profile was freed
+    again = _work(ctx, w, lens, seed=100)
+    for a, b in zip(again, want[0]):
+        assert np.array_equal(a, b)
