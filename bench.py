@@ -743,7 +743,7 @@ def gate_measure(ctx, args):
     residues), 2x10^7 hits (30% on two-piece planted homologs), sequence defaults (4 diagonals, window 48,
     span 6, gate 42, gaps 11/1), regions on.  Device-resident hits per step: one st_prefilter_gate_device call
     (sort, groups, top diagonals, segments, chains, gate, ranking).  e2e: st_prefilter_gate from host hits to
-    host candidates.  Algorithmic bytes: 16 B per hit + the residues of every scored window + 32 B per
+    host candidates, the hits in pinned host memory (and, reported beside, in a pageable array).  Algorithmic bytes: 16 B per hit + the residues of every scored window + 32 B per
     candidate, against the measured HBM copy bandwidth."""
     import torch
     from oracle import oracle as O
@@ -781,13 +781,22 @@ def gate_measure(ctx, args):
     got_dev = d_out[:n_c * 32].cpu().numpy().view(O.CANDIDATE_DTYPE)
     ctx.set_stream(0)
     ms = float(np.median(ts))
-    # e2e: host hits in, host candidates out
-    te = []
+    # e2e: host hits in (from pinned host memory, as a serving caller holds them; and from a pageable
+    # array, staged through pinned blocks by the library), host candidates out
+    hits_pin = torch.empty(hits.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(hits.dtype)
+    hits_pin[:] = hits
+    te, tp = [], []
     for _ in range(3):
         t0 = time.perf_counter()
-        got, _ = ctx.prefilter_gate(hits, params, gaps)
+        got, _ = ctx.prefilter_gate(hits_pin, params, gaps)
         te.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        got_p, _ = ctx.prefilter_gate(hits, params, gaps)
+        tp.append(time.perf_counter() - t0)
     ms_e2e = float(np.median(te)) * 1e3
+    ms_e2e_pageable = float(np.median(tp)) * 1e3
+    same_pageable = bool(np.array_equal(got, got_p))
+    del hits_pin
     # CPU baseline: the oracle's restatement of the reference's evidence stage with its AVX2 batched Kadane,
     # queries in parallel over all host threads, on the whole workload; its candidates are the parity check
     targets = [w.db_residues[int(a_):int(b_)] for a_, b_ in zip(w.db_offsets[:-1], w.db_offsets[1:])]
@@ -819,7 +828,11 @@ def gate_measure(ctx, args):
                         "sequence defaults, regions on",
             "ms_per_step": round(ms, 3), "mhits_per_s": round(n / ms / 1e3, 1),
             "e2e": {"ms_per_call": round(ms_e2e, 3), "mhits_per_s": round(n / ms_e2e / 1e3, 1),
-                    "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(32 * int(n_c))},
+                    "h2d_bytes_per_step": int(16 * n), "d2h_bytes_per_step": int(32 * int(n_c)),
+                    "inputs": "pinned host hits",
+                    "pageable": {"ms_per_call": round(ms_e2e_pageable, 3),
+                                 "mhits_per_s": round(n / ms_e2e_pageable / 1e3, 1),
+                                 "matches_pinned": same_pageable}},
             "candidates": int(n_c), "stats": {k: int(v) for k, v in stats.items()},
             "algorithmic_bytes": int(ab),
             "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
