@@ -11,9 +11,11 @@ reference's gapped_cells) / step time.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--scale S]
 
-Under torchrun (N > 1) every rank scores its own instance of the workload
-(seed + rank): weak scaling with no collective on the data path; the step
-time is the max over ranks.  Rank 0 prints one JSON line.
+Under torchrun (N > 1) the batch is split by target shards (residue-balanced
+contiguous shards of the database, profiles replicated): each rank scores the
+pairs whose target it holds, and every step ends with the exchange that
+gathers the scores to rank 0 in pair order (strong scaling; the step time is
+the max over ranks).  Rank 0 prints one JSON line.
 
 On one GPU the line also carries the other rows, each with its own CPU
 baseline and parity check: `calibration` (per-profile calibration of config-3
@@ -62,6 +64,9 @@ def parse():
     ap.add_argument("--search-queries", type=int, default=1000,
                     help="config-5 queries for the whole-search measurement (0: skip)")
     ap.add_argument("--search-targets", type=int, default=1_000_000, help="config-5 database sequences")
+    ap.add_argument("--exhaustive-queries", type=int, default=200,
+                    help="config-1 queries against its 20,000 targets (0: skip)")
+    ap.add_argument("--long-pairs", type=int, default=50_000, help="config-4 pairs, both halves (0: skip)")
     ap.add_argument("--gate-hits", type=int, default=20_000_000,
                     help="seed hits for the evidence / chain / gate measurement (0: skip)")
     return ap.parse_args()
@@ -87,7 +92,7 @@ def combine_ranks(ms, cells, device):
 
 
 def make_workload(args, rank):
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     nq = max(8, int(round(4000 * args.scale)))
     db = max(50_000, int(round(2_600_000 * args.scale)))
     return W.config3(seed=args.seed + rank, n_queries=nq, db_residues=db)
@@ -196,6 +201,19 @@ def cpu_baseline(w, gpu_scores, seconds, seed=0):
     return out
 
 
+def repo_libraries_mapped():
+    """Shared libraries of this repository mapped into the process (from /proc/self/maps)."""
+    out = set()
+    try:
+        for ln in open("/proc/self/maps"):
+            f = ln.split()
+            if len(f) >= 6 and f[-1].endswith(".so") and os.path.realpath(f[-1]).startswith(os.path.realpath(ROOT)):
+                out.add(os.path.relpath(os.path.realpath(f[-1]), os.path.realpath(ROOT)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if world > 1 and rank != 0:
@@ -216,16 +234,160 @@ def run_reference(args):
     cb = {"cores": cores, "sample": f"the whole workload per step ({w.n_pairs:,} pairs, {cells:,} cells): the "
                                     f"reference's default AVX2 path (u8 -> i16 striped -> scalar) restated in C, "
                                     f"queries in parallel over {cores} threads"}
+    mapped = repo_libraries_mapped()
+    if any(os.path.basename(x) == "libsabertooth_b200.so" for x in mapped):
+        raise RuntimeError("the reference arm mapped the product library: " + ", ".join(mapped))
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config_of(args, w, 1),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port",
                              "sample": "per step: " + cb["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "libraries_mapped": mapped,
             "note": "the reference (Rust) cannot be built here (no cargo, crates not vendored); its AVX2 "
-                    "scoring path restated in C runs on all host cores"}
+                    "scoring path restated in C runs on all host cores; the inputs come from synth/ (the PSSM "
+                    "builder in synth/libsynth.so), and no product code is loaded"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_sharded(args, rank, world, local):
+    """N > 1: the config-3 batch split by target shards (src/shard.rs:69-97 balance; queries and profiles
+    replicated).  Every rank builds the same workload, uploads only its shard of the database, and scores
+    the pairs whose target it holds through a captured plan; one step = that plan + the exchange: an NCCL
+    all-gather of (global pair index, score) records, placed in global pair order on rank 0 by one
+    index_copy (padding records point at a sink slot past the last pair).  Total work is fixed: strong
+    scaling.  Step time = the slowest rank's, value = all pairs' cells / that time."""
+    import torch
+    import torch.distributed as dist
+    from sabertooth_b200 import Context, GapCosts
+    from sabertooth_b200._lib import PAIR_DTYPE
+    from sabertooth_b200.shard import ShardMap
+    dev = torch.device("cuda", local)
+    t_gen = time.perf_counter()
+    w = make_workload(args, 0)
+    t_gen = time.perf_counter() - t_gen
+    gaps = GapCosts(w.gap_open, w.gap_extend)
+    n = w.n_pairs
+    smap = ShardMap.of(w.db_offsets, world)
+    res, offs = smap.shard_db(w.db_residues, w.db_offsets, rank)
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload_db(res, offs)
+    ids = ctx.create_profiles(w.rows)
+    gpairs = np.zeros(n, dtype=PAIR_DTYPE)
+    gpairs["profile"] = ids[w.pair_q]
+    gpairs["target"] = w.pair_t
+    gpairs["band_radius"] = -1
+    idx, pairs = smap.route(gpairs, rank)
+    k = len(idx)
+    qlen = np.array([len(r) for r in w.rows], dtype=np.int64)
+    tlen = np.diff(w.db_offsets.astype(np.int64))
+    my_cells = int((qlen[w.pair_q[idx]] * tlen[w.pair_t[idx]]).sum())
+    width_t = torch.tensor([k], dtype=torch.int64, device=dev)
+    dist.all_reduce(width_t, op=dist.ReduceOp.MAX)
+    width = max(int(width_t.item()), 1)
+    d_scores = torch.zeros(max(k, 1), dtype=torch.int32, device=dev)
+    rec = torch.zeros((width, 2), dtype=torch.int64, device=dev)
+    rec[:, 0] = n  # padding records land in the sink slot
+    if k:
+        rec[:k, 0] = torch.from_numpy(idx).to(dev)
+    gbuf = torch.zeros((world * width, 2), dtype=torch.int64, device=dev)
+    merged = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    plan = ctx.plan(pairs, gaps, d_scores.data_ptr()) if k else None
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        if plan is not None:
+            plan.run()
+            rec[:k, 1].copy_(d_scores[:k])
+        dist.all_gather_into_tensor(gbuf, rec)
+        if rank == 0:
+            merged.index_copy_(0, gbuf[:, 0], gbuf[:, 1])
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        launches0 = ctx.launch_count()
+        clk = ClockSampler(local)
+        clk.start()
+        for s in range(args.steps):
+            flush.zero_()
+            starts[s].record(stream)
+            step()
+            ends[s].record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        launches = ctx.launch_count() - launches0
+    ms_rank = float(np.mean([a.elapsed_time(b) for a, b in zip(starts, ends)]))
+    ms, _ = combine_ranks(ms_rank, my_cells, dev)
+    cells = w.cells()
+    gcups = cells / (ms * 1e-3) / 1e9
+
+    # end to end through the public API with host buffers, every step on every rank: profiles from pinned
+    # int32 rows, this rank's pairs up, scores down, the host (index, score) records gathered to rank 0 and
+    # placed there; timed per rank between barriers, the slowest rank's time
+    nrows = np.array([len(r) for r in w.rows], dtype=np.uint64)
+    row_offs = np.zeros(len(w.rows) + 1, dtype=np.uint64)
+    row_offs[1:] = np.cumsum(nrows)
+    rows_pin = torch.empty((int(row_offs[-1]), 21), dtype=torch.int32, pin_memory=True).numpy()
+    for q, r in enumerate(w.rows):
+        rows_pin[int(row_offs[q]):int(row_offs[q + 1])] = r
+    from sabertooth_b200.shard import gather_scores
+    e2e_ms, e2e_ok = [], True
+    dev_scores = merged[:n].to(torch.int32).cpu().numpy() if rank == 0 else None
+    for _ in range(max(args.e2e_steps, 3)):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eids = ctx.create_profiles_arena(rows_pin, row_offs)
+        lp = pairs.copy()
+        lp["profile"] = eids[w.pair_q[idx]]
+        sc = ctx.sw_score_pairs(lp, gaps) if k else np.zeros(0, np.int32)
+        got = gather_scores(idx, sc, n, device=dev)
+        ctx.free_profiles(eids)
+        t_rank = time.perf_counter() - t0
+        tmax, _ = combine_ranks(t_rank * 1e3, 0, dev)
+        e2e_ms.append(tmax)
+        if rank == 0:
+            e2e_ok &= bool(np.array_equal(got, dev_scores))
+    e2e_t = float(np.median(e2e_ms))
+    if plan is not None:
+        plan.close()
+    ctx.free_profiles(ids)
+    if rank != 0:
+        return None
+    # parity sample on rank 0: the merged scores of 2,000 random pairs against the oracle
+    from oracle import oracle as O
+    rng = np.random.default_rng(3)
+    sel = rng.choice(n, size=min(2000, n), replace=False)
+    ar = O.Arena(w.rows, w.targets())
+    sample_ok = bool(np.array_equal(O.sw_pairs(ar, w.pair_q[sel], w.pair_t[sel], w.gap_open, w.gap_extend),
+                                    dev_scores[sel]))
+    cfg = config_of(args, w, world)
+    cfg["parallelism"] = f"target shards x{world} (residue-balanced contiguous, profiles replicated), " \
+                         "scores gathered to rank 0 (NCCL all-gather) inside every step"
+    return {"metric": METRIC, "value": round(gcups, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "int16x2 (packed DPX) + int32 rescore", "data": "synthetic",
+            "config": cfg, "clocks": clocks, "gpu_launches": int(launches),
+            "e2e": {"value": round(cells / (e2e_t * 1e-3) / 1e9, 2), "unit": UNIT,
+                    "h2d_bytes_per_step": int(rows_pin.nbytes + k * PAIR_DTYPE.itemsize),
+                    "d2h_bytes_per_step": int(k * 4), "ms_per_step": round(e2e_t, 2),
+                    "matches_device_run": bool(e2e_ok),
+                    "includes": "per step on every rank: profile build from pinned int32 rows, this rank's pairs "
+                                "up, plan, launches, scores down, host records gathered to rank 0 and placed; "
+                                "rank 0's host-to-device bytes stated"},
+            "shards": [{"targets": int(b - a), "residues": int(w.db_offsets[b] - w.db_offsets[a])}
+                       for a, b in smap.ranges],
+            "matches_oracle_sample": sample_ok, "setup_s": {"generate": round(t_gen, 1)}}
 
 
 def main():
@@ -240,6 +402,12 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
+        result = run_sharded(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(result), flush=True)
+        dist.barrier()
+        dist.destroy_process_group()
+        return 0
     from sabertooth_b200 import Context, GapCosts
     from sabertooth_b200._lib import PAIR_DTYPE
 
@@ -458,6 +626,10 @@ def main():
         result["gate"] = gate_measure(ctx, args)
     if extra and args.search_queries > 0:
         result["search"] = search_measure(ctx, args)
+    if extra and args.exhaustive_queries > 0:
+        result["exhaustive"] = exhaustive_measure(ctx, args)
+    if extra and args.long_pairs > 0:
+        result["long_mix"] = long_mix_measure(ctx, args)
     if extra and args.serving_pairs > 0:
         result["serving"] = serving_measure(ctx, args)
     if world > 1:
@@ -476,7 +648,7 @@ def ungapped_measure(ctx, args):
     (window residues + 12 B hit + 4 B output per hit) / time against the measured HBM copy bandwidth."""
     import torch
     from oracle import oracle as O
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     t0 = time.perf_counter()
     w = W.config2(seed=args.seed, n_hits=args.ungapped_hits)
     t_gen = time.perf_counter() - t0
@@ -556,7 +728,7 @@ def search_measure(ctx, args):
     from oracle import oracle as O
     from sabertooth_b200 import GapCosts, PrefilterParams
     from sabertooth_b200._lib import PAIR_DTYPE
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     t0 = time.perf_counter()
     w = W.config5(seed=args.seed, n_queries=args.search_queries, n_targets=args.search_targets)
     t_gen = time.perf_counter() - t0
@@ -748,7 +920,7 @@ def gate_measure(ctx, args):
     import torch
     from oracle import oracle as O
     from sabertooth_b200 import GapCosts, PrefilterParams
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     t0 = time.perf_counter()
     w = W.seed_hits(seed=args.seed, n_hits=args.gate_hits)
     t_gen = time.perf_counter() - t0
@@ -880,6 +1052,161 @@ def gate_window_bytes(w, params):
     return int(np.maximum(hi - lo, 0)[keep].sum())
 
 
+def _timed_plans(ctx, plans, steps, warmup=3):
+    """Device time of one step = every plan run once, on one stream, L2 flushed before each step."""
+    import torch
+    st = torch.cuda.Stream()
+    ctx.set_stream(st.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ts = []
+    with torch.cuda.stream(st):
+        for _ in range(warmup):
+            for p in plans:
+                p.run()
+        st.synchronize()
+        for _ in range(max(3, steps)):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for p in plans:
+                p.run()
+            b.record(st)
+            st.synchronize()
+            ts.append(a.elapsed_time(b))
+    ctx.set_stream(0)
+    return ts
+
+
+def exhaustive_measure(ctx, args):
+    """Config 1, plain exhaustive SW-Gotoh (easysearch-style): every one of 200 BLOSUM62 queries against every
+    one of 20,000 targets (lengths lognormal median 250, 30-1,000; 10% planted homologs at ~40% identity),
+    gaps 11/1, an int32 score per pair (4x10^6 scores).  One step = one run of the captured plan; the scores
+    are compared with the CPU port's over the whole workload."""
+    import torch
+    from oracle import oracle as O
+    from sabertooth_b200 import GapCosts
+    from sabertooth_b200._lib import PAIR_DTYPE
+    from synth import workloads as W
+    t0 = time.perf_counter()
+    w = W.config1(seed=args.seed, n_queries=args.exhaustive_queries)
+    t_gen = time.perf_counter() - t0
+    gaps = GapCosts(w.gap_open, w.gap_extend)
+    ctx.upload_db(w.db_residues, w.db_offsets)
+    ids = ctx.create_profiles(w.rows)
+    pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
+    pairs["profile"] = ids[w.pair_q]
+    pairs["target"] = w.pair_t
+    pairs["band_radius"] = -1
+    d_s = torch.empty(w.n_pairs, dtype=torch.int32, device="cuda")
+    d_k = torch.empty(w.n_pairs, dtype=torch.int32, device="cuda")
+    plan = ctx.plan(pairs, gaps, d_s.data_ptr(), d_k.data_ptr())
+    ts = _timed_plans(ctx, [plan], args.steps)
+    stats = plan.stats()
+    plan.close()
+    got = d_s.cpu().numpy()
+    kern = d_k.cpu().numpy()
+    # end to end once: host pairs in, scores out (profiles resident)
+    t0 = time.perf_counter()
+    e2e = ctx.sw_score_pairs(pairs, gaps)
+    t_e2e = time.perf_counter() - t0
+    ctx.free_profiles(ids)
+    cells = w.cells()
+    t0 = time.perf_counter()
+    want = O.striped_pairs(O.Arena(w.rows, w.targets()), w.pair_q, w.pair_t, 11, 1, threads=os.cpu_count())
+    t_cpu = time.perf_counter() - t0
+    ms = float(np.median(ts))
+    return {"workload": f"config 1: {len(w.rows)} BLOSUM62 queries x {len(w.db_offsets) - 1} targets "
+                        f"({w.n_pairs:,} pairs, exhaustive), gaps 11/1",
+            "cells": int(cells), "ms_per_step": round(ms, 3), "gcups": round(cells / (ms * 1e-3) / 1e9, 1),
+            "e2e_gcups": round(cells / t_e2e / 1e9, 1), "e2e_how": "one st_sw_score_pairs call: host pairs in, "
+                                                                 "scores out, profiles and database resident",
+            "rescored_pairs": int(stats["rescored_pairs"]), "gpu32_pairs": int((kern == 2).sum()),
+            "matches_cpu_baseline": bool(np.array_equal(got, want)), "e2e_matches": bool(np.array_equal(e2e, want)),
+            "cpu_baseline": {"value": round(cells / t_cpu / 1e9, 2), "unit": UNIT, "cores": os.cpu_count(),
+                             "kind": "port", "sample": "the whole workload once: the reference's default AVX2 path "
+                                                       "(u8 -> i16 striped -> scalar) restated in C"},
+            "setup_s": round(t_gen, 1)}
+
+
+def long_mix_measure(ctx, args):
+    """Config 4, the long/overflow mix: half BLOSUM62 (11/1) and half PSSM (44/4) pairs, targets 1,000-35,000
+    residues (10% above 10,000), queries lognormal median 250 (30-2,000), 5% near-identical planted pairs, pairs
+    with a length ratio above 4 scored in the band of radius 64 around the planted diagonal (0 when unplanted,
+    src/align.rs:439-447).  One step = both halves' plans.  Cells: m*n for full pairs plus the in-band cells of
+    banded pairs.  Every score is compared with the CPU oracle's (the scalar band rule for banded pairs, the AVX2
+    port for full pairs)."""
+    import torch
+    from oracle import oracle as O
+    from sabertooth_b200 import GapCosts
+    from sabertooth_b200._lib import PAIR_DTYPE
+    from synth import workloads as W
+    half = max(1, args.long_pairs // 2)
+    t0 = time.perf_counter()
+    halves = [W.config4(seed=args.seed, n_pairs=half, kind="blosum62"),
+              W.config4(seed=args.seed, n_pairs=half, kind="pssm")]
+    t_gen = time.perf_counter() - t0
+    seqs = halves[0].targets() + halves[1].targets()
+    ctx.upload_db_list(seqs)
+    ids = ctx.create_profiles(halves[0].rows + halves[1].rows)
+    plans, outs, infos = [], [], []
+    q_base, t_base = 0, 0
+    for w in halves:
+        pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
+        pairs["profile"] = ids[q_base + w.pair_q.astype(np.int64)]
+        pairs["target"] = t_base + w.pair_t
+        pairs["band_center"] = w.band_center
+        pairs["band_radius"] = w.band_radius
+        d_s = torch.empty(w.n_pairs, dtype=torch.int32, device="cuda")
+        d_k = torch.empty(w.n_pairs, dtype=torch.int32, device="cuda")
+        plans.append(ctx.plan(pairs, GapCosts(w.gap_open, w.gap_extend), d_s.data_ptr(), d_k.data_ptr()))
+        outs.append((d_s, d_k))
+        q_base += len(w.rows)
+        t_base += len(w.db_offsets) - 1
+    ts = _timed_plans(ctx, plans, args.steps)
+    stats = [p.stats() for p in plans]
+    for p in plans:
+        p.close()
+    ctx.free_profiles(ids)
+    res = {"workload": f"config 4: {sum(w.n_pairs for w in halves):,} pairs, half BLOSUM62 11/1 and half PSSM 44/4, "
+                       "targets 1,000-35,000, band 64 for length ratio > 4", "halves": []}
+    cells_tot, ok_all, cpu_s = 0, True, 0.0
+    for w, (d_s, d_k), stt in zip(halves, outs, stats):
+        got = d_s.cpu().numpy()
+        kern = d_k.cpu().numpy()
+        banded = w.band_radius >= 0
+        m = np.array([len(r) for r in w.rows], dtype=np.int64)[w.pair_q]
+        n = np.diff(w.db_offsets.astype(np.int64))[w.pair_t]
+        full_cells = int((m[~banded] * n[~banded]).sum())
+        cells = w.cells()
+        ar = O.Arena(w.rows, w.targets())
+        want = np.zeros(w.n_pairs, dtype=np.int32)
+        t0 = time.perf_counter()
+        fi = np.nonzero(~banded)[0]
+        bi = np.nonzero(banded)[0]
+        want[fi] = O.striped_pairs(ar, w.pair_q[fi], w.pair_t[fi], w.gap_open, w.gap_extend,
+                                   threads=os.cpu_count())
+        want[bi] = O.sw_pairs(ar, w.pair_q[bi], w.pair_t[bi], w.gap_open, w.gap_extend, w.band_center[bi],
+                              w.band_radius[bi], threads=os.cpu_count())
+        cpu_s += time.perf_counter() - t0
+        ok = bool(np.array_equal(got, want))
+        ok_all &= ok
+        cells_tot += cells
+        res["halves"].append({"kind": w.name, "pairs": int(w.n_pairs), "banded_pairs": int(banded.sum()),
+                              "planted_pairs": int(w.info["planted"]), "cells": int(cells),
+                              "full_pair_cells": full_cells, "in_band_cells": int(cells - full_cells),
+                              "rescored_pairs": int(stt["rescored_pairs"]), "gpu32_pairs": int((kern == 2).sum()),
+                              "matches_cpu_baseline": ok})
+    ms = float(np.median(ts))
+    res.update({"cells": int(cells_tot), "ms_per_step": round(ms, 3),
+                "gcups": round(cells_tot / (ms * 1e-3) / 1e9, 1), "matches_cpu_baseline": bool(ok_all),
+                "cpu_baseline": {"value": round(cells_tot / cpu_s / 1e9, 2), "unit": UNIT, "cores": os.cpu_count(),
+                                 "kind": "port", "sample": "the whole workload once: the AVX2 striped port for full "
+                                                           "pairs, the scalar band rule for banded pairs"},
+                "setup_s": round(t_gen, 1)})
+    return res
+
+
 def hbm_peak_gbs():
     """The measured copy bandwidth of this pool's B200s, or the fallback figure."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -896,7 +1223,7 @@ def serving_measure(ctx, args):
     give the saturated throughput, compared with one batched call over the same pairs."""
     import threading
     from sabertooth_b200 import GapCosts, Server
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     from sabertooth_b200._lib import PAIR_DTYPE
     w = W.config4(seed=args.seed, n_pairs=args.serving_pairs, kind="blosum62")
     gaps = GapCosts(w.gap_open, w.gap_extend)

@@ -176,6 +176,25 @@ typedef struct {
  * buffers, blocking; any number of lanes per call. */
 int st_ungapped_score(st_ctx* ctx, uint32_t profile, const st_lane* lanes, uint32_t n, int32_t* out);
 
+/* The reference's Lane (src/ungapped.rs:265-270) field for field: `target` is
+ * a slice (pointer + length) of the host residue arena that was given to
+ * st_db_upload (the reference builds it from index.seq(tid),
+ * src/prefilter.rs:1563-1568); diag and the query window [lo, hi) are as in
+ * Lane.  Any slice of one database sequence is accepted. */
+typedef struct {
+  const uint8_t* target;
+  uint64_t len;
+  int64_t diag;
+  uint64_t lo;
+  uint64_t hi;
+} st_lane_slice;
+
+/* Drop-in for ungapped::score_batch (src/ungapped.rs:285-386) taking the
+ * reference's lanes unchanged: out[i] = kadane_score of lanes[i].  A lane
+ * whose slice is not inside the uploaded arena, or whose window is outside
+ * diag_range of the slice, fails with ST_EINVAL.  Host buffers, blocking. */
+int st_ungapped_score_slices(st_ctx* ctx, uint32_t profile, const st_lane_slice* lanes, uint32_t n, int32_t* out);
+
 /* A prefilter seed hit: query profile id, database ordinal, diagonal.  The
  * scored window is the whole diagonal (diag_range; diag_window = 0 semantics). */
 typedef struct {

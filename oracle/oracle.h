@@ -198,6 +198,13 @@ void or_prefilter_search(const int32_t* rows_arena, const uint64_t* row_off, con
                          const or_seed_params* sp, const or_prefilter_params* gp, or_candidate* out,
                          uint64_t cap_per_query, uint64_t* n_cand, uint64_t* n_hits, int nthreads);
 
+/* Sequence-query row preparation (rowprep.c): composition-bias correction
+ * (src/compbias.rs:38-70) and the low-complexity mask (src/mask.rs:68-128). */
+void or_comp_bias(const uint8_t* q, uint32_t n, const int32_t* score, const double* p_back, int penalize_only,
+                  int32_t* out);
+uint32_t or_low_complexity_mask(const uint8_t* seq, uint32_t n, uint32_t w, double locut, double hicut,
+                                uint8_t* mask);
+
 #ifdef __cplusplus
 }
 #endif

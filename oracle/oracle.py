@@ -20,7 +20,8 @@ def build():
 
 
 def _load():
-    if not os.path.exists(LIB):
+    srcs = [os.path.join(HERE, f) for f in os.listdir(HERE) if f.endswith((".c", ".h"))]
+    if not os.path.exists(LIB) or any(os.path.getmtime(f) > os.path.getmtime(LIB) for f in srcs):
         build()
     lib = C.CDLL(LIB)
     P, u32, i32, u64, i64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64, C.c_int64
@@ -62,6 +63,9 @@ def _load():
     lib.or_prefilter_search.argtypes = [P, P, P, P, u32, P, P, P, u32, u32, P, P, P, P, P, P, u64, P, P, C.c_int]
     lib.or_seed_hits.restype = u64
     lib.or_seed_hits.argtypes = [P, P, u32, P, u32, u32, P, P, u64, u32, P, P, P, u64, P]
+    lib.or_comp_bias.argtypes = [P, u32, P, P, C.c_int, P]
+    lib.or_low_complexity_mask.restype = u32
+    lib.or_low_complexity_mask.argtypes = [P, u32, u32, C.c_double, C.c_double, P]
     return lib
 
 
@@ -119,6 +123,39 @@ def reference_score(rows, t, open_, ext):
 def band_score(rows, t, open_, ext, center, radius):
     r, tt = _rows(rows), _t(t)
     return lib.or_band_score(_p(r), r.shape[0], _p(tt) if tt.size else None, tt.size, open_, ext, center, radius)
+
+
+def comp_bias(q, score, p_back, penalize_only=False):
+    """local_bias_correction_mode (src/compbias.rs:38-70): per-position integer corrections."""
+    qq = _t(q)
+    sc = np.ascontiguousarray(score, dtype=np.int32).reshape(NPROF, NPROF)
+    pb = np.ascontiguousarray(p_back[:20], dtype=np.float64)
+    out = np.zeros(max(qq.size, 1), dtype=np.int32)
+    lib.or_comp_bias(_p(qq), qq.size, _p(sc), _p(pb), int(penalize_only), _p(out))
+    return out[:qq.size]
+
+
+def low_complexity_mask(seq, window, locut, hicut):
+    """low_complexity_mask (src/mask.rs:62-128): a bool per position."""
+    s = _t(seq)
+    out = np.zeros(max(s.size, 1), dtype=np.uint8)
+    lib.or_low_complexity_mask(_p(s), s.size, window, locut, hicut, _p(out))
+    return out[:s.size].astype(bool)
+
+
+def search_rows(q, score, p_back, comp_bias_corr=True, mask_scoring=(15, 2.3, 2.3)):
+    """A sequence query's alignment rows as the reference's search builds them (src/search.rs:432-455):
+    matrix rows, plus the composition-bias correction of each column, and the X row for positions that
+    the scoring mask covers."""
+    qq = _t(q)
+    sc = np.ascontiguousarray(score, dtype=np.int32).reshape(NPROF, NPROF)
+    rows = sc[np.minimum(qq, NPROF - 1)].astype(np.int32)
+    if comp_bias_corr:
+        rows = rows + comp_bias(qq, sc, p_back)[:, None]
+    if mask_scoring is not None:
+        mk = low_complexity_mask(qq, *mask_scoring)
+        rows[mk] = sc[NPROF - 1]
+    return np.ascontiguousarray(rows, dtype=np.int32)
 
 
 class Arena:

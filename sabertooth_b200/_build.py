@@ -2,9 +2,9 @@
 
     python sabertooth_b200/_build.py          # libsabertooth_b200.so for sm_100a
 
-nvcc compiles the CUDA runtime and kernels for sm_100a (B200) and the host
-utilities into one shared library next to this file, so the built .so travels
-with the source tree.  Rebuilds only when a source is newer than the library.
+nvcc compiles the CUDA runtime, the kernels (sm_100a, B200) and the serving
+loops into one shared library next to this file, so the built .so travels with
+the source tree.  Rebuilds only when a source is newer than the library.
 """
 import os
 import subprocess
@@ -15,9 +15,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libsabertooth_b200.so")
 
-SOURCES = ["st_runtime.cu", "st_noalloc.cu", "st_host.cpp", "st_server.cpp"]
+SOURCES = ["st_runtime.cu", "st_noalloc.cu", "st_server.cpp"]
 HEADERS = ["st_common.cuh", "st_sw16.cuh", "st_sw32.cuh", "st_ungapped.cuh", "st_tuning.h", "st_dplan.cuh", "st_gate.cuh", "st_calib.cuh", "st_seed.cuh"]
-INCLUDES = [os.path.join(ROOT, "include", h) for h in ("sabertooth_b200.h", "sabertooth_b200_host.h")]
+INCLUDES = [os.path.join(ROOT, "include", "sabertooth_b200.h")]
 
 
 def nvcc():

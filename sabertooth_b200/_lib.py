@@ -32,16 +32,16 @@ class st_lane(C.Structure):
     _fields_ = [("target", C.c_uint32), ("lo", C.c_uint32), ("hi", C.c_uint32), ("diag", C.c_int32)]
 
 
+class st_lane_slice(C.Structure):
+    _fields_ = [("target", C.c_void_p), ("len", C.c_uint64), ("diag", C.c_int64), ("lo", C.c_uint64),
+                ("hi", C.c_uint64)]
+
+
 class st_hit(C.Structure):
     _fields_ = [("query", C.c_uint32), ("target", C.c_uint32), ("diag", C.c_int32)]
 
 
-PAIR_DTYPE = np.dtype([("profile", "<u4"), ("target", "<u4"), ("band_center", "<i4"), ("band_radius", "<i4")])
-LANE_DTYPE = np.dtype([("target", "<u4"), ("lo", "<u4"), ("hi", "<u4"), ("diag", "<i4")])
-HIT_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("diag", "<i4")])
-SEED_HIT_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("diag", "<i4"), ("qpos", "<u4")])
-CANDIDATE_DTYPE = np.dtype([("query", "<u4"), ("target", "<u4"), ("hits", "<u4"), ("diag_score", "<i4"),
-                            ("best_diag", "<i8"), ("t_lo", "<u4"), ("t_hi", "<u4")])
+from .dtypes import CANDIDATE_DTYPE, HIT_DTYPE, LANE_DTYPE, PAIR_DTYPE, SEED_HIT_DTYPE  # noqa: E402,F401
 PREFILTER_STATS_FIELDS = ("targets_hit", "targets_evaluated", "diagonals_scored", "chains_used", "candidates",
                           "candidates_capped", "hits_rejected")
 
@@ -111,6 +111,7 @@ SIGNATURES = {
     "st_plan_profile": (C.c_int, [_P, _u32, _P, _P, _P, _P]),
     "st_plan_destroy": (None, [_P]),
     "st_ungapped_score": (C.c_int, [_P, _u32, _P, _u32, _P]),
+    "st_ungapped_score_slices": (C.c_int, [_P, _u32, _P, _u32, _P]),
     "st_ungapped_hits": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
     "st_ungapped_hits_device": (C.c_int, [_P, _P, _u64, _P, _P, _P, _P, _P]),
     "st_prefilter_gate": (C.c_int, [_P, _P, _u64, _P, _P, _u64, _P, _P]),
@@ -134,9 +135,6 @@ SIGNATURES = {
     "st_sw_score_noalloc": (C.c_int, [_P, _u32, _P, _u32, _i32, _i32, _P, _P]),
     "st_probe_dpx": (C.c_int, [_P, _P]),
     "st_launch_count": (C.c_int, [_P, _P]),
-    "st_pssm_from_msa": (C.c_int, [_P, _u32, _u32, _P, _P, C.c_float, C.c_float, C.c_float, _P, _P]),
-    "st_pssm_batch": (C.c_int, [_P, _P, _P, _P, _u32, _P, _P, C.c_float, C.c_float, C.c_float, _P, _P,
-                                C.c_int]),
 }
 
 

@@ -148,6 +148,14 @@ class Context:
         check(lib.st_db_upload(self._h, ptr(residues) if residues.size else None, ptr(offsets), n))
         self.n_seqs = n
         self.db_lengths = np.diff(offsets).astype(np.uint32)
+        # the host arena stays referenced: lanes built from db_seq() slices point into it
+        self._db_host = (residues, offsets)
+
+    def db_seq(self, i):
+        """Residues of database sequence i as a view of the uploaded host arena (SeedIndex::seq,
+        src/index.rs:1975-1979): the target slice a Lane carries."""
+        res, offs = self._db_host
+        return res[int(offs[i]):int(offs[i + 1])]
 
     def db_info(self):
         """(sequences, residues) of the device database."""
@@ -694,9 +702,12 @@ class QueryProfile:
 
 @dataclass
 class Lane:
-    """One diagonal: database ordinal of the target, diagonal, query window [lo, hi)."""
+    """One diagonal job (src/ungapped.rs:265-270): the target, the diagonal and the query window [lo, hi).
 
-    target: int
+    As in the reference, `target` is a slice of a database sequence: a uint8 view of the host arena that was
+    uploaded (Context.db_seq(i), or any sub-slice of it).  A database ordinal (int) is accepted too."""
+
+    target: object
     diag: int
     lo: int
     hi: int
@@ -719,13 +730,23 @@ class DiagProfile:
 
 
 def score_batch(prof: DiagProfile, lanes, out=None):
-    """out[i] = best ungapped segment score of lanes[i] (src/ungapped.rs:285-386), any number of lanes."""
+    """out[i] = best ungapped segment score of lanes[i] (src/ungapped.rs:285-386), any number of lanes.
+    Lanes whose targets are arena slices go through st_ungapped_score_slices (the reference's Lane as it
+    is); lanes with database ordinals through st_ungapped_score."""
     n = len(lanes)
-    arr = np.zeros(n, dtype=LANE_DTYPE)
-    for i, l in enumerate(lanes):
-        arr[i] = (l.target, l.lo, l.hi, l.diag)
     res = np.zeros(n, dtype=np.int32)
-    if n:
+    if n and isinstance(lanes[0].target, np.ndarray):
+        arr = (_lib.st_lane_slice * n)()
+        for i, l in enumerate(lanes):
+            t = l.target
+            if not isinstance(t, np.ndarray) or t.dtype != np.uint8 or (t.size and not t.flags.c_contiguous):
+                raise TypeError("every lane's target must be a contiguous uint8 slice of the uploaded arena")
+            arr[i] = _lib.st_lane_slice(t.ctypes.data if t.size else 0, t.size, l.diag, l.lo, l.hi)
+        check(lib.st_ungapped_score_slices(prof.qp.ctx.handle, prof.qp.id, arr, n, ptr(res)))
+    elif n:
+        arr = np.zeros(n, dtype=LANE_DTYPE)
+        for i, l in enumerate(lanes):
+            arr[i] = (l.target, l.lo, l.hi, l.diag)
         check(lib.st_ungapped_score(prof.qp.ctx.handle, prof.qp.id, ptr(arr), n, ptr(res)))
     if out is not None:
         out[:n] = res

@@ -21,7 +21,9 @@
 // GPU that loads this library until the process exits; it bounds the target
 // length to kNoAllocMaxCols residues.  All calls on a device share it and it
 // keeps whatever the last call wrote.  Nothing in it has to start at zero: a
-// call writes every column it reads back before reading it.  Calls whose
+// call reads an entry back only after writing it in the same call (a query of
+// more than 256 rows streams at least 32 columns per pass, so the boundary of
+// a column is written before the next pass reaches it).  Calls whose
 // kernels overlap on the GPU (for example on two streams without an event
 // between them) race on the array and may return wrong scores; issue them on
 // one stream or order them.
@@ -62,6 +64,13 @@ __global__ void __launch_bounds__(32) sw_noalloc_kernel(const int32_t* __restric
     return;
   }
   const int P = (m + G * R - 1) / (G * R);
+  // Columns streamed per pass: lane 0 reads column c's boundary of pass p at
+  // step p*W + c, and lane G-1 wrote it at step (p-1)*W + c + G-1, so W must be
+  // at least G.  Against a target shorter than G, a multi-pass query streams
+  // idle columns [n, G) after the real ones; they carry the sentinel residue,
+  // never count toward the maximum, never touch the boundary array, and the
+  // state they leave is reset when the next pass starts at column 0.
+  const int W = P > 1 ? max(n, G) : n;
   const int32_t E0 = max(wsub(0, open), wsub(kNeg32, ext));  // first-column E, first-row F
   const int32_t F0 = E0;
   int32_t Hp[R], E[R];
@@ -76,7 +85,7 @@ __global__ void __launch_bounds__(32) sw_noalloc_kernel(const int32_t* __restric
   int pass = 0;
   uint32_t nxt = kSentinel;
   if (lane == 0) nxt = min(static_cast<uint32_t>(t[0]), static_cast<uint32_t>(kSentinel));
-  const int steps = P * n + G - 1;
+  const int steps = P * W + G - 1;
   for (int s = 0; s < steps; ++s) {
     int32_t hin = __shfl_up_sync(FULL, h_bot, 1);
     int32_t fin = __shfl_up_sync(FULL, f_out, 1);
@@ -85,10 +94,11 @@ __global__ void __launch_bounds__(32) sw_noalloc_kernel(const int32_t* __restric
       if (pass < P) {
         rin = nxt;
         int cn = c + 1;
-        const bool last = (cn == n);
+        const bool last = (cn == W);
         if (last) cn = 0;
-        nxt = (last && pass + 1 >= P) ? kSentinel : min(static_cast<uint32_t>(t[cn]), static_cast<uint32_t>(kSentinel));
-        if (pass > 0) {
+        nxt = ((last && pass + 1 >= P) || cn >= n) ? kSentinel
+                                                   : min(static_cast<uint32_t>(t[cn]), static_cast<uint32_t>(kSentinel));
+        if (pass > 0 && c < n) {
           const int2 bv = bnd[c];
           hin = bv.x;
           fin = bv.y;
@@ -113,7 +123,7 @@ __global__ void __launch_bounds__(32) sw_noalloc_kernel(const int32_t* __restric
     }
     const int pp = pass < P ? pass : P - 1;
     const int row0 = pp * G * R + lane * R;
-    const bool live = (c >= 0) && (pass < P);
+    const bool live = (c >= 0) && (c < n) && (pass < P);
     int32_t hd = hup_prev;
     int32_t F = fin;
     int32_t lmax = 0;
@@ -134,8 +144,8 @@ __global__ void __launch_bounds__(32) sw_noalloc_kernel(const int32_t* __restric
     hup_prev = hin;
     h_bot = Hp[R - 1];
     f_out = F;
-    if (lane == G - 1 && pass + 1 < P && c >= 0) bnd[c] = make_int2(h_bot, f_out);
-    if (++c == n) {
+    if (lane == G - 1 && pass + 1 < P && c >= 0 && c < n) bnd[c] = make_int2(h_bot, f_out);
+    if (++c == W) {
       c = 0;
       ++pass;
     }

@@ -276,6 +276,10 @@ struct st_ctx {
   DevMem db_arena, db_off, db_len;
   std::vector<uint32_t> h_db_len;
   std::vector<uint64_t> h_db_off;  // arena offset of each sequence (multiple of 16)
+  // the caller's host arena at the last st_db_upload: its address and offsets[0..n_seqs], so that a
+  // lane given as a slice of that arena (the reference's Lane) maps back to a sequence
+  uintptr_t h_src_base = 0;
+  std::vector<uint64_t> h_src_off;
   uint32_t n_seqs = 0;
   uint32_t max_len = 0;  // longest sequence
   uint64_t n_res = 0;
@@ -521,6 +525,7 @@ static DeviceProfiles prof_view(st_ctx* c) {
 
 static int g_class_smem[kNumClasses];  // dynamic shared memory each 16-bit class may use
 static int g_ung_smem = 0;              // dynamic shared memory the ungapped kernels may use
+static int g_ung_split_smem = 0;        // the same for ungapped_hits_split_kernel (more static shared memory)
 static int g_gate_smem = 0;             // dynamic shared memory of the prefilter segment kernel
 
 static int set_smem_limits(int device) {
@@ -542,6 +547,11 @@ static int set_smem_limits(int device) {
   ST_CUDA(cudaFuncGetAttributes(&fa_r, reinterpret_cast<const void*>(ungapped_hits_refill_kernel)));
   g_ung_smem = std::min<int>(g_ung_smem, optin - static_cast<int>(fa_r.sharedSizeBytes));
   ST_CUDA(cudaFuncSetAttribute(ungapped_hits_refill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g_ung_smem));
+  cudaFuncAttributes fa_s;
+  ST_CUDA(cudaFuncGetAttributes(&fa_s, reinterpret_cast<const void*>(ungapped_hits_split_kernel)));
+  g_ung_split_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(fa_s.sharedSizeBytes));
+  ST_CUDA(cudaFuncSetAttribute(ungapped_hits_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               g_ung_split_smem));
   cudaFuncAttributes fa_g;
   ST_CUDA(cudaFuncGetAttributes(&fa_g, reinterpret_cast<const void*>(gate_score_kernel)));
   g_gate_smem = std::min<int>(kMaxSmem, optin - static_cast<int>(fa_g.sharedSizeBytes));
@@ -710,6 +720,8 @@ extern "C" int st_db_upload(st_ctx* c, const uint8_t* residues, const uint64_t* 
   c->max_len = len.empty() ? 0 : *std::max_element(len.begin(), len.end());
   c->h_db_len = std::move(len);
   c->h_db_off.assign(off.begin(), off.end() - 1);
+  c->h_src_base = reinterpret_cast<uintptr_t>(residues);
+  c->h_src_off.assign(offsets, offsets + n_seqs + 1);
   c->n_seqs = n_seqs;
   c->n_res = offsets[n_seqs] - offsets[0];
   c->has_db = true;
@@ -2787,7 +2799,12 @@ static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n,
     return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", max_m ? max_m : c->max_m);
   const uint64_t grid = (n + kUngChunk - 1) / kUngChunk;
   if (grid > 0x7FFFFFFFull) return fail(ST_EINVAL, "too many ungapped jobs");
-  if (hits)
+  // hit lists: the run's work split evenly over the lanes; the per-lane refill form for queries whose staged
+  // rows do not fit beside the split kernel's static shared memory (or when ST_UNGAPPED_REFILL=1)
+  static const bool force_refill = env_u64("ST_UNGAPPED_REFILL", 0) != 0;
+  if (hits && !force_refill && smem <= static_cast<size_t>(g_ung_split_smem))
+    ungapped_hits_split_kernel<<<static_cast<uint32_t>(grid), kUngSplitLanes, smem, c->stream>>>(prm);
+  else if (hits)
     ungapped_hits_refill_kernel<<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
   else
     ungapped_kernel<false><<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);
@@ -2832,6 +2849,60 @@ extern "C" int st_ungapped_score(st_ctx* c, uint32_t profile, const st_lane* lan
   ST_CUDA(cudaMemcpyAsync(out, d_out, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, c->stream));
   ST_CUDA(cudaStreamSynchronize(c->stream));
   return ST_OK;
+}
+
+// The reference's Lane as it is (src/ungapped.rs:265-270): the target is a
+// slice of the database arena that the caller gave st_db_upload (prefilter.rs
+// builds lanes from index.seq(tid), src/prefilter.rs:1563-1568).  Each slice is
+// mapped back to its sequence by a binary search of the caller's offsets; a
+// slice that starts `a` residues into its sequence scores diagonal diag + a of
+// the whole sequence over the same query window, which reads the same residues
+// (slice[q + diag] = sequence[q + diag + a]).
+extern "C" int st_ungapped_score_slices(st_ctx* c, uint32_t profile, const st_lane_slice* lanes, uint32_t n,
+                                        int32_t* out) {
+  CTX_GUARD(c);
+  if (n && (!lanes || !out)) return fail(ST_EINVAL, "st_ungapped_score_slices: null argument");
+  if (!c->has_db) return fail(ST_ESTATE, "no target database uploaded (st_db_upload)");
+  ST_TRY(check_profile(c, profile));
+  if (n == 0) return ST_OK;
+  const int64_t m = c->profs[profile].m;
+  std::vector<st_lane> mapped(n);
+  bool any_live = false;
+  const uint64_t* so = c->h_src_off.data();
+  const uint64_t first = so[0], last = so[c->n_seqs];
+  for (uint32_t i = 0; i < n; ++i) {
+    const st_lane_slice& l = lanes[i];
+    // diag_range of the slice (src/ungapped.rs:38-46); score_batch requires lo..hi inside it
+    const int64_t len = static_cast<int64_t>(l.len);
+    const int64_t rlo = std::max<int64_t>(-l.diag, 0);
+    const int64_t rhi = std::min<int64_t>(m, len - l.diag);
+    if (l.lo >= l.hi || rhi <= rlo) {
+      mapped[i] = st_lane{0, 0, 0, 0};  // an empty window scores 0 (kadane_score's best starts at 0)
+      continue;
+    }
+    if (static_cast<int64_t>(l.lo) < rlo || static_cast<int64_t>(l.hi) > rhi)
+      return fail(ST_EINVAL, "lane %u: window [%llu, %llu) outside the diagonal's range [%lld, %lld)", i,
+                  static_cast<unsigned long long>(l.lo), static_cast<unsigned long long>(l.hi),
+                  static_cast<long long>(rlo), static_cast<long long>(rhi));
+    const uintptr_t p = reinterpret_cast<uintptr_t>(l.target);
+    if (!l.target || p < c->h_src_base || p - c->h_src_base < first || p - c->h_src_base + l.len > last)
+      return fail(ST_EINVAL, "lane %u: the target slice is not inside the database arena given to st_db_upload", i);
+    const uint64_t pos = p - c->h_src_base;
+    // the last sequence starting at or before pos
+    const uint64_t* it = std::upper_bound(so, so + c->n_seqs + 1, pos);
+    const uint32_t s = static_cast<uint32_t>(it - so - 1);
+    if (s >= c->n_seqs || pos + l.len > so[s + 1])
+      return fail(ST_EINVAL, "lane %u: the target slice crosses the end of database sequence %u", i, s);
+    const int64_t diag = l.diag + static_cast<int64_t>(pos - so[s]);
+    if (diag < INT32_MIN || diag > INT32_MAX) return fail(ST_EINVAL, "lane %u: diagonal out of range", i);
+    mapped[i] = st_lane{s, static_cast<uint32_t>(l.lo), static_cast<uint32_t>(l.hi), static_cast<int32_t>(diag)};
+    any_live = true;
+  }
+  if (!any_live) {
+    std::fill(out, out + n, 0);
+    return ST_OK;
+  }
+  return st_ungapped_score(c, profile, mapped.data(), n, out);
 }
 
 // Per-(query, target) runs of hits (consecutive hits with the same query and

@@ -93,6 +93,13 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
   const int cstart = static_cast<int>(c_lo);
   const int ncols = static_cast<int>(c_hi - c_lo);
   const int P = (m + G * R - 1) / (G * R);
+  // Columns streamed per pass.  Lane 0 reads column c's boundary of pass p at
+  // step p*W + c; lane G-1 wrote it at step (p-1)*W + c + G-1, which is earlier
+  // only when W >= G.  A multi-pass query against fewer than G columns streams
+  // idle columns [ncols, G) after the real ones: they carry the sentinel
+  // residue, never count toward the maximum and never touch the boundary, and
+  // the state they leave is reset when the next pass starts at column 0.
+  const int W = P > 1 ? max(ncols, G) : ncols;
   const uint8_t* t = prm.db.arena + prm.db.offset[tid];
   const int32_t* prof = prm.prof.p32[q];
   const uint32_t stride = prm.prof.stride32[q];
@@ -118,7 +125,7 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     return min(static_cast<uint32_t>(__ldg(t + jj)), static_cast<uint32_t>(kSentinel));
   };
   if (lane == 0) nxt = tcol(cstart);
-  const int steps = P * ncols + G - 1;
+  const int steps = P * W + G - 1;
 
   for (int s = 0; s < steps; ++s) {
     int32_t hin = __shfl_up_sync(FULL, h_bot, 1);
@@ -128,10 +135,10 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
       if (pass < P) {
         rin = nxt;
         int cn = c + 1;
-        bool last = (cn == ncols);
+        bool last = (cn == W);
         if (last) cn = 0;
-        nxt = (last && pass + 1 >= P) ? kSentinel : tcol(cstart + cn);
-        if (pass > 0) {
+        nxt = ((last && pass + 1 >= P) || cn >= ncols) ? kSentinel : tcol(cstart + cn);
+        if (pass > 0 && c < ncols) {
           int2 bv = bnd[c];
           hin = bv.x;
           fin = bv.y;
@@ -170,7 +177,7 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
       S[4] = b.x; S[5] = b.y; S[6] = b.z; S[7] = b.w;
     }
     const int col = cstart + c;  // target column (0-based) of this lane
-    const bool live = (c >= 0) && (pass < P);
+    const bool live = (c >= 0) && (c < ncols) && (pass < P);
     int32_t hd = hup_prev;
     int32_t F = fin;
     int32_t lmax = 0;
@@ -213,8 +220,8 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     hup_prev = hin;
     h_bot = Hp[R - 1];
     f_out = F;
-    if (lane == G - 1 && pass + 1 < P && c >= 0) bnd[c] = make_int2(h_bot, f_out);
-    if (++c == ncols) {
+    if (lane == G - 1 && pass + 1 < P && c >= 0 && c < ncols) bnd[c] = make_int2(h_bot, f_out);
+    if (++c == W) {
       c = 0;
       ++pass;
     }

@@ -310,4 +310,238 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
   }
 }
 
+
+// Hits with the work of a query run split evenly over the CTA's lanes.
+//
+// Per run of one query inside the CTA's chunk: the profile is staged as
+// above; every hit of the run is decoded once (diag_range, the first aligned
+// target vector, the number of 16-byte vectors) into shared memory, and an
+// exclusive scan of the vector counts lays the run's vectors end to end.  Lane
+// t then scores vectors [t*S, (t+1)*S) of that stream, S = ceil(V / lanes), so
+// every lane does the same work whatever the diagonal lengths; a diagonal may
+// be split over consecutive lanes.
+//
+// Splitting is exact.  With u = max(cur, 0) carried (u' = max(u + s, 0)) and
+// any u_in >= 0, the states after k cells are u_k = max(u_in + P_k, z_k), where
+// P_k is the k-th prefix sum of the cell scores and z_k the state of the same
+// cells scored from u = 0; the best over the piece is max(u_in + C, D) with
+// C = max_k P_k and D = max_k z_k.  A lane that starts inside a diagonal scores
+// its piece from 0 (giving z, D) and from a large H (u never reaches 0 from
+// there, so that run carries H + P_k and its maximum H + C), and stores
+// (A = P_last, B = z_last, C, D).  After one barrier the lane that started the
+// diagonal folds the summaries of the lanes after it in order: best = max(best,
+// u + C, D), u = max(u + A, B), which is Kadane's result over the whole
+// diagonal (src/ungapped.rs:53-62).  Rows outside int8 take the plain loop.
+constexpr int kUngSplitLanes = 256;
+constexpr int32_t kUngH = 1 << 24;  // > 127 * rows of any staged profile: H + P_k stays positive
+
+__global__ void __launch_bounds__(kUngSplitLanes) ungapped_hits_split_kernel(const UngappedParams prm) {
+  extern __shared__ __align__(16) int8_t smem[];
+  __shared__ unsigned long long s_run_end;
+  __shared__ unsigned long long s_vec0[kUngChunk];  // arena offset of the hit's first (aligned) vector
+  __shared__ int32_t s_qa0[kUngChunk];               // query row of that vector's first byte
+  __shared__ uint32_t s_vstart[kUngChunk + 1];       // exclusive scan of the vector counts
+  __shared__ int4 s_sum[kUngSplitLanes];             // (A, B, C, D) of a lane's leading piece
+  __shared__ uint32_t s_warp[kUngSplitLanes / 32];
+  const HitRec* hits = reinterpret_cast<const HitRec*>(prm.jobs);
+  const uint32_t stride = prm.max_m_pad;
+  int8_t* base = smem + 16;
+  const int t = threadIdx.x;
+  const int lane = t & 31, warp = t >> 5;
+  const uint64_t c0 = static_cast<uint64_t>(blockIdx.x) * kUngChunk;
+  if (c0 >= prm.n) return;
+  const uint64_t c1 = u64min(prm.n, c0 + kUngChunk);
+  uint64_t a = c0;
+  while (a < c1) {
+    const uint32_t q = hits[a].query;
+    if (t < 32) {
+      uint64_t e = a;
+      for (;;) {
+        const uint64_t k = e + lane;
+        const bool same = (k < c1) && (hits[k].query == q);
+        const uint32_t ball = __ballot_sync(0xFFFFFFFFu, same);
+        if (ball != 0xFFFFFFFFu) {
+          e += __ffs(~ball) - 1;
+          break;
+        }
+        e += 32;
+      }
+      if (t == 0) s_run_end = e;
+    }
+    const uint32_t m = prm.prof.qlen[q];
+    const uint32_t pstride = prm.prof.stride8[q];
+    const int8_t* src = prm.prof.p8[q];
+    for (uint32_t idx = t; idx < kProfRows * (stride / 16); idx += blockDim.x) {
+      const uint32_t r = idx / (stride / 16);
+      const uint32_t i = (idx - r * (stride / 16)) * 16;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (i < pstride) v = *reinterpret_cast<const uint4*>(src + static_cast<size_t>(r) * pstride + i);
+      *reinterpret_cast<uint4*>(base + static_cast<size_t>(r) * stride + i) = v;
+    }
+    if (t < 16) smem[t] = 0;
+    __syncthreads();
+    const uint64_t b = s_run_end;
+    const uint32_t nb = static_cast<uint32_t>(b - a);
+    const HitRec* run = hits + a;
+    int32_t* out = prm.out + a;
+    if (prm.prof.fits8[q] == 0) {
+      // rows outside int8: the int32 profile, every cell tested against the window
+      const int32_t* p32 = prm.prof.p32[q];
+      const int32_t s32 = static_cast<int32_t>(prm.prof.stride32[q]);
+      for (uint32_t j = t; j < nb; j += blockDim.x) {
+        const HitRec h = run[j];
+        const int64_t n = prm.db.length[h.target];
+        const int64_t lo = i64max(-static_cast<int64_t>(h.diag), 0), hi = i64min(m, n - h.diag);
+        int32_t cur = 0, best = 0;
+        const uint8_t* tp = prm.db.arena + prm.db.offset[h.target];
+        for (int64_t i = lo; i < hi; ++i) {
+          const uint32_t r = tp[i + h.diag];
+          cur = wadd(max(cur, 0), __ldg(p32 + static_cast<int32_t>(r) * s32 + static_cast<int32_t>(i)));
+          best = max(best, cur);
+        }
+        out[j] = best;
+      }
+      __syncthreads();
+      a = b;
+      continue;
+    }
+    // decode: four consecutive hits per lane, so the scan below is a lane-local sum plus a block scan
+    uint32_t cnt[4];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t j = 4 * t + i;
+      cnt[i] = 0;
+      if (j < nb) {
+        const HitRec h = run[j];
+        const int64_t n = prm.db.length[h.target];
+        // diag_range, src/ungapped.rs:38-46
+        const int64_t lo = i64max(-static_cast<int64_t>(h.diag), 0), hi = i64min(m, n - h.diag);
+        if (hi > lo) {
+          const int32_t p0 = static_cast<int32_t>(lo) + h.diag, p1 = static_cast<int32_t>(hi) + h.diag;
+          const int32_t pa = p0 & ~15;
+          s_vec0[j] = prm.db.offset[h.target] + static_cast<uint64_t>(pa);
+          s_qa0[j] = pa - h.diag;
+          cnt[i] = static_cast<uint32_t>((p1 - pa + 15) >> 4);
+        } else {
+          out[j] = 0;  // an empty diagonal scores 0
+        }
+      }
+      tot += cnt[i];
+    }
+    // block-wide exclusive scan of the lanes' totals
+    uint32_t incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0, V = 0;
+#pragma unroll
+    for (int w = 0; w < kUngSplitLanes / 32; ++w) {
+      const uint32_t x = s_warp[w];
+      wbase += w < warp ? x : 0;
+      V += x;
+    }
+    uint32_t run_start = wbase + incl - tot;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t j = 4 * t + i;
+      if (j < nb) s_vstart[j] = run_start;
+      run_start += cnt[i];
+    }
+    if (t == 0) s_vstart[nb] = V;
+    __syncthreads();
+    const uint32_t S = (V + kUngSplitLanes - 1) / kUngSplitLanes;
+    const uint32_t v0 = static_cast<uint32_t>(t) * S;
+    const uint32_t v1 = min(v0 + S, V);
+    bool tail = false;  // this lane started a diagonal that continues past its range
+    uint32_t tail_h = 0;
+    int32_t tail_u = 0, tail_b = 0;
+    if (v0 < v1) {
+      // the hit holding vector v0: the last one whose first vector is at or before v0 (hits with no vectors
+      // share their successor's start and are passed over)
+      uint32_t lo_i = 0, hi_i = nb;  // s_vstart[lo_i] <= v0 < s_vstart[hi_i]
+      while (hi_i - lo_i > 1) {
+        const uint32_t mid = (lo_i + hi_i) >> 1;
+        if (s_vstart[mid] <= v0) lo_i = mid; else hi_i = mid;
+      }
+      uint32_t h = lo_i;
+      while (s_vstart[h + 1] <= v0) ++h;
+      uint32_t hend = s_vstart[h + 1];
+      uint32_t w0 = v0 - s_vstart[h];
+      bool head = w0 > 0;  // a piece of a diagonal that an earlier lane started
+      const uint8_t* tp = prm.db.arena + s_vec0[h] + 16u * w0;
+      const int8_t* rowbase = base + s_qa0[h] + 16 * static_cast<int32_t>(w0);
+      int32_t u = 0, best = 0, uh = kUngH, bh = 0;
+      for (uint32_t v = v0; v < v1;) {
+        const uint4 vec = *reinterpret_cast<const uint4*>(tp);
+        const uint32_t w[4] = {vec.x, vec.y, vec.z, vec.w};
+        // every cell of a whole vector is scored: cells outside the window score 0 (guard bytes and padding
+        // of the staged rows, sentinel residues past the target), which cannot change Kadane's result
+#pragma unroll
+        for (int bb = 0; bb < 16; bb += 2) {
+          const uint32_t r0 = (w[bb >> 2] >> ((bb & 3) * 8)) & 0xFFu;
+          const uint32_t r1 = (w[bb >> 2] >> (((bb + 1) & 3) * 8)) & 0xFFu;
+          const int32_t s0 = rowbase[static_cast<int32_t>(r0 * stride) + bb];
+          const int32_t s1 = rowbase[static_cast<int32_t>(r1 * stride) + bb + 1];
+          const int32_t u0 = __viaddmax_s32_relu(u, s0, 0);
+          u = __viaddmax_s32_relu(u0, s1, 0);
+          best = __vimax3_s32(best, u0, u);
+          const int32_t h0 = uh + s0;
+          uh = h0 + s1;
+          bh = __vimax3_s32(bh, h0, uh);
+        }
+        ++v;
+        tp += 16;
+        rowbase += 16;
+        if (v == hend) {
+          if (head) {
+            s_sum[t] = make_int4(uh - kUngH, u, bh - kUngH, best);
+            head = false;
+          } else {
+            out[h] = best;
+          }
+          ++h;
+          while (h < nb && s_vstart[h + 1] == s_vstart[h]) ++h;
+          if (v < v1) {
+            hend = s_vstart[h + 1];
+            tp = prm.db.arena + s_vec0[h];
+            rowbase = base + s_qa0[h];
+            u = 0;
+            best = 0;
+            uh = kUngH;
+            bh = 0;
+          }
+        }
+      }
+      if (v1 < hend) {  // the range ended inside diagonal h
+        if (head) {
+          s_sum[t] = make_int4(uh - kUngH, u, bh - kUngH, best);
+        } else {
+          tail = true;
+          tail_h = h;
+          tail_u = u;
+          tail_b = best;
+        }
+      }
+    }
+    __syncthreads();
+    if (tail) {
+      const uint32_t t_last = (s_vstart[tail_h + 1] - 1) / S;
+      int32_t u = tail_u, best = tail_b;
+      for (uint32_t tt = t + 1; tt <= t_last; ++tt) {
+        const int4 sm = s_sum[tt];
+        best = max(best, max(u + sm.z, sm.w));
+        u = max(u + sm.x, sm.y);
+      }
+      out[tail_h] = best;
+    }
+    __syncthreads();
+    a = b;
+  }
+}
+
 }  // namespace st

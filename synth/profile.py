@@ -1,13 +1,15 @@
-"""PSSM query profiles (reference src/profile.rs).
+"""PSSM query profiles (reference src/profile.rs): an input generator.
 
 parse_msa restates src/profile.rs:372-449; the numeric PSSM construction runs
-in the native library (st_pssm_from_msa), which restates
-Profile::from_numeric_msa in the reference's f32 operation order.
+in synth/libsynth.so (st_pssm_from_msa, synth/pssm.cpp), which restates
+Profile::from_numeric_msa in the reference's f32 operation order.  The kernels
+take any int32 score rows; this module makes the PSSM rows of the synthetic
+workloads and is pinned by the reference's demo/family.pssm.
 """
 import numpy as np
 
 from . import _lib
-from .matrix import AA2NUM, ALPHABET_SIZE, GAP, PROFILE_AA_SIZE, blosum62
+from sabertooth_b200.matrix import AA2NUM, ALPHABET_SIZE, GAP, PROFILE_AA_SIZE, blosum62
 
 PCA_DEFAULT, PCB_DEFAULT, SCORE_BIAS_DEFAULT = 1.0, 1.5, 0.0  # src/profile.rs:56-65
 

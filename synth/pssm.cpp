@@ -1,4 +1,5 @@
-// Host-side row preparation: PSSM construction from a numeric MSA, restating
+// Input generation (synthetic workloads, golden fixtures): PSSM construction
+// from a numeric MSA, restating
 // the reference's Profile::from_numeric_msa (src/profile.rs:90-341) step for
 // step in single precision and in the reference's operation order, so the
 // resulting int8 PSSM is the one the reference would build.  Compiled without
@@ -8,7 +9,7 @@
 #include <cstring>
 #include <vector>
 
-#include "../../include/sabertooth_b200_host.h"
+#include "pssm.h"
 
 namespace {
 

@@ -1,12 +1,13 @@
 /*
- * sabertooth_b200 — host-side row preparation utilities (no GPU).
+ * synth — PSSM construction for the synthetic workloads (host only, no GPU).
  *
- * These build the score rows the kernels consume, following the reference's
- * host code so synthetic workloads and golden fixtures use the same inputs as
- * the reference would.  They are part of libsabertooth_b200.so.
+ * Builds int8 PSSM rows from family MSAs, following the reference's host code
+ * so that synthetic workloads and golden fixtures use the same inputs as the
+ * reference would.  Built into synth/libsynth.so, an input generator for the
+ * tests and the benchmark; the product library does not contain it.
  */
-#ifndef SABERTOOTH_B200_HOST_H
-#define SABERTOOTH_B200_HOST_H
+#ifndef SYNTH_PSSM_H
+#define SYNTH_PSSM_H
 
 #include <stdint.h>
 

@@ -11,7 +11,7 @@ distributions and residue composition:
   otherwise draws from P(b|a) = prob[a][b] / p_back[a] (src/matrix.rs:137-151),
   with geometric indels;
 * PSSM queries from 50-member family MSAs (40-90% identity) through the
-  reference's PSSM construction (sabertooth_b200.profile).
+  reference's PSSM construction (synth.profile).
 
 Random numbers come from SplitMix64 (src/evalue.rs:54-75) evaluated in counter
 form: output i of a stream seeded s is mix(s + (i+1)*gamma), so whole arrays
@@ -21,7 +21,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .matrix import PROFILE_AA_SIZE, blosum62
+from sabertooth_b200.matrix import PROFILE_AA_SIZE, blosum62
 
 GAMMA = np.uint64(0x9E3779B97F4A7C15)
 M1 = np.uint64(0xBF58476D1CE4E5B9)
@@ -362,7 +362,7 @@ class HitWorkload:
 
 def config2(seed=0, n_queries=1000, n_targets=374_000, n_hits=20_000_000, homolog_frac=0.10, homolog_hit_frac=0.30,
             model=None):
-    from ._lib import HIT_DTYPE
+    from sabertooth_b200.dtypes import HIT_DTYPE
     model = model or Model()
     rng = Rng(seed)
     ql = lognormal_lengths(rng, n_queries, 250, 0.5, 30, 1000)
@@ -431,7 +431,7 @@ def seed_hits(seed=0, n_queries=1000, n_targets=374_000, n_hits=20_000_000, homo
     (substitutions keep `keep` of the sites); homolog hits lie on either
     piece's diagonal at a position inside that piece, the rest are uniform over
     random (query, target, valid diagonal, position on it)."""
-    from ._lib import SEED_HIT_DTYPE
+    from sabertooth_b200.dtypes import SEED_HIT_DTYPE
     model = model or Model()
     rng = Rng(seed)
     ql = lognormal_lengths(rng, n_queries, 250, 0.5, 30, 1000)

@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = set()
-    for h in ("sabertooth_b200.h", "sabertooth_b200_host.h"):
+    for h in ("sabertooth_b200.h",):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"\b(st_[a-z0-9_]+)\s*\(", text):

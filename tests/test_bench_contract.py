@@ -30,3 +30,7 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert "workload" in d["config"]
+    # the arm runs no product code: only the oracle and the input generator are mapped
+    assert d["libraries_mapped"], d
+    assert all(not x.endswith("libsabertooth_b200.so") for x in d["libraries_mapped"]), d["libraries_mapped"]
+    assert "oracle/liboracle.so" in d["libraries_mapped"]

@@ -15,7 +15,7 @@ import numpy as np
 
 import oracle.oracle as O
 from sabertooth_b200 import blosum62
-from sabertooth_b200.profile import Profile
+from synth.profile import Profile
 from tests.refrng import SplitMix64
 
 MSA_A = ">a\nMKVLLACDEFGHIKLMNPQRSTVWYACDEFGHIK\n>b\nMKILLSCDEFGHLKLMNPQRSTVWFACDEYGHIK\n"

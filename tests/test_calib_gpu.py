@@ -11,8 +11,8 @@ import pytest
 
 import oracle.oracle as O
 from sabertooth_b200 import GapCosts, blosum62
-from sabertooth_b200 import workloads as W
-from sabertooth_b200.profile import Profile
+from synth import workloads as W
+from synth.profile import Profile
 from tests.test_calib import MSA_A, MSA_B
 
 pytestmark = pytest.mark.gpu

@@ -12,7 +12,7 @@ import pytest
 
 import oracle.oracle as O
 from sabertooth_b200 import blosum62, encode
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from tests.seedhits import brute_seed_hits, default_params, py_prefilter, similar_kmer_count
 
 

@@ -12,7 +12,7 @@ import pytest
 
 from oracle import oracle as O
 from sabertooth_b200 import GapCosts, PrefilterParams, blosum62, encode
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from sabertooth_b200._lib import SEED_HIT_DTYPE, StError
 from tests.seedhits import brute_seed_hits, default_params
 

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from sabertooth_b200 import blosum62, encode
-from sabertooth_b200.profile import Profile, parse_msa
+from synth.profile import Profile, parse_msa
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 

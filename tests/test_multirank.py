@@ -1,6 +1,6 @@
-"""The N > 1 path of bench.py on CPU: two ranks over gloo (127.0.0.1). Each rank scores its own
-instance of the workload (seed + rank: weak scaling, no collective on the data path); the job's
-step time is the slowest rank's and its work the sum of the ranks'."""
+"""The N > 1 path of bench.py on CPU: two ranks over gloo (127.0.0.1). Every rank builds the same
+config-3 workload and takes the pairs whose target lies in its residue-balanced shard; the shares
+partition the batch, and the job's step time is the slowest rank's (the max reduction of bench.py)."""
 import os
 import socket
 import sys
@@ -34,18 +34,25 @@ def _worker(rank, world, port, out):
 
     class A:
         scale, seed = 0.002, 5
-    w = bench.make_workload(A, r)
-    ms, cells = bench.combine_ranks(10.0 + r, w.cells(), "cpu")
-    out[rank] = (ms, cells, w.cells(), int(sum(len(r) for r in w.rows)))
+    w = bench.make_workload(A, 0)
+    from sabertooth_b200.dtypes import PAIR_DTYPE
+    from sabertooth_b200.shard import ShardMap
+    pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
+    pairs["profile"] = w.pair_q
+    pairs["target"] = w.pair_t
+    idx, local = ShardMap.of(w.db_offsets, world).route(pairs, r)
+    ms, cells = bench.combine_ranks(10.0 + r, len(idx), "cpu")
+    out[rank] = (ms, cells, w.n_pairs, idx.tolist())
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_two_ranks_weak_scaling_max_over_ranks():
+def test_two_ranks_split_one_batch_by_target_shard():
     port = _free_port()
     out = mp.Manager().dict()
     mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
-    (ms0, c0, own0, sig0), (ms1, c1, own1, sig1) = out[0], out[1]
+    (ms0, c0, n0, idx0), (ms1, c1, n1, idx1) = out[0], out[1]
     assert ms0 == ms1 == 11.0  # the slowest rank's step time
-    assert c0 == c1 == float(own0 + own1)  # the whole job's work
-    assert sig0 != sig1  # each rank scores its own instance (seed + rank)
+    assert n0 == n1 and c0 == c1 == float(n0)  # the same batch on both ranks, split between them
+    assert len(idx0) and len(idx1) and not set(idx0) & set(idx1)
+    assert sorted(idx0 + idx1) == list(range(n0))

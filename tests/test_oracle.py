@@ -156,7 +156,7 @@ def test_diag_range():
 def test_striped_cpu_baseline_equals_scalar_oracle():
     """The AVX2 restatement of the reference's CPU path (the timed CPU baseline) gives the oracle's scores,
     including u8 headroom fallbacks, i16 saturation and gap costs that force the scalar path."""
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     m = blosum62()
     rng = XorShift(777)
     rows_list, targets, pq, pt = [], [], [], []
@@ -190,7 +190,7 @@ def test_avx2_ungapped_baseline_equals_scalar_kadane():
     """The AVX2 restatement of the reference's batched Kadane (the CPU baseline of ungapped scoring)
     gives the scalar oracle's score on every hit: BLOSUM62 rows on the u8 path, rows with scores
     high enough to saturate u8 (rescored), and PSSM-like rows outside the u8 range (scalar)."""
-    from sabertooth_b200 import workloads as W
+    from synth import workloads as W
     w = W.config2(seed=7, n_queries=40, n_targets=3000, n_hits=60_000)
     targets = [w.db_residues[int(a):int(b)] for a, b in zip(w.db_offsets[:-1], w.db_offsets[1:])]
     rows = list(w.rows)

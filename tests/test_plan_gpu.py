@@ -4,7 +4,7 @@ import pytest
 
 from oracle import oracle as O
 from sabertooth_b200 import GapCosts
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from sabertooth_b200._lib import PAIR_DTYPE
 
 pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("planner")]

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from sabertooth_b200 import GapCosts, PrefilterParams, SearchServer, blosum62
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from sabertooth_b200._lib import PAIR_DTYPE, check, lib, ptr
 
 pytestmark = pytest.mark.gpu

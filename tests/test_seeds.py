@@ -17,7 +17,7 @@ import numpy as np
 
 import oracle.oracle as O
 from sabertooth_b200 import blosum62, encode
-from sabertooth_b200.profile import Profile
+from synth.profile import Profile
 from tests.refrng import SplitMix64
 from tests.seedhits import default_params
 

@@ -13,9 +13,9 @@ import pytest
 
 from oracle import oracle as O
 from sabertooth_b200 import GapCosts, PrefilterParams, blosum62, encode
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from sabertooth_b200._lib import StError
-from sabertooth_b200.profile import Profile
+from synth.profile import Profile
 from tests.seedhits import default_params
 
 pytestmark = pytest.mark.gpu

@@ -7,7 +7,7 @@ import pytest
 
 from oracle import oracle as O
 from sabertooth_b200 import GapCosts, Server
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 
 pytestmark = pytest.mark.gpu
 

@@ -12,7 +12,7 @@ import pytest
 
 from oracle import oracle as O
 from sabertooth_b200 import GapCosts, Kernel, QueryProfile, blosum62, encode, tile_classes
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from tests.refrng import XorShift, rand_seq
 
 pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("planner")]

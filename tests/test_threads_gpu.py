@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from sabertooth_b200 import GapCosts
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from sabertooth_b200._lib import HIT_DTYPE, PAIR_DTYPE, check, lib
 
 pytestmark = pytest.mark.gpu

@@ -10,7 +10,7 @@ import pytest
 
 from oracle import oracle as O
 from sabertooth_b200 import DiagProfile, Lane, blosum62, score_batch
-from sabertooth_b200 import workloads as W
+from synth import workloads as W
 from sabertooth_b200.api import diag_range
 from tests.refrng import SplitMix64
 
@@ -136,3 +136,44 @@ def test_unsorted_hits_are_still_exact(ctx):
     assert np.array_equal(got, want)
     for i in ids:
         ctx.free_profile(i)
+
+
+def test_lanes_carry_arena_slices_as_the_reference_builds_them(ctx):
+    """Lanes whose target is a slice of the uploaded arena (src/ungapped.rs:265-270, built from
+    index.seq(tid) in src/prefilter.rs:1563-1568), through st_ungapped_score_slices: whole sequences
+    and sub-slices, every diagonal, sub-windows, empty windows."""
+    rng = SplitMix64(29)
+    m = blosum62()
+    seqs = [np.array([rng.below(21) for _ in range(rng.below(150))], np.uint8) for _ in range(40)]
+    seqs[0] = np.array([rng.below(20) for _ in range(60)], np.uint8)
+    seqs[1] = np.array([rng.below(20) for _ in range(60)], np.uint8)
+    seqs[3] = np.zeros(0, np.uint8)  # an empty sequence inside the arena
+    ctx.upload_db_list(seqs)
+    for case in range(10):
+        q = [rng.below(21) for _ in range(1 + rng.below(90))]
+        rows = m.sequence_rows(q)
+        prof = DiagProfile.build(rows, ctx)
+        lanes, want = [], []
+        for tid in range(len(seqs)):
+            full = ctx.db_seq(tid)
+            assert np.array_equal(full, seqs[tid])
+            a = rng.below(len(full) + 1)
+            b = a + rng.below(len(full) - a + 1)
+            for t in (full, full[a:b]):
+                for d in range(-len(q) - 1, len(t) + 1, 1 + case):
+                    lo, hi = diag_range(len(q), len(t), d)
+                    lanes.append(Lane(t, d, lo, hi))
+                    want.append(O.kadane_score(rows, t, d, lo, hi))
+                    if hi > lo + 2:
+                        lanes.append(Lane(t, d, lo + 1, hi - 1))
+                        want.append(O.kadane_score(rows, t, d, lo + 1, hi - 1))
+        got = score_batch(prof, lanes)
+        assert np.array_equal(got, np.array(want, dtype=np.int32)), case
+        # a buffer that is not the uploaded arena, and a window outside the slice's diagonal range, are errors
+        from sabertooth_b200._lib import StError
+        with pytest.raises(StError, match="not inside the database arena"):
+            score_batch(prof, [Lane(seqs[0].copy(), 0, 0, min(len(q), len(seqs[0])))])
+        t = ctx.db_seq(1)
+        with pytest.raises(StError, match="outside the diagonal's range"):
+            score_batch(prof, [Lane(t[:5], 0, 0, min(len(q), 5) + 1)])
+        prof.qp.free()
