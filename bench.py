@@ -510,6 +510,33 @@ def main():
         plain_s = time.perf_counter() - t0
         plain_gcups = pc / plain_s / 1e9
         del qps
+        # the same drop-in under concurrent callers, as the reference's rayon workers call sw_score_with
+        # (src/search.rs:552-556): one host thread per core, each calling st_sw_score on its share
+        n_thr = os.cpu_count() or 1
+        csample = rng.choice(w.n_pairs, size=min(args.plain_pairs * 8, w.n_pairs), replace=False)
+        cres = np.zeros(len(csample), dtype=np.int64)
+        c_cells = int(sum(len(w.rows[int(w.pair_q[p])]) * targets[int(w.pair_t[p])].size for p in csample))
+
+        def plain_worker(k):
+            s_, k_ = C.c_int32(), C.c_uint32()
+            for i in range(k, len(csample), n_thr):
+                p_ = int(csample[i])
+                t_ = targets[int(w.pair_t[p_])]
+                check(lib.st_sw_score(ctx.handle, int(ids[int(w.pair_q[p_])]), t_.ctypes.data, t_.size, gaps.open,
+                                      gaps.extend, C.byref(s_), C.byref(k_)))
+                cres[i] = s_.value
+
+        ths = [threading.Thread(target=plain_worker, args=(k,)) for k in range(n_thr)]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        conc_s = time.perf_counter() - t0
+        plain_conc = {"value": round(c_cells / conc_s / 1e9, 3), "unit": UNIT, "pairs": int(len(csample)),
+                      "threads": n_thr, "matches_batched": bool(np.array_equal(cres, scores[csample])),
+                      "how": "one host thread per core, each calling st_sw_score (host target, blocking) on its "
+                             "share of the sample; calls run side by side on per-call streams"}
 
         # end to end through the C ABI with host buffers, the database resident (uploaded once, as an index
         # is): every step uploads the query profiles' int32 rows and the pairs from pinned host memory, plans,
@@ -600,6 +627,7 @@ def main():
             "plain": {"value": round(plain_gcups, 3), "unit": UNIT, "pairs": int(len(sample)),
                       "matches_batched": bool(plain_ok),
                       "how": "one st_sw_score call per pair (host target, 2 launches, blocking)"},
+            "plain_concurrent": plain_conc,
             "batched_vs_plain": round(gcups / world / plain_gcups, 1),
             "clocks": clocks,
             "gpu_launches": int(launches),
@@ -1217,121 +1245,133 @@ def hbm_peak_gbs():
 
 
 def serving_measure(ctx, args):
-    """The serving loop (st_server_*) on the long/overflow mix (config 4, BLOSUM62 half): one request
-    per pair (query rows + a target of 1,000-35,000 residues, banded when the length ratio is above 4).
-    Poisson arrivals at swept rates give p50/p99 latency (submit to completion); all requests at once
-    give the saturated throughput, compared with one batched call over the same pairs."""
+    """The serving loop (st_server_*) on the long/overflow mix (config 4, both halves: BLOSUM62 rows at 11/1 and
+    PSSM rows at 44/4, one server per gap setting on the same context): one request per pair (query rows + a
+    target of 1,000-35,000 residues, banded when the length ratio is above 4).  Poisson arrivals at swept
+    rates, spread over both halves, give p50/p99 latency (submit to completion); all requests at once give the
+    saturated throughput, compared with one batched call per half over the same pairs (profile build and free
+    included in both)."""
     import threading
     from sabertooth_b200 import GapCosts, Server
-    from synth import workloads as W
     from sabertooth_b200._lib import PAIR_DTYPE
-    w = W.config4(seed=args.seed, n_pairs=args.serving_pairs, kind="blosum62")
-    gaps = GapCosts(w.gap_open, w.gap_extend)
-    ctx.upload_db(w.db_residues, w.db_offsets)
-    cells = w.cells()
-    per_cells = np.array([w.cells_of(i) for i in range(w.n_pairs)], dtype=np.float64)
-    # batched reference: every request in one batch, profiles built and freed inside the timing as the
-    # server does
-    pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
-    pairs["target"] = w.pair_t
-    pairs["band_center"] = w.band_center
-    pairs["band_radius"] = w.band_radius
-    nrows = np.array([len(r) for r in w.rows], dtype=np.uint64)
-    row_offs = np.zeros(len(w.rows) + 1, dtype=np.uint64)
-    row_offs[1:] = np.cumsum(nrows)
-    rows_arena = np.concatenate(w.rows).astype(np.int32)
-    want = None
-    reps = 4
+    from synth import workloads as W
+    half = max(1, args.serving_pairs // 2)
+    ws = [W.config4(seed=args.seed, n_pairs=half, kind="blosum62"), W.config4(seed=args.seed, n_pairs=half, kind="pssm")]
+    gaps = [GapCosts(w.gap_open, w.gap_extend) for w in ws]
+    ctx.upload_db_list(ws[0].targets() + ws[1].targets())
+    tbase = [0, len(ws[0].db_offsets) - 1]
+    cells = sum(w.cells() for w in ws)
+    per_cells = [np.array([w.cells_of(i) for i in range(w.n_pairs)], dtype=np.float64) for w in ws]
+    nrows = [np.array([len(r) for r in w.rows], dtype=np.uint64) for w in ws]
+    # batched reference: every request of a half in one batch, profiles built and freed inside the timing as
+    # the server does
+    want = [None, None]
     times = []
-    for _ in range(reps):
+    for rep in range(4):
         t0 = time.perf_counter()
-        ids = ctx.create_profiles_arena(rows_arena, row_offs)
-        pairs["profile"] = ids[w.pair_q]
-        got = ctx.sw_score_pairs(pairs, gaps)
-        ctx.free_profiles(ids)
+        for h, w in enumerate(ws):
+            ro = np.zeros(len(w.rows) + 1, dtype=np.uint64)
+            ro[1:] = np.cumsum(nrows[h])
+            ids = ctx.create_profiles_arena(np.concatenate(w.rows).astype(np.int32), ro)
+            pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
+            pairs["profile"] = ids[w.pair_q]
+            pairs["target"] = tbase[h] + w.pair_t
+            pairs["band_center"] = w.band_center
+            pairs["band_radius"] = w.band_radius
+            got = ctx.sw_score_pairs(pairs, gaps[h])
+            ctx.free_profiles(ids)
+            want[h] = got if want[h] is None else want[h]
         times.append(time.perf_counter() - t0)
-        want = got if want is None else want
     batched_gcups = cells / float(np.median(times[1:])) / 1e9
-    srv = Server(ctx, gaps)
+    srv = [Server(ctx, g) for g in gaps]
     ok = True
-    # each config-4 pair is its own query: request i = rows of query pair_q[i], target pair_t[i]
-    t_offs = np.arange(w.n_pairs + 1, dtype=np.uint64)
+    t_offs = [np.arange(w.n_pairs + 1, dtype=np.uint64) for w in ws]
 
-    def burst(order):
-        """The requests of `order` as one bulk submission, built before the clock starts."""
+    def burst(h, order):
+        """The requests `order` of half h as one bulk submission, built before the clock starts."""
+        w = ws[h]
         q = w.pair_q[order]
         ro = np.zeros(len(order) + 1, dtype=np.uint64)
-        ro[1:] = np.cumsum(nrows[q])
+        ro[1:] = np.cumsum(nrows[h][q])
         arena = np.concatenate([w.rows[int(j)] for j in q]).astype(np.int32)
-        return (arena, ro, np.ascontiguousarray(w.pair_t[order]), t_offs[:len(order) + 1],
-                np.ascontiguousarray(w.band_center[order]), np.ascontiguousarray(w.band_radius[order]))
+        return (arena, ro, np.ascontiguousarray(tbase[h] + w.pair_t[order]).astype(np.uint32),
+                t_offs[h][:len(order) + 1], np.ascontiguousarray(w.band_center[order]),
+                np.ascontiguousarray(w.band_radius[order]))
 
-    for rid in srv.submit_many(*burst(np.arange(min(500, w.n_pairs)))):  # warm-up: pools, pinned blocks, streams
-        srv.wait(rid)
+    for h in range(2):  # warm-up: pools, pinned blocks, streams
+        for rid in srv[h].submit_many(*burst(h, np.arange(min(250, ws[h].n_pairs)))):
+            srv[h].wait(rid)
 
     def run(order, arrivals):
+        """order: (half, pair) requests in arrival order."""
         nonlocal ok
         rids = [None] * len(order)
         lat = np.zeros(len(order))
-        done = threading.Event()
 
         def waiter():
             nonlocal ok
-            for k, i in enumerate(order):
+            for k, (h, i) in enumerate(order):
                 while rids[k] is None:
                     time.sleep(0.0002)
-                s, lat[k] = srv.wait(rids[k])
-                ok &= bool(s[0] == want[i])
-            done.set()
+                s_, lat[k] = srv[h].wait(rids[k])
+                ok &= bool(s_[0] == want[h][i])
 
         th = threading.Thread(target=waiter)
         th.start()
         t0 = time.perf_counter()
-        for k, i in enumerate(order):
+        for k, (h, i) in enumerate(order):
             if arrivals is not None:
                 dt = t0 + arrivals[k] - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
-            rids[k] = srv.submit(w.rows[w.pair_q[i]], w.pair_t[i:i + 1], w.band_center[i:i + 1],
-                                 w.band_radius[i:i + 1])
+            w = ws[h]
+            rids[k] = srv[h].submit(w.rows[w.pair_q[i]], tbase[h] + w.pair_t[i:i + 1], w.band_center[i:i + 1],
+                                    w.band_radius[i:i + 1])
         th.join()
         wall = time.perf_counter() - t0
-        c = float(per_cells[order].sum())
+        c = float(sum(per_cells[h][i] for h, i in order))
         return {"requests": len(order), "p50_ms": round(float(np.percentile(lat, 50)), 2),
                 "p99_ms": round(float(np.percentile(lat, 99)), 2), "gcups": round(c / wall / 1e9, 2),
                 "q_per_s": round(len(order) / wall, 1)}
 
     rng = np.random.default_rng(args.seed + 11)
+    everyone = [(h, i) for h in range(2) for i in range(ws[h].n_pairs)]
     rates = []
     for rate in (50, 200, 1000, 2000):
-        n = int(min(w.n_pairs, max(40, rate * args.serving_seconds)))
-        order = rng.choice(w.n_pairs, size=n, replace=False)
+        n = int(min(len(everyone), max(40, rate * args.serving_seconds)))
+        pick = rng.choice(len(everyone), size=n, replace=False)
+        order = [everyone[int(k)] for k in pick]
         arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
         rates.append(dict(rate_q_per_s=rate, **run(order, arrivals)))
-    # saturated: every request arrives at once (one bulk submit); throughput from the submit to the last
-    # completion, both stamped inside the server (one unmeasured round first: the server's pinned arena
-    # grows to the burst's size)
-    b_all = burst(np.arange(w.n_pairs))
+    # saturated: every request arrives at once (one bulk submit per half); throughput from the first submit to
+    # the last completion, both stamped inside the servers (one unmeasured round first: the servers' pinned
+    # arenas grow to the burst's size)
+    bursts = [burst(h, np.arange(ws[h].n_pairs)) for h in range(2)]
     for rnd in range(3):
-        rids = srv.submit_many(*b_all)
-        lat = np.zeros(w.n_pairs)
-        for i, rid in enumerate(rids):
-            s_, lat[i] = srv.wait(rid)
-            ok &= bool(s_[0] == want[i])
+        rids = [srv[h].submit_many(*bursts[h]) for h in range(2)]
+        lat = []
+        for h in range(2):
+            for i, rid in enumerate(rids[h]):
+                s_, l_ = srv[h].wait(rid)
+                lat.append(l_)
+                ok &= bool(s_[0] == want[h][i])
+        lat = np.array(lat)
         wall = float(lat.max()) * 1e-3
-    sat = {"requests": int(w.n_pairs), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+    n_all = sum(w.n_pairs for w in ws)
+    sat = {"requests": int(n_all), "p50_ms": round(float(np.percentile(lat, 50)), 2),
            "p99_ms": round(float(np.percentile(lat, 99)), 2), "gcups": round(cells / wall / 1e9, 2),
-           "q_per_s": round(w.n_pairs / wall, 1)}
-    st = srv.stats()
-    srv.close()
-    return {"workload": f"config 4 BLOSUM62 half: {w.n_pairs} requests (query lognormal median 250, target "
-                        f"1,000-35,000, {w.info['banded']} banded with radius 64), gaps 11/1",
+           "q_per_s": round(n_all / wall, 1)}
+    stats = [s_.stats() for s_ in srv]
+    for s_ in srv:
+        s_.close()
+    return {"workload": f"config 4 mix: {ws[0].n_pairs} BLOSUM62 (11/1) + {ws[1].n_pairs} PSSM (44/4) requests "
+                        f"(query lognormal median 250, target 1,000-35,000, "
+                        f"{ws[0].info['banded'] + ws[1].info['banded']} banded with radius 64)",
             "cells": int(cells), "batched_gcups": round(batched_gcups, 2),
-            "batched_how": "one st_sw_score_pairs over every request, profile build and free included", "poisson": rates,
-            "saturated": dict(sat, frac_of_batched=round(sat["gcups"] / batched_gcups, 3)),
-            "batches": st["batches"], "matches_batched": bool(ok),
+            "batched_how": "one st_sw_score_pairs per half over every request, profile build and free included",
+            "poisson": rates, "saturated": dict(sat, frac_of_batched=round(sat["gcups"] / batched_gcups, 3)),
+            "batches": int(sum(st["batches"] for st in stats)), "matches_batched": bool(ok),
             "latency": "submit to completion inside the server (C++ steady clock)"}
-
 
 if __name__ == "__main__":
     sys.exit(main())

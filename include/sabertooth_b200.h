@@ -454,8 +454,12 @@ int st_autotune(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, int
  * kernel's scratch is a fixed 512 KiB static device array that every GPU
  * loading the library holds until exit; all calls on a device share it, so
  * calls that overlap on the GPU race and must be ordered by the caller.  The
- * first call on a device resolves the array's address; make it before any
- * stream capture.  Same scores as st_sw_score for every gap cost. */
+ * first call on a device resolves the array's address and keeps it for the
+ * process; make it before any stream capture.  A cudaDeviceReset discards the
+ * device's copy of the array, so the kept address is stale afterwards: reset
+ * no device that this entry point has run on.  Nothing in the array needs to
+ * start at zero (a call writes every boundary entry before it reads it back).
+ * Same scores as st_sw_score for every gap cost. */
 int st_sw_score_noalloc(const int32_t* d_rows, uint32_t m, const uint8_t* d_target, uint32_t n, int32_t open,
                         int32_t ext, int32_t* d_score, void* stream);
 

@@ -31,7 +31,9 @@
 // Set-up: the first call on a device looks up the device address of the array
 // (cudaGetSymbolAddress, with that device current) and caches it; later calls
 // only launch.  Make that first call before any stream capture begins (a warm-up
-// call with n = 0 is enough).
+// call with n = 0 is enough).  The cache lives for the process: after a
+// cudaDeviceReset the device holds a new copy of the array at an address this
+// cache does not know, so a device that was reset must not be used here again.
 #include <cstdint>
 #include <cstdio>
 #include <mutex>

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <condition_variable>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -261,6 +262,17 @@ struct ProfileMeta {
   uint32_t stride8 = 0, stride32 = 0;
 };
 
+// One per-call scoring in flight (st_sw_score): its own stream, pinned block,
+// device staging and scratch, so that calls from several host threads run at
+// once; the context lock covers only their set-up and launches.
+struct CallSlot {
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev_in = nullptr;    // the context stream's work before the call (profile tables ready)
+  cudaEvent_t ev_done = nullptr;  // the call's result is in the pinned block
+  Pinned pin;
+  DevMem stage, scratch;
+};
+
 struct st_ctx {
   int device = 0;
   int sms = 0;
@@ -312,6 +324,12 @@ struct st_ctx {
   Pinned pin;
   DevMem stage;
   DevMem scratch_small;
+  // st_sw_score calls in flight: slots handed out under call_mu (not the context lock)
+  static constexpr size_t kMaxCallSlots = 32;
+  std::mutex call_mu;
+  std::condition_variable call_cv;
+  std::vector<std::unique_ptr<CallSlot>> call_slots;
+  std::vector<CallSlot*> call_idle;
   Tuning tuning;
   // seed index over the database (st_seed_index_build): offsets of the 20^w codes, postings
   DevMem seed_off, seed_post;
@@ -451,6 +469,38 @@ static int side_stream(st_ctx* c, cudaStream_t* out) {
 // profiles were created or freed since, refreshes the device tables of
 // profile pointers, strides and lengths. The tables go up on the stream from
 // a ring of pinned blocks, so work already queued keeps reading the old ones.
+// Waits for every per-call scoring in flight (before memory they may read is reallocated).
+static int calls_drain(st_ctx* c) {
+  std::lock_guard<std::mutex> lk(c->call_mu);
+  for (auto& sl : c->call_slots)
+    if (sl->s) ST_CUDA(cudaStreamSynchronize(sl->s));
+  return ST_OK;
+}
+
+static CallSlot* call_acquire(st_ctx* c) {
+  std::unique_lock<std::mutex> lk(c->call_mu);
+  for (;;) {
+    if (!c->call_idle.empty()) {
+      CallSlot* sl = c->call_idle.back();
+      c->call_idle.pop_back();
+      return sl;
+    }
+    if (c->call_slots.size() < st_ctx::kMaxCallSlots) {
+      c->call_slots.push_back(std::make_unique<CallSlot>());
+      return c->call_slots.back().get();
+    }
+    c->call_cv.wait(lk);  // every slot is in a call; the first to finish hands its slot over
+  }
+}
+
+static void call_release(st_ctx* c, CallSlot* sl) {
+  {
+    std::lock_guard<std::mutex> lk(c->call_mu);
+    c->call_idle.push_back(sl);
+  }
+  c->call_cv.notify_one();
+}
+
 static int sync_profiles(st_ctx* c) {
   if (c->prof_ev_set) {
     ST_CUDA(cudaStreamWaitEvent(c->stream, c->prof_ev, 0));
@@ -491,6 +541,7 @@ static int sync_profiles(st_ctx* c) {
   auto up = [&](DevMem& d, size_t off, size_t bytes) -> int {
     if (d.bytes < bytes) {
       ST_CUDA(cudaStreamSynchronize(c->stream));  // queued work may read the old table
+      ST_TRY(calls_drain(c));                     // and so may per-call scorings in flight
       ST_TRY(dev_alloc(&c->mt, d, bytes * 2));
     }
     ST_CUDA(cudaMemcpyAsync(d.p, h + off, bytes, cudaMemcpyHostToDevice, c->stream));
@@ -624,6 +675,16 @@ extern "C" void st_shutdown(st_ctx* c) {
     for (auto e : f.ev)
       if (e) cudaEventDestroy(e);
   }
+  for (auto& sl : c->call_slots) {
+    if (sl->s) {
+      cudaStreamSynchronize(sl->s);
+      cudaStreamDestroy(sl->s);
+    }
+    if (sl->ev_in) cudaEventDestroy(sl->ev_in);
+    if (sl->ev_done) cudaEventDestroy(sl->ev_done);
+  }
+  c->call_slots.clear();
+  c->call_idle.clear();
   cudaStream_t own = c->own;
   if (c->copy) {
     cudaStreamSynchronize(c->copy);
@@ -2638,10 +2699,12 @@ extern "C" int st_sw_align_span_pairs(st_ctx* c, const st_pair* pairs, uint64_t 
 // ---------------------------------------------------------------------------
 // plain per-call SW (one pair, one launch of each kernel, blocking)
 // ---------------------------------------------------------------------------
-extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
-                           int32_t* score, uint32_t* kernel) {
-  CTX_GUARD(c);
-  if (!score || (n && !target)) return fail(ST_EINVAL, "st_sw_score: null argument");
+// Set-up and launches of one per-call scoring on slot `sl` (context lock held). *queued says whether
+// work was launched; its score and kernel tag then land in the slot's pinned block at `*res_off`.
+static int sw_score_enqueue(st_ctx* c, CallSlot* sl, uint32_t profile, const uint8_t* target, uint32_t n,
+                            int32_t open, int32_t ext, int32_t* score, uint32_t* kernel, bool* queued,
+                            size_t* res_off) {
+  *queued = false;
   ST_TRY(check_profile(c, profile));
   ST_TRY(sync_profiles(c));
   const ProfileMeta& pm = c->profs[profile];
@@ -2688,11 +2751,16 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
   const uint32_t sstride = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(n) + 32));
   // any warp of the CTA may take the task: room for every group of the CTA
   const size_t scratch_need = static_cast<size_t>(kClasses[k].W) * 8 * sstride * sizeof(uint2);
-  ST_TRY(c->pin.reserve(total));
-  if (c->stage.bytes < total) ST_TRY(dev_alloc(&c->mt, c->stage, total * 2));
-  if (c->scratch_small.bytes < scratch_need) ST_TRY(dev_alloc(&c->mt, c->scratch_small, scratch_need * 2));
-  char* h = c->pin.as<char>();
-  ST_CUDA(cudaStreamSynchronize(c->stream));  // the pinned block is reused per call
+  if (!sl->s) {
+    ST_CUDA(cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
+    ST_CUDA(cudaEventCreateWithFlags(&sl->ev_in, cudaEventDisableTiming));
+    ST_CUDA(cudaEventCreateWithFlags(&sl->ev_done, cudaEventDisableTiming));
+  }
+  // the slot's previous call has been waited for, so its pinned block and device buffers are free
+  ST_TRY(sl->pin.reserve(total + 16));
+  if (sl->stage.bytes < total) ST_TRY(dev_alloc(&c->mt, sl->stage, total * 2));
+  if (sl->scratch.bytes < scratch_need) ST_TRY(dev_alloc(&c->mt, sl->scratch, scratch_need * 2));
+  char* h = sl->pin.as<char>();
   memset(h, 0, total);
   for (uint32_t i = 0; i < n; ++i) h[i] = static_cast<char>(target[i] < kSentinel ? target[i] : kSentinel);
   memset(h + n, kSentinel, tbytes - n);
@@ -2717,8 +2785,12 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
     const size_t nz = (total - o_zline) / sizeof(uint2);
     for (size_t i = 0; i < nz; ++i) z[i] = make_uint2(0u, pk_splat(-open));
   }
-  char* d = c->stage.as<char>();
-  ST_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, c->stream));
+  char* d = sl->stage.as<char>();
+  cudaStream_t st = sl->s;
+  // the profile tables and layouts are written in the context stream's order: start after its work so far
+  ST_CUDA(cudaEventRecord(sl->ev_in, c->stream));
+  ST_CUDA(cudaStreamWaitEvent(st, sl->ev_in, 0));
+  ST_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, st));
   DeviceDb db;
   db.arena = reinterpret_cast<const uint8_t*>(d);
   db.offset = reinterpret_cast<const uint64_t*>(d + o_off);
@@ -2742,12 +2814,12 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
     prm.ovf_count = d_cnt + kNumClasses + 1;
     prm.ovf_pairs = d_list;
     prm.work_counter = d_cnt + k;
-    prm.scratch = c->scratch_small.as<uint2>();
+    prm.scratch = sl->scratch.as<uint2>();
     prm.zline = reinterpret_cast<const uint2*>(d + o_zline);
     prm.scratch_stride = sstride;
     prm.open = open;
     prm.ext = ext;
-    kClasses[k].fn<<<1, kClasses[k].W * 32, kProfRows * P * rows, c->stream>>>(prm);
+    kClasses[k].fn<<<1, kClasses[k].W * 32, kProfRows * P * rows, st>>>(prm);
     ++c->launches;
   }
   // the 32-bit kernel scores the pair only when it is in the list (headroom reached, or not 16-bit eligible)
@@ -2763,19 +2835,49 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
   p32.scores = d_score;
   p32.kernels = d_kern;
   p32.work_counter = d_cnt + kNumClasses;
-  p32.scratch = reinterpret_cast<int2*>(c->scratch_small.p);
+  p32.scratch = reinterpret_cast<int2*>(sl->scratch.p);
   p32.scratch_stride = static_cast<uint32_t>(up16(n) + 32);
   p32.open = open;
   p32.ext = ext;
-  sw32_kernel<kWarps32><<<1, kWarps32 * 32, 0, c->stream>>>(p32);
+  sw32_kernel<kWarps32><<<1, kWarps32 * 32, 0, st>>>(p32);
   ++c->launches;
   ST_CUDA(cudaGetLastError());
-  int32_t res[2];
-  ST_CUDA(cudaMemcpyAsync(res, d_score, 8, cudaMemcpyDeviceToHost, c->stream));
-  ST_CUDA(cudaStreamSynchronize(c->stream));
-  *score = res[0];
-  if (kernel) *kernel = static_cast<uint32_t>(res[1]);
+  // score and kernel tag into the pinned block behind the staged inputs
+  *res_off = up16(total);
+  ST_CUDA(cudaMemcpyAsync(h + *res_off, d_score, 8, cudaMemcpyDeviceToHost, st));
+  ST_CUDA(cudaEventRecord(sl->ev_done, st));
+  *queued = true;
   return ST_OK;
+}
+
+// The plain per-call drop-in for sw_score_with.  Calls from several host threads proceed at once: each
+// takes a call slot (its own stream and buffers), holds the context lock only while it sets up and
+// launches, and waits for its result outside the lock.
+extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
+                           int32_t* score, uint32_t* kernel) {
+  if (!c) return fail(ST_EINVAL, "null context");
+  if (!score || (n && !target)) return fail(ST_EINVAL, "st_sw_score: null argument");
+  CallSlot* sl = call_acquire(c);
+  bool queued = false;
+  size_t res_off = 0;
+  int rc;
+  {
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    rc = cudaSetDevice(c->device) == cudaSuccess ? ST_OK : fail(ST_ECUDA, "cudaSetDevice(%d) failed", c->device);
+    if (rc == ST_OK) rc = sw_score_enqueue(c, sl, profile, target, n, open, ext, score, kernel, &queued, &res_off);
+  }
+  if (queued) {
+    const cudaError_t e = cudaEventSynchronize(sl->ev_done);
+    if (e != cudaSuccess) {
+      rc = fail(ST_ECUDA, "st_sw_score: %s", cudaGetErrorString(e));
+    } else if (rc == ST_OK) {
+      const int32_t* res = sl->pin.as<int32_t>(res_off);
+      *score = res[0];
+      if (kernel) *kernel = static_cast<uint32_t>(res[1]);
+    }
+  }
+  call_release(c, sl);
+  return rc;
 }
 
 // ---------------------------------------------------------------------------

@@ -115,44 +115,74 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
   }
   int32_t best = 0, hup_prev = 0, h_bot = 0, f_out = F0;
   int32_t bcol = 0x7FFFFFFF, brow = 0x7FFFFFFF;  // end modes: this lane's first optimum
-  uint32_t res = kSentinel;
   int c = -lane;
   int pass = 0;
-  uint32_t nxt = kSentinel;
   // target column j of the scored sequence (reversed in the reverse mode)
   auto tcol = [&](int j) -> uint32_t {
     const int jj = MODE == kSw32RevEnd ? rt - j : j;
     return min(static_cast<uint32_t>(__ldg(t + jj)), static_cast<uint32_t>(kSentinel));
   };
-  if (lane == 0) nxt = tcol(cstart);
+  // This lane's R profile scores of residue r at rows row0 .. row0 + R - 1.
+  auto load_rows = [&](uint32_t r, int row0, int32_t (&S)[R]) {
+    if constexpr (MODE == kSw32RevEnd) {
+      // row i of the reversed query is row rq - i of the profile (rows past the prefix: any in-range row)
+      const int32_t* rb = prof + static_cast<size_t>(r) * stride;
+#pragma unroll
+      for (int k = 0; k < R; ++k) S[k] = __ldg(rb + max(rq - (row0 + k), 0));
+    } else {
+      const int32_t* prow = prof + static_cast<size_t>(r) * stride + row0;
+      const int4 a = __ldg(reinterpret_cast<const int4*>(prow));
+      const int4 b = __ldg(reinterpret_cast<const int4*>(prow + 4));
+      S[0] = a.x; S[1] = a.y; S[2] = a.z; S[3] = a.w;
+      S[4] = b.x; S[5] = b.y; S[6] = b.z; S[7] = b.w;
+    }
+  };
+  // Software pipeline: a step computes with the residue and profile scores loaded during the step before,
+  // and loads the next step's.  A lane's next residue is the one its upper neighbour uses now (one extra
+  // shuffle); lane 0 reads its target columns one more step ahead.  (c2, p2): lane 0's column and pass two
+  // steps ahead.
+  uint32_t res = kSentinel, q1 = kSentinel;
+  int c2 = 2, p2 = 0;
+  while (c2 >= W) {
+    c2 -= W;
+    ++p2;
+  }
+  if (lane == 0) {
+    res = tcol(cstart);
+    q1 = (1 < W) ? (1 < ncols ? tcol(cstart + 1) : kSentinel) : (1 < P ? tcol(cstart) : kSentinel);
+  }
+  int32_t S[R];
+  load_rows(res, lane * R, S);
   const int steps = P * W + G - 1;
 
   for (int s = 0; s < steps; ++s) {
     int32_t hin = __shfl_up_sync(FULL, h_bot, 1);
     int32_t fin = __shfl_up_sync(FULL, f_out, 1);
-    uint32_t rin = __shfl_up_sync(FULL, res, 1);
+    uint32_t rn = __shfl_up_sync(FULL, res, 1);  // the upper lane's residue now: this lane's next one
     if (lane == 0) {
-      if (pass < P) {
-        rin = nxt;
-        int cn = c + 1;
-        bool last = (cn == W);
-        if (last) cn = 0;
-        nxt = ((last && pass + 1 >= P) || cn >= ncols) ? kSentinel : tcol(cstart + cn);
-        if (pass > 0 && c < ncols) {
-          int2 bv = bnd[c];
-          hin = bv.x;
-          fin = bv.y;
-        } else {
-          hin = 0;
-          fin = F0;
-        }
+      if (pass < P && pass > 0 && c < ncols) {
+        const int2 bv = bnd[c];
+        hin = bv.x;
+        fin = bv.y;
       } else {
-        rin = kSentinel;
         hin = 0;
         fin = F0;
       }
+      rn = q1;
+      q1 = (p2 < P && c2 < ncols) ? tcol(cstart + c2) : kSentinel;
+      if (++c2 == W) {
+        c2 = 0;
+        ++p2;
+      }
     }
-    res = rin;
+    // the next step's column and pass, and its profile scores
+    int cn = c + 1, pn = pass;
+    if (cn == W) {
+      cn = 0;
+      ++pn;
+    }
+    int32_t Sn[R];
+    load_rows(rn, (pn < P ? pn : P - 1) * G * R + lane * R, Sn);
     if (c == 0) {
 #pragma unroll
       for (int k = 0; k < R; ++k) {
@@ -163,19 +193,6 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     }
     const int pp = pass < P ? pass : P - 1;
     const int row0 = pp * G * R + lane * R;
-    const int32_t* prow = prof + static_cast<size_t>(res) * stride + row0;
-    int32_t S[R];
-    if constexpr (MODE == kSw32RevEnd) {
-      // row r of the reversed query is row rq - r of the profile (rows past the prefix: any in-range row)
-      const int32_t* rb = prof + static_cast<size_t>(res) * stride;
-#pragma unroll
-      for (int k = 0; k < R; ++k) S[k] = __ldg(rb + max(rq - (row0 + k), 0));
-    } else {
-      const int4 a = __ldg(reinterpret_cast<const int4*>(prow));
-      const int4 b = __ldg(reinterpret_cast<const int4*>(prow + 4));
-      S[0] = a.x; S[1] = a.y; S[2] = a.z; S[3] = a.w;
-      S[4] = b.x; S[5] = b.y; S[6] = b.z; S[7] = b.w;
-    }
     const int col = cstart + c;  // target column (0-based) of this lane
     const bool live = (c >= 0) && (c < ncols) && (pass < P);
     int32_t hd = hup_prev;
@@ -221,10 +238,11 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     h_bot = Hp[R - 1];
     f_out = F;
     if (lane == G - 1 && pass + 1 < P && c >= 0 && c < ncols) bnd[c] = make_int2(h_bot, f_out);
-    if (++c == W) {
-      c = 0;
-      ++pass;
-    }
+    c = cn;
+    pass = pn;
+    res = rn;
+#pragma unroll
+    for (int k = 0; k < R; ++k) S[k] = Sn[k];
     __syncwarp();
   }
   if constexpr (MODE == kSw32Score) {

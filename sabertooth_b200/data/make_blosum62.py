@@ -82,7 +82,9 @@ def build(text, bit_factor=2.0, bias=-0.2):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/data/blosum62.out"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_blosum62.py /path/to/reference/src/data/blosum62.out")
+    src = sys.argv[1]
     with open(src) as f:
         data = build(f.read())
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "blosum62.json")

@@ -99,3 +99,42 @@ def test_concurrent_calls_equal_single_thread_results(ctx):
     again = _work(ctx, w, lens, seed=100)
     for a, b in zip(again, want[0]):
         assert np.array_equal(a, b)
+
+
+def test_per_call_scores_from_many_threads_at_once(ctx):
+    """st_sw_score (the per-call drop-in of sw_score_with) from 24 threads at once, more threads than the
+    context has call slots would need to be busy: every call returns the oracle's score, with profiles
+    created by one thread while the others score (the profile tables grow under running calls)."""
+    from oracle import oracle as O
+    w = W.config3(seed=43, n_queries=24, db_residues=60_000, per_query=40)
+    targets = w.targets()
+    ids = ctx.create_profiles(w.rows)
+    want = O.sw_pairs(O.Arena(w.rows, targets), w.pair_q, w.pair_t, GAPS.open, GAPS.extend)
+    got = np.full(w.n_pairs, -1, dtype=np.int64)
+    errors = []
+    n_thr = 24
+    start = threading.Barrier(n_thr + 1)
+
+    def run(k):
+        try:
+            start.wait()
+            for i in range(k, w.n_pairs, n_thr):
+                got[i] = _plain(ctx, int(ids[w.pair_q[i]]), targets[int(w.pair_t[i])])
+        except Exception as e:  # reported below
+            errors.append(repr(e))
+
+    def churn():
+        # profile creation and frees while calls run: the device profile tables are rebuilt and grown
+        start.wait()
+        for _ in range(20):
+            extra = ctx.create_profiles(w.rows[:8] * 8)
+            ctx.free_profiles(extra)
+
+    th = [threading.Thread(target=run, args=(k,)) for k in range(n_thr)] + [threading.Thread(target=churn)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=600)
+    ctx.free_profiles(ids)
+    assert not errors, errors
+    assert np.array_equal(got, want.astype(np.int64))
