@@ -2901,10 +2901,11 @@ static int launch_ungapped(st_ctx* c, bool hits, const void* d_jobs, uint64_t n,
     return fail(ST_EINVAL, "query too long for the ungapped kernel (%u rows)", max_m ? max_m : c->max_m);
   const uint64_t grid = (n + kUngChunk - 1) / kUngChunk;
   if (grid > 0x7FFFFFFFull) return fail(ST_EINVAL, "too many ungapped jobs");
-  // hit lists: the run's work split evenly over the lanes; the per-lane refill form for queries whose staged
-  // rows do not fit beside the split kernel's static shared memory (or when ST_UNGAPPED_REFILL=1)
-  static const bool force_refill = env_u64("ST_UNGAPPED_REFILL", 0) != 0;
-  if (hits && !force_refill && smem <= static_cast<size_t>(g_ung_split_smem))
+  // hit lists: one hit per lane with refill; with ST_UNGAPPED_SPLIT=1 the form that splits a run's work evenly
+  // over the lanes (measured slower on 2x10^7 hits: 2.33 against 1.68 ms; its static shared memory halves the
+  // CTAs per SM and its phases add barriers)
+  const bool split = env_u64("ST_UNGAPPED_SPLIT", 0) != 0;
+  if (hits && split && smem <= static_cast<size_t>(g_ung_split_smem))
     ungapped_hits_split_kernel<<<static_cast<uint32_t>(grid), kUngSplitLanes, smem, c->stream>>>(prm);
   else if (hits)
     ungapped_hits_refill_kernel<<<static_cast<uint32_t>(grid), 256, smem, c->stream>>>(prm);

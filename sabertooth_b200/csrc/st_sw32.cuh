@@ -195,38 +195,37 @@ __device__ __forceinline__ void sw32_pair(const Sw32Params& prm, uint32_t p, int
     const int row0 = pp * G * R + lane * R;
     const int col = cstart + c;  // target column (0-based) of this lane
     const bool live = (c >= 0) && (c < ncols) && (pass < P);
+    // band rows of this column among the lane's R rows: row0 + k is in the band when
+    // col - center - radius <= row0 + k <= col - center + radius, i.e. k_lo <= k <= k_hi (clamped to [-1, R])
+    int k_lo = 0, k_hi = R - 1;
+    if (banded) {
+      const int64_t base = static_cast<int64_t>(col) - row0 - center;
+      k_lo = static_cast<int>(i64max(-1, i64min(R, base - radius)));
+      k_hi = static_cast<int>(i64max(-1, i64min(R, base + radius)));
+    }
     int32_t hd = hup_prev;
     int32_t F = fin;
     int32_t lmax = 0;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int row = row0 + k;
-      int32_t H, En, Fn;
-      bool inband = true;
-      if (banded) {
-        const int64_t off = static_cast<int64_t>(col) - row - center;
-        inband = (off >= -radius) && (off <= radius);
-      }
-      if (inband) {
-        const int32_t tt = max(wadd(hd, S[k]), E[k]);
-        H = max(max(tt, F), 0);
-        const int32_t Ho = wsub(H, open);
-        En = max(wsub(E[k], ext), Ho);
-        Fn = max(wsub(F, ext), Ho);
-        if (row < m) {
-          lmax = max(lmax, H);
-          if constexpr (MODE != kSw32Score) {
-            if (live && end_before(H, col, row, best, bcol, brow)) {
-              best = H;
-              bcol = col;
-              brow = row;
-            }
+      const bool inband = (k >= k_lo) && (k <= k_hi);
+      const int32_t tt = max(wadd(hd, S[k]), E[k]);
+      const int32_t Hc = max(max(tt, F), 0);
+      const int32_t Ho = wsub(Hc, open);
+      // out of the band: H = 0 and E = F = minus infinity (their successors then start from -open)
+      const int32_t H = inband ? Hc : 0;
+      const int32_t En = inband ? max(wsub(E[k], ext), Ho) : E0;
+      const int32_t Fn = inband ? max(wsub(F, ext), Ho) : F0;
+      if (row < m) {
+        lmax = max(lmax, H);
+        if constexpr (MODE != kSw32Score) {
+          if (live && end_before(H, col, row, best, bcol, brow)) {
+            best = H;
+            bcol = col;
+            brow = row;
           }
         }
-      } else {
-        H = 0;
-        En = E0;
-        Fn = F0;
       }
       E[k] = En;
       F = Fn;

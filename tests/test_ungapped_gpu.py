@@ -99,7 +99,14 @@ def test_window_outside_the_diagonal_is_rejected(ctx):
     prof.qp.free()
 
 
-def test_hits_and_pair_runs_match_oracle(ctx):
+@pytest.fixture(params=["refill", "split"])
+def hit_kernel(request, monkeypatch):
+    """Runs a hit test with the default refill kernel and with the split-work kernel (ST_UNGAPPED_SPLIT=1)."""
+    monkeypatch.setenv("ST_UNGAPPED_SPLIT", "1" if request.param == "split" else "0")
+    return request.param
+
+
+def test_hits_and_pair_runs_match_oracle(ctx, hit_kernel):
     w = W.config2(seed=2, n_queries=40, n_targets=3000, n_hits=60_000)
     ctx.upload_db(w.db_residues, w.db_offsets)
     ids = ctx.create_profiles(w.rows)
@@ -122,7 +129,7 @@ def test_hits_and_pair_runs_match_oracle(ctx):
         ctx.free_profile(i)
 
 
-def test_unsorted_hits_are_still_exact(ctx):
+def test_unsorted_hits_are_still_exact(ctx, hit_kernel):
     w = W.config2(seed=4, n_queries=30, n_targets=2000, n_hits=20_000)
     ctx.upload_db(w.db_residues, w.db_offsets)
     ids = ctx.create_profiles(w.rows)
