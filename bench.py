@@ -475,7 +475,7 @@ def main():
         total_cells = float(cells)
     gcups = total_cells / (ms * 1e-3) / 1e9
     stats = plan.stats()
-    launch_profile = [{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if sh else "sw32"), "cells": c, "ms": round(t, 3),
+    launch_profile = [{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if isinstance(sh, tuple) else sh), "cells": c, "ms": round(t, 3),
                        "gcups": round(c / (t * 1e-3) / 1e9, 1) if t > 0 else None}
                       for sh, c, t in plan.profile()] if rank == 0 else None
     scores = d_scores.cpu().numpy()
@@ -1193,7 +1193,7 @@ def long_mix_measure(ctx, args):
         t_base += len(w.db_offsets) - 1
     ts = _timed_plans(ctx, plans, args.steps)
     stats = [p.stats() for p in plans]
-    profiles = [[{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if sh else "sw32"), "cells": c, "ms": round(t, 3)}
+    profiles = [[{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if isinstance(sh, tuple) else sh), "cells": c, "ms": round(t, 3)}
                  for sh, c, t in p.profile()] for p in plans]
     for p in plans:
         p.close()

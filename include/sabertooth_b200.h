@@ -155,8 +155,10 @@ int st_plan_create(st_ctx* ctx, const st_pair* pairs, uint64_t n, int32_t open, 
 int st_plan_run(st_plan* plan);
 int st_plan_stats(st_plan* plan, uint64_t* cells, uint64_t* rescored_pairs, uint32_t* n_launch_classes);
 /* Runs each launch of the plan alone, timed with CUDA events on the context stream:
- * entry i = tile class index (-1 = the 32-bit kernel), its planned cells and its time.
- * cap >= n_launch_classes + 1; *n_out receives the count.  Scores are written as by a run. */
+ * entry i = tile class index (-1 = the 32-bit kernel, -2 = the packed kernel of
+ * banded pairs, whose cells are counted in the 32-bit entry), its planned cells
+ * and its time.  cap >= n_launch_classes + 2; *n_out receives the count.  Scores
+ * are written as by a run. */
 int st_plan_profile(st_plan* plan, uint32_t cap, int32_t* classes, uint64_t* cells, float* ms, uint32_t* n_out);
 void st_plan_destroy(st_plan* plan);
 

@@ -619,7 +619,8 @@ class Plan:
         return {"cells": cells.value, "rescored_pairs": resc.value, "launch_classes": ncls.value}
 
     def profile(self):
-        """Each launch alone: [(tile class (G, R) or None for the 32-bit kernel, cells, ms)]."""
+        """Each launch alone: [(tile class (G, R, C), or "sw32" for the 32-bit kernel, or "band16" for the packed
+        kernel of banded pairs, cells, ms)]."""
         cap = 32
         cls = np.zeros(cap, dtype=np.int32)
         cells = np.zeros(cap, dtype=np.uint64)
@@ -627,7 +628,9 @@ class Plan:
         n = C.c_uint32()
         check(lib.st_plan_profile(self._h, cap, ptr(cls), ptr(cells), ptr(ms), C.byref(n)))
         shapes = tile_classes()
-        return [(shapes[cls[i]] if cls[i] >= 0 else None, int(cells[i]), float(ms[i])) for i in range(n.value)]
+        names = {-1: "sw32", -2: "band16"}
+        return [(shapes[cls[i]] if cls[i] >= 0 else names[int(cls[i])], int(cells[i]), float(ms[i]))
+                for i in range(n.value)]
 
     def close(self):
         if self._h:

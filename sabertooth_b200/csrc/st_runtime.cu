@@ -21,6 +21,7 @@
 #include "st_common.cuh"
 #include "st_sw16.cuh"
 #include "st_sw32.cuh"
+#include "st_band16.cuh"
 #include "st_tuning.h"
 #include "st_ungapped.cuh"
 #include "st_dplan.cuh"
@@ -1155,8 +1156,10 @@ static int plan_enqueue(st_plan* p, cudaStream_t st, st_ctx::ForkSet* fs, bool g
       cudaSuccess)
     return ST_ECUDA;
   const size_t nc = p->classes.size();
-  if (!fs || nc <= 1) {
+  const bool band16 = p->p32.band16 != 0;
+  if (!fs || nc + (band16 ? 1 : 0) <= 1) {
     for (auto& cp : p->classes) kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, st>>>(cp.prm);
+    if (band16) sw16_band_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, st>>>(p->p32);
   } else {
     // The classes run side by side: the costliest on the launching stream, the
     // others on forks joined before sw32. The launch order matters, as the block
@@ -1198,12 +1201,25 @@ static int plan_enqueue(st_plan* p, cudaStream_t st, st_ctx::ForkSet* fs, bool g
       kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, s>>>(cp.prm);
       if (cudaGetLastError() != cudaSuccess) return ST_ECUDA;
     }
+    if (band16) {  // the banded pairs of the static list, beside the classes (it reads only that list)
+      cudaStream_t s = st;
+      if (nc > 0) {
+        const int j = next++ % st_ctx::ForkSet::kForks;
+        if (!used[j] && cudaStreamWaitEvent(fs->s[j], fs->ev[0], 0) != cudaSuccess) return ST_ECUDA;
+        used[j] = true;
+        s = fs->s[j];
+      }
+      sw16_band_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, s>>>(p->p32);
+      if (cudaGetLastError() != cudaSuccess) return ST_ECUDA;
+    }
     for (int j = 0; j < st_ctx::ForkSet::kForks; ++j) {
       if (!used[j]) continue;
       if (cudaEventRecord(fs->ev[1 + j], fs->s[j]) != cudaSuccess) return ST_ECUDA;
       if (cudaStreamWaitEvent(st, fs->ev[1 + j], 0) != cudaSuccess) return ST_ECUDA;
     }
   }
+  // the band kernel used the 32-bit kernel's work counter
+  if (band16 && cudaMemsetAsync(p->p32.work_counter, 0, 4, st) != cudaSuccess) return ST_ECUDA;
   sw32_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, st>>>(p->p32);
   return cudaGetLastError() == cudaSuccess ? ST_OK : ST_ECUDA;
 }
@@ -1735,9 +1751,11 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
     p32.scratch_stride = plan->scratch32_stride;
     p32.open = open;
     p32.ext = ext;
+    p32.n_static = plan->n_static32;
+    p32.band16 = (g16 && plan->n_static32 > 0) ? 1u : 0u;
   }
 
-  plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1;
+  plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1 + plan->p32.band16;
   if (capture) {
     // capture a run into a CUDA graph on the context's own stream (ordered after the upload)
     ST_CUDA(cudaStreamSynchronize(up));
@@ -1811,7 +1829,8 @@ extern "C" int st_plan_profile(st_plan* p, uint32_t cap, int32_t* classes, uint6
   st_ctx* c = p->ctx;
   CTX_GUARD(c);
   if (!n_out || (cap && (!classes || !cells || !ms))) return fail(ST_EINVAL, "st_plan_profile: null output");
-  const uint32_t n = static_cast<uint32_t>(p->classes.size()) + 1;
+  const uint32_t nb = p->p32.band16 ? 1u : 0u;
+  const uint32_t n = static_cast<uint32_t>(p->classes.size()) + 1 + nb;
   *n_out = n;
   if (cap < n) return fail(ST_EINVAL, "st_plan_profile: room for %u entries needed", n);
   cudaEvent_t e0, e1;
@@ -1821,11 +1840,17 @@ extern "C" int st_plan_profile(st_plan* p, uint32_t cap, int32_t* classes, uint6
                           c->stream));
   for (uint32_t i = 0; i < n; ++i) {
     ST_CUDA(cudaEventRecord(e0, c->stream));
-    if (i + 1 < n) {
+    if (i < p->classes.size()) {
       const ClassPlan& cp = p->classes[i];
       kClasses[cp.cls].fn<<<cp.grid, kClasses[cp.cls].W * 32, cp.smem, c->stream>>>(cp.prm);
       classes[i] = cp.cls;
       cells[i] = cp.cells;
+    } else if (nb && i + 1 < n) {
+      // the banded pairs of the static list (their cells are counted with the 32-bit list's)
+      sw16_band_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, c->stream>>>(p->p32);
+      ST_CUDA(cudaMemsetAsync(p->p32.work_counter, 0, 4, c->stream));
+      classes[i] = -2;
+      cells[i] = 0;
     } else {
       // every 16-bit class has run: the list holds the static and the rescored pairs
       sw32_kernel<kWarps32><<<p->grid32, kWarps32 * 32, 0, c->stream>>>(p->p32);
@@ -2111,6 +2136,7 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
     plan->classes.push_back(std::move(cp));
   }
   plan->scratch32_stride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
+  plan->n_static32 = n_list32;
   ST_TRY(grid_sw32(c, n_list32, plan->scratch32_stride, &plan->grid32));
   size_t t_lpt = 0;
   {
@@ -2200,7 +2226,9 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   p32.scratch_stride = plan->scratch32_stride;
   p32.open = open;
   p32.ext = ext;
-  plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1;
+  p32.n_static = plan->n_static32;
+  p32.band16 = (gaps16_ok(open, ext) && plan->n_static32 > 0) ? 1u : 0u;
+  plan->kernels_per_run = static_cast<uint32_t>(plan->classes.size()) + 1 + p32.band16;
   tc.lap("stage 2 (enqueue)");
   if (trace_on())
     for (auto& cp : plan->classes)

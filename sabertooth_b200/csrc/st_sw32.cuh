@@ -42,6 +42,10 @@ struct Sw32Params {
   int32_t* end_t;
   const int32_t* rev_q;
   const int32_t* rev_t;
+  // with band16 set, the entries [0, n_static) that sw16_band_kernel takes (banded pairs with int8 rows;
+  // st_band16.cuh) were scored there and are skipped here
+  uint32_t n_static = 0;
+  uint32_t band16 = 0;
 };
 
 enum Sw32Mode { kSw32Score = 0, kSw32End = 1, kSw32RevEnd = 2 };
@@ -281,7 +285,11 @@ __global__ void __launch_bounds__(WARPS * 32) sw32_kernel(const Sw32Params prm) 
     if (lane == 0) w = atomicAdd(prm.work_counter, 1u);
     w = __shfl_sync(0xFFFFFFFFu, w, 0);
     if (w >= count) break;
-    sw32_pair<kSw32Score>(prm, prm.list[w], bnd);
+    const uint32_t p = prm.list[w];
+    // banded pairs with int8 rows of the static list: scored by the packed band kernel
+    if (prm.band16 && w < prm.n_static && prm.pair_radius[p] >= 0 && prm.prof.fits8[prm.pair_query[p]] != 0)
+      continue;
+    sw32_pair<kSw32Score>(prm, p, bnd);
   }
 }
 

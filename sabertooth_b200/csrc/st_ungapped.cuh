@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
     uint32_t k = threadIdx.x;
     const uint8_t* tp = nullptr;
     int32_t d = 0, p0 = 0, p1 = 0, pa = 0, cur = 0, best = 0;
+    uint4 vnext = make_uint4(0, 0, 0, 0);  // the lane's next target vector, requested a step ahead
     bool live = false;
     auto take = [&](uint32_t j) {
       k = j;
@@ -257,6 +258,7 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
           p0 = static_cast<int32_t>(lo) + d;
           p1 = static_cast<int32_t>(hi) + d;
           pa = p0 & ~15;
+          vnext = *reinterpret_cast<const uint4*>(tp + pa);
         } else {
           p0 = p1 = pa = 0;  // empty: done at once
         }
@@ -268,7 +270,9 @@ __global__ void __launch_bounds__(256) ungapped_hits_refill_kernel(const Ungappe
     while (__any_sync(0xFFFFFFFFu, live)) {
       if (live) {
         if (pa < p1) {
-          const uint4 v = *reinterpret_cast<const uint4*>(tp + pa);
+          // the vector loaded one step ago; the next one is requested before this one is scored
+          const uint4 v = vnext;
+          if (pa + 16 < p1) vnext = *reinterpret_cast<const uint4*>(tp + pa + 16);
           const uint32_t w[4] = {v.x, v.y, v.z, v.w};
           const int32_t qa = pa - d;
           if (narrow) {
