@@ -1377,6 +1377,24 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
       else if (route[i] == 2) list32[k32++] = static_cast<uint32_t>(i);
     }
   }
+  // The 32-bit list longest first (its kernels pull entries in order), by the steps a warp spends on a pair:
+  // passes x (streamed columns + ramp), a banded pair streaming one 256-row pass's band window per pass.
+  // The packed band kernel scores neighbouring entries together, so similar pairs share a warp.
+  if (list32.size() > 1) {
+    std::vector<std::pair<uint64_t, uint32_t>> ord(list32.size());
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < static_cast<int64_t>(list32.size()); ++k) {
+      const uint32_t i = list32[k];
+      const uint64_t m = c->profs[pq[i]].m, tl = tlen[i];
+      const uint64_t P = (m + kSw32Rows - 1) / kSw32Rows;
+      uint64_t w = tl;
+      if (pr[i] >= 0) w = std::min<uint64_t>(tl, static_cast<uint64_t>(kSw32Rows) + 2 * static_cast<uint64_t>(pr[i]));
+      ord[k] = {P * (w + 31), i};
+    }
+    std::stable_sort(ord.begin(), ord.end(), [](const std::pair<uint64_t, uint32_t>& a,
+                                                 const std::pair<uint64_t, uint32_t>& b) { return a.first > b.first; });
+    for (size_t k = 0; k < ord.size(); ++k) list32[k] = ord[k].second;
+  }
   tc.lap("group");
   // per query (in parallel): targets longest first, then the tile class
   std::vector<uint32_t> qlist;

@@ -90,7 +90,7 @@ def test_headroom_overflow_is_rescored_exactly(ctx):
     m = blosum62()
     w = 18  # W, s(W, W) = 11
     rows, targets, centers, radii = [], [], [], []
-    for k, n in enumerate((4000, 4100, 3500, 5000, 3300)):
+    for k, n in enumerate((4000, 4100, 3500, 5000, 3700)):
         q = np.full(n - 50, w, dtype=np.uint8)
         t = np.full(n, w, dtype=np.uint8)
         t[::97] = 3  # a few mismatches
