@@ -48,10 +48,17 @@ void trace_slow(const char* what, Clock::time_point t0, size_t reqs, size_t pair
   if (ms > 5.0) fprintf(stderr, "[st] server %s %.3f ms (%zu requests, %zu pairs)\n", what, ms, reqs, pairs);
 }
 
+// Score rows of one submission: one request's, or a whole bulk submission's
+// (its requests hold consecutive rows of the block).
+struct RowBlock {
+  std::vector<int32_t> rows;
+};
+
 struct Request {
   uint64_t id = 0;
   uint32_t m = 0;
-  std::vector<int32_t> rows;
+  std::shared_ptr<RowBlock> block;  // rows [row0, row0 + m) of the block are this request's
+  uint64_t row0 = 0;
   std::vector<st_pair> pairs;  // profile field filled when batched
   std::vector<int32_t> scores;
   Clock::time_point t_submit, t_done;
@@ -104,28 +111,42 @@ struct st_server {
 int st_server::launch(std::unique_ptr<Batch>& b) {
   std::vector<uint64_t> offs(b->reqs.size() + 1, 0);
   for (size_t i = 0; i < b->reqs.size(); ++i) offs[i + 1] = offs[i] + b->reqs[i]->m;
-  const size_t need = std::max<size_t>(static_cast<size_t>(offs.back()) * 21 * 4, 64);
-  if (arena_bytes < need) {
-    // at least 16 MB, and at least double: freeing pinned memory waits for the
-    // batch in flight, so growth should be rare
-    const size_t want = std::max<size_t>({need + need / 4, 2 * arena_bytes, 16u << 20});
-    if (arena) cudaFreeHost(arena);
-    arena = nullptr;
-    arena_bytes = 0;
-    if (cudaHostAlloc(reinterpret_cast<void**>(&arena), want, cudaHostAllocPortable) != cudaSuccess) {
-      cudaGetLastError();
-      st_internal_set_error("serving: pinned host allocation failed");
-      return ST_ENOMEM;
-    }
-    arena_bytes = want;
-  }
   size_t n_pairs = 0;
   for (size_t i = 0; i < b->reqs.size(); ++i) n_pairs += b->reqs[i]->pairs.size();
-#pragma omp parallel for schedule(dynamic, 16)
-  for (int64_t i = 0; i < static_cast<int64_t>(b->reqs.size()); ++i)
-    if (b->reqs[i]->m) memcpy(arena + offs[i] * 21, b->reqs[i]->rows.data(), b->reqs[i]->rows.size() * 4);
   b->ids.assign(b->reqs.size(), 0);
-  int rc = st_profiles_create(ctx, arena, offs.data(), static_cast<uint32_t>(b->reqs.size()), b->ids.data());
+  // A batch that is one run of consecutive requests of a bulk submission uploads straight from the
+  // submission's rows (the library stages them, copy and upload overlapped); any other batch is gathered
+  // into the pinned arena first.
+  bool run = true;
+  for (size_t i = 1; i < b->reqs.size() && run; ++i)
+    run = b->reqs[i]->block == b->reqs[0]->block && b->reqs[i]->row0 == b->reqs[i - 1]->row0 + b->reqs[i - 1]->m;
+  int rc;
+  if (run && offs.back() > 0) {
+    rc = st_profiles_create(ctx, b->reqs[0]->block->rows.data() + b->reqs[0]->row0 * 21, offs.data(),
+                            static_cast<uint32_t>(b->reqs.size()), b->ids.data());
+  } else {
+    const size_t need = std::max<size_t>(static_cast<size_t>(offs.back()) * 21 * 4, 64);
+    if (arena_bytes < need) {
+      // at least 16 MB, and at least double: freeing pinned memory waits for the
+      // batch in flight, so growth should be rare
+      const size_t want = std::max<size_t>({need + need / 4, 2 * arena_bytes, 16u << 20});
+      if (arena) cudaFreeHost(arena);
+      arena = nullptr;
+      arena_bytes = 0;
+      if (cudaHostAlloc(reinterpret_cast<void**>(&arena), want, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        st_internal_set_error("serving: pinned host allocation failed");
+        return ST_ENOMEM;
+      }
+      arena_bytes = want;
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < static_cast<int64_t>(b->reqs.size()); ++i)
+      if (b->reqs[i]->m)
+        memcpy(arena + offs[i] * 21, b->reqs[i]->block->rows.data() + b->reqs[i]->row0 * 21,
+               static_cast<size_t>(b->reqs[i]->m) * 21 * 4);
+    rc = st_profiles_create(ctx, arena, offs.data(), static_cast<uint32_t>(b->reqs.size()), b->ids.data());
+  }
   if (rc != ST_OK) return rc;
   b->pairs.reserve(n_pairs);
   for (size_t i = 0; i < b->reqs.size(); ++i)
@@ -256,7 +277,8 @@ extern "C" int st_server_submit(st_server* s, const int32_t* rows, uint32_t m, c
   }
   auto r = std::make_shared<Request>();
   r->m = m;
-  r->rows.assign(rows, rows + static_cast<size_t>(m) * 21);
+  r->block = std::make_shared<RowBlock>();
+  r->block->rows.assign(rows, rows + static_cast<size_t>(m) * 21);
   r->pairs.resize(n);
   for (uint32_t i = 0; i < n; ++i)
     r->pairs[i] = st_pair{0, targets[i], band_center ? band_center[i] : 0, band_radius ? band_radius[i] : -1};
@@ -298,12 +320,24 @@ extern "C" int st_server_submit_many(st_server* s, uint32_t n_requests, const in
     }
   }
   std::vector<std::shared_ptr<Request>> rs(n_requests);
+  // the submission's rows in one block (copied in parallel), each request a run of it
+  auto block = std::make_shared<RowBlock>();
+  const uint64_t first = n_requests ? row_offsets[0] : 0, last = n_requests ? row_offsets[n_requests] : 0;
+  block->rows.resize((last - first) * 21);
+  {
+    const int64_t chunk = 1 << 20;  // values per copy task
+    const int64_t total = static_cast<int64_t>(block->rows.size());
+#pragma omp parallel for schedule(static)
+    for (int64_t o = 0; o < total; o += chunk)
+      memcpy(block->rows.data() + o, rows + first * 21 + o, static_cast<size_t>(std::min(chunk, total - o)) * 4);
+  }
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t k = 0; k < static_cast<int64_t>(n_requests); ++k) {
     auto r = std::make_shared<Request>();
     const uint64_t r0 = row_offsets[k], r1 = row_offsets[k + 1], t0 = target_offsets[k], t1 = target_offsets[k + 1];
     r->m = static_cast<uint32_t>(r1 - r0);
-    r->rows.assign(rows + r0 * 21, rows + r1 * 21);
+    r->block = block;
+    r->row0 = r0 - first;
     r->pairs.resize(t1 - t0);
     for (uint64_t i = t0; i < t1; ++i)
       r->pairs[i - t0] = st_pair{0, targets[i], band_center ? band_center[i] : 0, band_radius ? band_radius[i] : -1};

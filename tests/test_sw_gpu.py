@@ -188,7 +188,9 @@ def test_banded_random(ctx):
     got, kern = batch_scores(ctx, rows_list, targets, [(i, i) for i in range(300)], GapCosts(11, 1), centers, radii,
                              with_kernels=True)
     assert np.array_equal(got, np.array(want, dtype=np.int32)), np.nonzero(got != np.array(want))[0][:8]
-    assert set(kern.tolist()) <= {int(Kernel.GPU32), int(Kernel.NONE)}
+    # banded pairs with int8 rows take the packed band kernel (16-bit cells, 32-bit past the headroom)
+    assert set(kern.tolist()) <= {int(Kernel.GPU16), int(Kernel.GPU32), int(Kernel.NONE)}
+    assert (kern == int(Kernel.GPU16)).sum() > 0
 
 
 def test_multipass_queries_and_long_targets(ctx):
