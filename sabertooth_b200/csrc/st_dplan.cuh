@@ -165,6 +165,23 @@ __global__ void __launch_bounds__(256) dp_classify_kernel(const DpIn in, const D
   }
 }
 
+// ---- 32-bit list order: longest first by the steps a warp spends on a pair ----
+// passes x (streamed columns + ramp); a banded pair streams one 256-row pass's band window per pass.  The
+// key is inverted so that an ascending sort puts the costliest first.
+__global__ void __launch_bounds__(256) dp_list_keys_kernel(const DpIn in, const DpWork w, uint32_t n_list,
+                                                            unsigned long long* keys, uint32_t* vals) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_list; k += gridDim.x * blockDim.x) {
+    const uint32_t i = w.list32[k];
+    const unsigned long long m = in.prof.qlen[w.pq[i]], tl = in.db.length[w.pt[i]];
+    const unsigned long long P = (m + 255) / 256;
+    unsigned long long wc = tl;
+    if (w.pr[i] >= 0) wc = min(tl, 256ull + 2ull * static_cast<unsigned long long>(w.pr[i]));
+    const unsigned long long cost = min(P * (wc + 31), (1ull << 48) - 1);
+    keys[k] = ((1ull << 48) - 1) - cost;
+    vals[k] = i;
+  }
+}
+
 // ---- pick: one warp per query ----
 __global__ void __launch_bounds__(256) dp_pick_kernel(const DpIn in, const DpWork w, const DpClasses cls) {
   const uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;

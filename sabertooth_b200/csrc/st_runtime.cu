@@ -2156,6 +2156,28 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   plan->scratch32_stride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
   plan->n_static32 = n_list32;
   ST_TRY(grid_sw32(c, n_list32, plan->scratch32_stride, &plan->grid32));
+  if (n_list32 > 1) {
+    // the 32-bit list longest first (the packed band kernel scores neighbouring entries together), in the
+    // stage-1 buffers that are free now: both key buffers and the value buffer the pair sort left unused
+    uint32_t* vfree = w.vals_sorted == w.vals ? w.vals_alt : w.vals;
+    size_t t_ls = 0;
+    {
+      cub::DoubleBuffer<ull> lk(nullptr, nullptr);
+      cub::DoubleBuffer<uint32_t> lv(nullptr, nullptr);
+      ST_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t_ls, lk, lv, static_cast<int>(n_list32), 0, 48, s1));
+    }
+    if (t_ls <= t_tmp) {
+      const uint32_t gl = static_cast<uint32_t>(std::min<uint64_t>((n_list32 + 255) / 256,
+                                                                   static_cast<uint64_t>(c->sms) * 8));
+      dp_list_keys_kernel<<<gl, 256, 0, s1>>>(in, w, n_list32, w.keys, vfree);
+      cub::DoubleBuffer<ull> lk(w.keys, w.keys_alt);
+      cub::DoubleBuffer<uint32_t> lv(vfree, w.list32);
+      ST_CUDA(cub::DeviceRadixSort::SortPairs(tmp, t_ls, lk, lv, static_cast<int>(n_list32), 0, 48, s1));
+      if (lv.Current() != w.list32)
+        ST_CUDA(cudaMemcpyAsync(w.list32, lv.Current(), static_cast<size_t>(n_list32) * 4, cudaMemcpyDeviceToDevice,
+                                s1));
+    }
+  }
   size_t t_lpt = 0;
   {
     cub::DoubleBuffer<ull> ck(nullptr, nullptr);
