@@ -736,7 +736,8 @@ def ungapped_measure(ctx, args):
             "ms_per_step": round(ms, 3), "mhits_per_s": round(n / ms / 1e3, 1),
             "algorithmic_bytes": int(ab), "runs": n_runs,
             "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(gbs / peak, 4), "traffic": read_traffic("ungapped_config2.md")},
+                         "frac": round(gbs / peak, 4), "traffic": read_traffic("ungapped_config2.md"),
+                         "peak_source": hbm_peak()[1]},
             "matches_cpu_baseline": bool(np.array_equal(got, want)), "cpu_baseline_matches_scalar_sample": scalar_ok,
             "cpu_baseline": {"value": round(n / t_cpu / 1e6, 2), "unit": "Mhits/s", "cores": os.cpu_count(),
                              "kind": "port", "sample": f"the whole workload ({n} hits), median of 3 runs: the "
@@ -1239,11 +1240,17 @@ def long_mix_measure(ctx, args):
 
 def hbm_peak_gbs():
     """The measured copy bandwidth of this pool's B200s, or the fallback figure."""
+    return hbm_peak()[0]
+
+
+def hbm_peak():
+    """(GB/s, source): MEASURED_PEAKS.json's measured copy bandwidth when the file is present, else the
+    pool's earlier measurement (6.65 TB/s)."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        return float(json.load(open(p))["hbm_gbs"])
+        return float(json.load(open(p))["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except Exception:
-        return 6650.0
+        return 6650.0, "fallback (6.65 TB/s, an earlier copy-bandwidth measurement on this pool)"
 
 
 def serving_measure(ctx, args):

@@ -261,6 +261,14 @@ extern "C" st_server* st_server_create(st_ctx* ctx, int32_t open, int32_t ext, u
   s->ctx = ctx;
   s->open = open;
   s->ext = ext;
+  // the pinned arena that gathers a batch's rows, allocated now rather than by the first batch that
+  // gathers (a large pinned allocation stalls the worker for milliseconds)
+  if (cudaHostAlloc(reinterpret_cast<void**>(&s->arena), 16u << 20, cudaHostAllocPortable) == cudaSuccess) {
+    s->arena_bytes = 16u << 20;
+  } else {
+    cudaGetLastError();
+    s->arena = nullptr;
+  }
   s->max_pairs = max_batch_pairs ? max_batch_pairs : (1ull << 22);
   s->budget = hbm_budget_bytes ? hbm_budget_bytes : (16ull << 30);
   st_server* p = s.get();
