@@ -84,6 +84,20 @@ static uint64_t env_u64(const char* name, uint64_t dflt) {
   return strtoull(v, nullptr, 10);
 }
 
+// Traces a driver call of the memory helpers that took longer than a millisecond.
+struct SlowCall {
+  const char* what;
+  size_t bytes;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  SlowCall(const char* w, size_t b) : what(w), bytes(b) {}
+  ~SlowCall() {
+    if (!trace_on()) return;
+    const double ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (ms > 1.0) fprintf(stderr, "[st] slow %s %zu bytes %.3f ms\n", what, bytes, ms);
+  }
+};
+
 struct TraceClock {
   const char* what;
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -129,6 +143,7 @@ struct DevMem {
   ~DevMem() { release(); }
   void release() {
     if (p) {
+      SlowCall sc("cudaFree", bytes);
       cudaFree(p);
       if (mt) mt->used -= bytes;
     }
@@ -147,7 +162,11 @@ static int dev_alloc(MemTracker* mt, DevMem& m, size_t bytes) {
   if (mt->budget && mt->used + bytes > mt->budget)
     return fail(ST_ENOMEM, "device memory budget exceeded: %zu used + %zu requested > %zu budget", mt->used,
                 bytes, mt->budget);
-  cudaError_t e = cudaMalloc(&m.p, bytes);
+  cudaError_t e;
+  {
+    SlowCall sc("cudaMalloc", bytes);
+    e = cudaMalloc(&m.p, bytes);
+  }
   if (e != cudaSuccess) {
     m.p = nullptr;
     return fail(ST_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
@@ -179,6 +198,7 @@ struct Pinned {
         want = cls / 8 * k;
         break;
       }
+    SlowCall sc("pinned regrow", want);
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
@@ -1119,11 +1139,14 @@ struct st_plan {
 
 static int occupancy_grid(st_ctx* c, const void* fn, int threads, size_t smem, uint32_t work, uint32_t* grid);
 
-// Grid of the 32-bit kernel: a few CTAs for the rare rescores; for a long
-// static list (banded pairs, wide rows, gap costs outside 16 bits) as many as
-// the SMs hold, bounded so its pass scratch stays within 1 GiB.
-static int grid_sw32(st_ctx* c, uint64_t n_static, uint32_t scratch_stride, uint32_t* grid) {
-  const uint64_t want = std::max<uint64_t>(2ull * c->sms, (n_static + kWarps32 - 1) / kWarps32);
+// Grid of the 32-bit kernel: two CTAs per SM for the rare rescores the 16-bit
+// classes flag at run time; for a long static list (banded pairs, wide rows,
+// gap costs outside 16 bits) as many as the SMs hold; never more warps than
+// the run has pairs (a one-pair batch would otherwise carry pass scratch lines
+// for 2 x 148 CTAs); bounded so the pass scratch stays within 1 GiB.
+static int grid_sw32(st_ctx* c, uint64_t n_static, uint64_t n_pairs, uint32_t scratch_stride, uint32_t* grid) {
+  const uint64_t want = std::min<uint64_t>(std::max<uint64_t>(2ull * c->sms, (n_static + kWarps32 - 1) / kWarps32),
+                                           std::max<uint64_t>(1, (n_pairs + kWarps32 - 1) / kWarps32));
   ST_TRY(occupancy_grid(c, reinterpret_cast<const void*>(sw32_kernel<kWarps32>), kWarps32 * 32, 0,
                         static_cast<uint32_t>(std::min<uint64_t>(want, 1u << 20)), grid));
   if (scratch_stride) {
@@ -1610,7 +1633,7 @@ static int plan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open,
   }
   plan->scratch32_stride = max_m32 > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
   plan->n_static32 = static_cast<uint32_t>(list32.size());
-  ST_TRY(grid_sw32(c, plan->n_static32, plan->scratch32_stride, &plan->grid32));
+  ST_TRY(grid_sw32(c, plan->n_static32, n, plan->scratch32_stride, &plan->grid32));
 
   // one device arena: [initialised data (one upload)] [scratch]
   size_t off = 0;
@@ -2155,7 +2178,7 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
   }
   plan->scratch32_stride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
   plan->n_static32 = n_list32;
-  ST_TRY(grid_sw32(c, n_list32, plan->scratch32_stride, &plan->grid32));
+  ST_TRY(grid_sw32(c, n_list32, n, plan->scratch32_stride, &plan->grid32));
   if (n_list32 > 1) {
     // the 32-bit list longest first (the packed band kernel scores neighbouring entries together), in the
     // stage-1 buffers that are free now: both key buffers and the value buffer the pair sort left unused
@@ -2603,7 +2626,7 @@ static int end_pairs_run(st_ctx* c, const DeviceDb& db, const uint32_t* pq_h, co
   if (n > 0xFFFFFFF0ull) return fail(ST_EINVAL, "too many pairs");
   uint32_t grid = 0;
   const uint32_t sstride = max_m > static_cast<uint32_t>(kSw32Rows) ? max_len : 0;
-  ST_TRY(grid_sw32(c, n, sstride, &grid));
+  ST_TRY(grid_sw32(c, n, n, sstride, &grid));
   size_t off = 0;
   auto carve = [&](size_t bytes) {
     const size_t o = off;
