@@ -145,6 +145,43 @@ def test_unsorted_hits_are_still_exact(ctx, hit_kernel):
         ctx.free_profile(i)
 
 
+@pytest.mark.parametrize("wide", [False, True])
+def test_hit_edges(ctx, hit_kernel, wide):
+    """Every diagonal of short and vector-edge lengths (queries of 1, 15, 16, 17, 33 and 1,024 residues, targets
+    of 1, 15, 16, 17, 32 and 48 residues, so windows start and end on and off the 16-byte target vectors and
+    targets end on and off the arena's 16-byte boundaries), hits in query runs and shuffled, with int8 rows and
+    with rows outside int8 (the int32 path)."""
+    rng = np.random.default_rng(31)
+    qlens, tlens = [1, 15, 16, 17, 33, 1024], [1, 15, 16, 17, 32, 48]
+    span = 300 if wide else 11
+    rows = [rng.integers(-span, span + 1, size=(m, 21)).astype(np.int32) for m in qlens]
+    seqs = [rng.integers(0, 21, size=n).astype(np.uint8) for n in tlens]
+    offs = np.zeros(len(seqs) + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum([len(x) for x in seqs])
+    ctx.upload_db(np.concatenate(seqs), offs)
+    ids = ctx.create_profiles(rows)
+    q, t, d = [], [], []
+    for qi, m in enumerate(qlens):
+        for ti, n in enumerate(tlens):
+            for dd in range(-(m - 1) - 2, n + 2):
+                if abs(dd) > 80 and rng.random() < 0.9:
+                    continue
+                q.append(qi)
+                t.append(ti)
+                d.append(dd)
+    from sabertooth_b200.dtypes import HIT_DTYPE
+    hits = np.zeros(len(q), dtype=HIT_DTYPE)
+    hits["query"], hits["target"], hits["diag"] = q, t, d
+    want = O.ungapped_hits(O.Arena(rows, seqs), hits["query"], hits["target"], hits["diag"])
+    for order in (np.arange(len(hits)), np.random.default_rng(1).permutation(len(hits))):
+        h = hits[order].copy()
+        h["query"] = ids[h["query"]]
+        got = ctx.ungapped_hits(h, with_pairs=False)
+        assert np.array_equal(got, want[order])
+    for i in ids:
+        ctx.free_profile(i)
+
+
 def test_lanes_carry_arena_slices_as_the_reference_builds_them(ctx):
     """Lanes whose target is a slice of the uploaded arena (src/ungapped.rs:265-270, built from
     index.seq(tid) in src/prefilter.rs:1563-1568), through st_ungapped_score_slices: whole sequences
