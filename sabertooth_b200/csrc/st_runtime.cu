@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -290,6 +291,7 @@ struct CallSlot {
   cudaStream_t s = nullptr;
   cudaEvent_t ev_in = nullptr;    // the context stream's work before the call (profile tables ready)
   cudaEvent_t ev_done = nullptr;  // the call's result is in the pinned block
+  uint64_t epoch = 0;             // the context's profile epoch the slot's stream is ordered after
   Pinned pin;
   DevMem stage, scratch;
 };
@@ -348,6 +350,8 @@ struct st_ctx {
   // st_sw_score calls in flight: slots handed out under call_mu (not the context lock)
   static constexpr size_t kMaxCallSlots = 32;
   std::mutex call_mu;
+  std::shared_mutex call_rw;  // held shared by per-call scorings from their checks to their launches
+  uint64_t prof_epoch = 1;    // changes whenever profile layouts or tables are (re)written on the streams
   std::condition_variable call_cv;
   std::vector<std::unique_ptr<CallSlot>> call_slots;
   std::vector<CallSlot*> call_idle;
@@ -562,7 +566,10 @@ static int sync_profiles(st_ctx* c) {
   auto up = [&](DevMem& d, size_t off, size_t bytes) -> int {
     if (d.bytes < bytes) {
       ST_CUDA(cudaStreamSynchronize(c->stream));  // queued work may read the old table
-      ST_TRY(calls_drain(c));                     // and so may per-call scorings in flight
+      // and so may per-call scorings: none is between its checks and its launches (they hold the call
+      // lock shared), and those launched are waited for
+      std::unique_lock<std::shared_mutex> calls(c->call_rw);
+      ST_TRY(calls_drain(c));
       ST_TRY(dev_alloc(&c->mt, d, bytes * 2));
     }
     ST_CUDA(cudaMemcpyAsync(d.p, h + off, bytes, cudaMemcpyHostToDevice, c->stream));
@@ -580,6 +587,7 @@ static int sync_profiles(st_ctx* c) {
   c->meta_used[slot] = true;
   c->max_m = max_m;
   c->prof_dirty = false;
+  ++c->prof_epoch;
   return ST_OK;
 }
 
@@ -651,6 +659,10 @@ extern "C" st_ctx* st_init(int device, size_t hbm_budget_bytes) {
   if (prop.major < 10) {
     fail(ST_ECUDA, "device %d is sm_%d%d; this library is built for sm_100a (B200)", device, prop.major,
          prop.minor);
+    return nullptr;
+  }
+  if (!prop.unifiedAddressing) {  // per-call scorings write their results straight into pinned host memory
+    fail(ST_ECUDA, "device %d lacks unified addressing", device);
     return nullptr;
   }
   auto c = std::make_unique<st_ctx>();
@@ -960,6 +972,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   ST_CUDA(cudaGetLastError());
   ST_CUDA(cudaEventRecord(c->prof_ev, bs));
   c->prof_ev_set = true;
+  ++c->prof_epoch;
   ST_CUDA(cudaEventSynchronize(c->copy_ev));
   tc.lap("upload");
   int bi;
@@ -2790,12 +2803,26 @@ extern "C" int st_sw_align_span_pairs(st_ctx* c, const st_pair* pairs, uint64_t 
 // ---------------------------------------------------------------------------
 // plain per-call SW (one pair, one launch of each kernel, blocking)
 // ---------------------------------------------------------------------------
-// Set-up and launches of one per-call scoring on slot `sl` (context lock held). *queued says whether
-// work was launched; its score and kernel tag then land in the slot's pinned block at `*res_off`.
-static int sw_score_enqueue(st_ctx* c, CallSlot* sl, uint32_t profile, const uint8_t* target, uint32_t n,
-                            int32_t open, int32_t ext, int32_t* score, uint32_t* kernel, bool* queued,
-                            size_t* res_off) {
-  *queued = false;
+// One per-call scoring on slot `sl`, in two phases.  sw_score_prepare runs under the context lock: the
+// checks, the profile tables, the sizes, the slot's buffers (device memory is accounted to the context) and,
+// when profiles changed since the slot's last call, the event that orders the call after the context
+// stream's work so far.  sw_score_launch runs outside it, on the slot's own stream: the staged inputs, the
+// copy and the launches.  Between the two the call holds the context's call lock shared, so the profile
+// tables it captured cannot be reallocated under it (table growth takes that lock exclusively, then waits
+// for the calls' streams).
+struct SwCall {
+  uint32_t profile = 0, n = 0, k = 0, P = 1, rows = 0, ncols = 0, sstride = 0;
+  int32_t open = 0, ext = 0;
+  bool use16 = false, wait = false;
+  size_t tbytes = 0, o_off = 0, o_len = 0, o_pt = 0, o_pq = 0, o_pc = 0, o_pr = 0, o_cta = 0, o_wt = 0, o_slots = 0,
+         o_cnt = 0, o_list = 0, o_zline = 0, total = 0;
+  DeviceProfiles pv;
+};
+
+// *launch says whether there is work to launch (an empty query or target scores 0 at once).
+static int sw_score_prepare(st_ctx* c, CallSlot* sl, uint32_t profile, uint32_t n, int32_t open, int32_t ext,
+                            int32_t* score, uint32_t* kernel, SwCall* w, bool* launch) {
+  *launch = false;
   ST_TRY(check_profile(c, profile));
   ST_TRY(sync_profiles(c));
   const ProfileMeta& pm = c->profs[profile];
@@ -2806,166 +2833,196 @@ static int sw_score_enqueue(st_ctx* c, CallSlot* sl, uint32_t profile, const uin
   }
   // staging block (one host->device copy per call):
   //   [target codes, padded] [db offset u64] [db length u32] [pair: target u32, query u32, center i32, radius i32]
-  //   [cta task] [warp task] [slots x64] [counters x(kNumClasses+2)] [32-bit list u32] [score i32, kernel u32]
-  const size_t tbytes = up16(n) + 32;
-  size_t o = tbytes;
-  const size_t o_off = o; o += 8;
-  const size_t o_len = o; o += 4;
-  const size_t o_pt = o; o += 4;
-  const size_t o_pq = o; o += 4;
-  const size_t o_pc = o; o += 4;
-  const size_t o_pr = o; o += 4;
+  //   [cta task] [warp task] [slots x64] [counters x(kNumClasses+2)] [32-bit list u32] [first-pass boundary]
+  // and, behind it in the pinned block only, the score and kernel tag the kernels write
+  w->profile = profile;
+  w->n = n;
+  w->open = open;
+  w->ext = ext;
+  w->tbytes = up16(n) + 32;
+  size_t o = w->tbytes;
+  w->o_off = o; o += 8;
+  w->o_len = o; o += 4;
+  w->o_pt = o; o += 4;
+  w->o_pq = o; o += 4;
+  w->o_pc = o; o += 4;
+  w->o_pr = o; o += 4;
   o = up16(o);
-  const size_t o_cta = o; o += sizeof(Sw16CtaTask);
-  const size_t o_wt = o; o += sizeof(Sw16WarpTask);
+  w->o_cta = o; o += sizeof(Sw16CtaTask);
+  w->o_wt = o; o += sizeof(Sw16WarpTask);
   o = up16(o);  // slot records are read as 16-byte vectors
-  const size_t o_slots = o; o += 64 * sizeof(Sw16Slot);
-  const size_t o_cnt = o; o += (kNumClasses + 2) * 4;
-  const size_t o_list = o; o += 4;
-  const size_t o_res = o; o += 8;
+  w->o_slots = o; o += 64 * sizeof(Sw16Slot);
+  w->o_cnt = o; o += (kNumClasses + 2) * 4;
+  w->o_list = o; o += 4;
   o = up16(o);
-  const size_t o_zline = o; o += (static_cast<size_t>(std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)))) + 
-                                  static_cast<size_t>(32 * 4 + 16)) * sizeof(uint2);
-  const size_t total = up16(o);
-  const bool use16 = pm.fits8 && gaps16_ok(open, ext);
-  int k = 0;
-  uint32_t P = 1, rows = 0;
-  if (use16) {
-    k = tuning_pick_single(&c->tuning, pm.m, n);
-    rows = kClasses[k].G * kClasses[k].R;
-    P = (pm.m + rows - 1) / rows;
-    if (static_cast<size_t>(kProfRows) * P * rows > static_cast<size_t>(g_class_smem[k]))
+  w->o_zline = o; o += (static_cast<size_t>(std::max<uint32_t>(32, static_cast<uint32_t>(up16(n)))) +
+                        static_cast<size_t>(32 * 4 + 16)) * sizeof(uint2);
+  w->total = up16(o);
+  w->use16 = pm.fits8 && gaps16_ok(open, ext);
+  w->k = 0;
+  w->P = 1;
+  w->rows = 0;
+  if (w->use16) {
+    w->k = static_cast<uint32_t>(tuning_pick_single(&c->tuning, pm.m, n));
+    w->rows = kClasses[w->k].G * kClasses[w->k].R;
+    w->P = (pm.m + w->rows - 1) / w->rows;
+    if (static_cast<size_t>(kProfRows) * w->P * w->rows > static_cast<size_t>(g_class_smem[w->k]))
       return fail(ST_EINVAL, "query of %u rows too long for the shared-memory profile", pm.m);
   }
-  uint32_t ncols = std::max<uint32_t>(32, static_cast<uint32_t>(up4(n)));
-  if (use16 && P > 1) ncols = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(kClasses[k].C * kClasses[k].G)));
-  const uint32_t sstride = std::max<uint32_t>(ncols, static_cast<uint32_t>(up16(n) + 32));
+  w->ncols = std::max<uint32_t>(32, static_cast<uint32_t>(up4(n)));
+  if (w->use16 && w->P > 1)
+    w->ncols = std::max<uint32_t>(w->ncols, static_cast<uint32_t>(up16(kClasses[w->k].C * kClasses[w->k].G)));
+  w->sstride = std::max<uint32_t>(w->ncols, static_cast<uint32_t>(up16(n) + 32));
   // any warp of the CTA may take the task: room for every group of the CTA
-  const size_t scratch_need = static_cast<size_t>(kClasses[k].W) * 8 * sstride * sizeof(uint2);
+  const size_t scratch_need = static_cast<size_t>(kClasses[w->k].W) * 8 * w->sstride * sizeof(uint2);
   if (!sl->s) {
     ST_CUDA(cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
     ST_CUDA(cudaEventCreateWithFlags(&sl->ev_in, cudaEventDisableTiming));
     ST_CUDA(cudaEventCreateWithFlags(&sl->ev_done, cudaEventDisableTiming));
   }
   // the slot's previous call has been waited for, so its pinned block and device buffers are free
-  ST_TRY(sl->pin.reserve(total + 16));
-  if (sl->stage.bytes < total) ST_TRY(dev_alloc(&c->mt, sl->stage, total * 2));
+  ST_TRY(sl->pin.reserve(w->total + 16));
+  if (sl->stage.bytes < w->total) ST_TRY(dev_alloc(&c->mt, sl->stage, w->total * 2));
   if (sl->scratch.bytes < scratch_need) ST_TRY(dev_alloc(&c->mt, sl->scratch, scratch_need * 2));
+  w->pv = prof_view(c);
+  // the profile tables and layouts are written in the context stream's order: unless none changed since the
+  // slot's last call (its stream is ordered after that point already), start after the stream's work so far
+  w->wait = sl->epoch != c->prof_epoch;
+  if (w->wait) {
+    ST_CUDA(cudaEventRecord(sl->ev_in, c->stream));
+    sl->epoch = c->prof_epoch;
+  }
+  c->launches += w->use16 ? 2 : 1;
+  *launch = true;
+  return ST_OK;
+}
+
+// The call's inputs staged and uploaded and its kernels launched; they write the score and kernel tag
+// straight into the slot's pinned block at *res_off (pinned memory is device-accessible under unified
+// addressing, so no copy back is queued), and ev_done marks their arrival.
+static int sw_score_launch(CallSlot* sl, const uint8_t* target, const SwCall& w, size_t* res_off) {
+  const uint32_t n = w.n;
   char* h = sl->pin.as<char>();
-  memset(h, 0, total);
+  memset(h, 0, w.total);
   for (uint32_t i = 0; i < n; ++i) h[i] = static_cast<char>(target[i] < kSentinel ? target[i] : kSentinel);
-  memset(h + n, kSentinel, tbytes - n);
-  *reinterpret_cast<uint64_t*>(h + o_off) = 0;
-  *reinterpret_cast<uint32_t*>(h + o_len) = n;
-  *reinterpret_cast<uint32_t*>(h + o_pt) = 0;
-  *reinterpret_cast<uint32_t*>(h + o_pq) = profile;
-  *reinterpret_cast<int32_t*>(h + o_pc) = 0;
-  *reinterpret_cast<int32_t*>(h + o_pr) = -1;  // no band
-  Sw16CtaTask ct{profile, 0, 1, P * std::max<uint32_t>(rows, 1)};
-  Sw16WarpTask wt{0, ncols};
-  memcpy(h + o_cta, &ct, sizeof(ct));
-  memcpy(h + o_wt, &wt, sizeof(wt));
-  Sw16Slot* slots = reinterpret_cast<Sw16Slot*>(h + o_slots);
+  memset(h + n, kSentinel, w.tbytes - n);
+  *reinterpret_cast<uint64_t*>(h + w.o_off) = 0;
+  *reinterpret_cast<uint32_t*>(h + w.o_len) = n;
+  *reinterpret_cast<uint32_t*>(h + w.o_pt) = 0;
+  *reinterpret_cast<uint32_t*>(h + w.o_pq) = w.profile;
+  *reinterpret_cast<int32_t*>(h + w.o_pc) = 0;
+  *reinterpret_cast<int32_t*>(h + w.o_pr) = -1;  // no band
+  Sw16CtaTask ct{w.profile, 0, 1, w.P * std::max<uint32_t>(w.rows, 1)};
+  Sw16WarpTask wt{0, w.ncols};
+  memcpy(h + w.o_cta, &ct, sizeof(ct));
+  memcpy(h + w.o_wt, &wt, sizeof(wt));
+  Sw16Slot* slots = reinterpret_cast<Sw16Slot*>(h + w.o_slots);
   for (int s = 0; s < 64; ++s) slots[s] = Sw16Slot{kNoPair, 0, 0, 0};
   slots[0] = Sw16Slot{0, 0, static_cast<uint32_t>(up16(n)), n};  // the staged target sits at offset 0
-  uint32_t* cnt = reinterpret_cast<uint32_t*>(h + o_cnt);
-  if (!use16) cnt[kNumClasses + 1] = 1;  // the pair goes straight to the 32-bit list
-  *reinterpret_cast<uint32_t*>(h + o_list) = 0;
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(h + w.o_cnt);
+  if (!w.use16) cnt[kNumClasses + 1] = 1;  // the pair goes straight to the 32-bit list
+  *reinterpret_cast<uint32_t*>(h + w.o_list) = 0;
   {
-    uint2* z = reinterpret_cast<uint2*>(h + o_zline);
-    const size_t nz = (total - o_zline) / sizeof(uint2);
-    for (size_t i = 0; i < nz; ++i) z[i] = make_uint2(0u, pk_splat(-open));
+    uint2* z = reinterpret_cast<uint2*>(h + w.o_zline);
+    const size_t nz = (w.total - w.o_zline) / sizeof(uint2);
+    for (size_t i = 0; i < nz; ++i) z[i] = make_uint2(0u, pk_splat(-w.open));
   }
+  *res_off = w.total;
+  int32_t* h_res = sl->pin.as<int32_t>(*res_off);
+  h_res[0] = 0;
+  h_res[1] = 0;
   char* d = sl->stage.as<char>();
   cudaStream_t st = sl->s;
-  // the profile tables and layouts are written in the context stream's order: start after its work so far
-  ST_CUDA(cudaEventRecord(sl->ev_in, c->stream));
-  ST_CUDA(cudaStreamWaitEvent(st, sl->ev_in, 0));
-  ST_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, st));
+  if (w.wait) ST_CUDA(cudaStreamWaitEvent(st, sl->ev_in, 0));
+  ST_CUDA(cudaMemcpyAsync(d, h, w.total, cudaMemcpyHostToDevice, st));
   DeviceDb db;
   db.arena = reinterpret_cast<const uint8_t*>(d);
-  db.offset = reinterpret_cast<const uint64_t*>(d + o_off);
-  db.length = reinterpret_cast<const uint32_t*>(d + o_len);
+  db.offset = reinterpret_cast<const uint64_t*>(d + w.o_off);
+  db.length = reinterpret_cast<const uint32_t*>(d + w.o_len);
   db.n_seqs = 1;
-  const DeviceProfiles pv = prof_view(c);
-  uint32_t* d_cnt = reinterpret_cast<uint32_t*>(d + o_cnt);
-  int32_t* d_score = reinterpret_cast<int32_t*>(d + o_res);
-  uint32_t* d_kern = reinterpret_cast<uint32_t*>(d + o_res + 4);
-  uint32_t* d_list = reinterpret_cast<uint32_t*>(d + o_list);
-  if (use16) {
+  uint32_t* d_cnt = reinterpret_cast<uint32_t*>(d + w.o_cnt);
+  int32_t* d_score = h_res;
+  uint32_t* d_kern = reinterpret_cast<uint32_t*>(h_res + 1);
+  uint32_t* d_list = reinterpret_cast<uint32_t*>(d + w.o_list);
+  if (w.use16) {
     Sw16Params prm;
     prm.arena = reinterpret_cast<const uint8_t*>(d);
-    prm.prof = pv;
-    prm.cta_tasks = reinterpret_cast<const Sw16CtaTask*>(d + o_cta);
+    prm.prof = w.pv;
+    prm.cta_tasks = reinterpret_cast<const Sw16CtaTask*>(d + w.o_cta);
     prm.n_cta_tasks = 1;
-    prm.warp_tasks = reinterpret_cast<const Sw16WarpTask*>(d + o_wt);
-    prm.slots = reinterpret_cast<const Sw16Slot*>(d + o_slots);
+    prm.warp_tasks = reinterpret_cast<const Sw16WarpTask*>(d + w.o_wt);
+    prm.slots = reinterpret_cast<const Sw16Slot*>(d + w.o_slots);
     prm.scores = d_score;
     prm.kernels = d_kern;
     prm.ovf_count = d_cnt + kNumClasses + 1;
     prm.ovf_pairs = d_list;
-    prm.work_counter = d_cnt + k;
+    prm.work_counter = d_cnt + w.k;
     prm.scratch = sl->scratch.as<uint2>();
-    prm.zline = reinterpret_cast<const uint2*>(d + o_zline);
-    prm.scratch_stride = sstride;
-    prm.open = open;
-    prm.ext = ext;
-    kClasses[k].fn<<<1, kClasses[k].W * 32, kProfRows * P * rows, st>>>(prm);
-    ++c->launches;
+    prm.zline = reinterpret_cast<const uint2*>(d + w.o_zline);
+    prm.scratch_stride = w.sstride;
+    prm.open = w.open;
+    prm.ext = w.ext;
+    kClasses[w.k].fn<<<1, kClasses[w.k].W * 32, kProfRows * w.P * w.rows, st>>>(prm);
   }
   // the 32-bit kernel scores the pair only when it is in the list (headroom reached, or not 16-bit eligible)
   Sw32Params p32;
   p32.db = db;
-  p32.prof = pv;
+  p32.prof = w.pv;
   p32.list = d_list;
   p32.list_count = d_cnt + kNumClasses + 1;
-  p32.pair_query = reinterpret_cast<const uint32_t*>(d + o_pq);
-  p32.pair_target = reinterpret_cast<const uint32_t*>(d + o_pt);
-  p32.pair_center = reinterpret_cast<const int32_t*>(d + o_pc);
-  p32.pair_radius = reinterpret_cast<const int32_t*>(d + o_pr);
+  p32.pair_query = reinterpret_cast<const uint32_t*>(d + w.o_pq);
+  p32.pair_target = reinterpret_cast<const uint32_t*>(d + w.o_pt);
+  p32.pair_center = reinterpret_cast<const int32_t*>(d + w.o_pc);
+  p32.pair_radius = reinterpret_cast<const int32_t*>(d + w.o_pr);
   p32.scores = d_score;
   p32.kernels = d_kern;
   p32.work_counter = d_cnt + kNumClasses;
   p32.scratch = reinterpret_cast<int2*>(sl->scratch.p);
   p32.scratch_stride = static_cast<uint32_t>(up16(n) + 32);
-  p32.open = open;
-  p32.ext = ext;
+  p32.open = w.open;
+  p32.ext = w.ext;
   sw32_kernel<kWarps32><<<1, kWarps32 * 32, 0, st>>>(p32);
-  ++c->launches;
   ST_CUDA(cudaGetLastError());
-  // score and kernel tag into the pinned block behind the staged inputs
-  *res_off = up16(total);
-  ST_CUDA(cudaMemcpyAsync(h + *res_off, d_score, 8, cudaMemcpyDeviceToHost, st));
   ST_CUDA(cudaEventRecord(sl->ev_done, st));
-  *queued = true;
   return ST_OK;
 }
 
 // The plain per-call drop-in for sw_score_with.  Calls from several host threads proceed at once: each
-// takes a call slot (its own stream and buffers), holds the context lock only while it sets up and
-// launches, and waits for its result outside the lock.
+// takes a call slot (its own stream and buffers), holds the context lock only while it checks and sizes
+// the call, stages and launches on its own stream outside that lock, and waits for its result.
 extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
                            int32_t* score, uint32_t* kernel) {
   if (!c) return fail(ST_EINVAL, "null context");
   if (!score || (n && !target)) return fail(ST_EINVAL, "st_sw_score: null argument");
   CallSlot* sl = call_acquire(c);
-  bool queued = false;
+  SwCall w;
+  bool launch = false, queued = false;
   size_t res_off = 0;
   int rc;
+  std::shared_lock<std::shared_mutex> tables;  // the profile tables stay while this call's work is enqueued
   {
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     rc = cudaSetDevice(c->device) == cudaSuccess ? ST_OK : fail(ST_ECUDA, "cudaSetDevice(%d) failed", c->device);
-    if (rc == ST_OK) rc = sw_score_enqueue(c, sl, profile, target, n, open, ext, score, kernel, &queued, &res_off);
+    if (rc == ST_OK) rc = sw_score_prepare(c, sl, profile, n, open, ext, score, kernel, &w, &launch);
+    if (rc == ST_OK && launch) tables = std::shared_lock<std::shared_mutex>(c->call_rw);
   }
+  if (rc == ST_OK && launch) {
+    rc = sw_score_launch(sl, target, w, &res_off);
+    queued = rc == ST_OK;
+  }
+  if (tables.owns_lock()) tables.unlock();
   if (queued) {
     const cudaError_t e = cudaEventSynchronize(sl->ev_done);
     if (e != cudaSuccess) {
       rc = fail(ST_ECUDA, "st_sw_score: %s", cudaGetErrorString(e));
-    } else if (rc == ST_OK) {
+    } else {
       const int32_t* res = sl->pin.as<int32_t>(res_off);
       *score = res[0];
       if (kernel) *kernel = static_cast<uint32_t>(res[1]);
     }
+  } else if (launch && sl->s) {
+    cudaStreamSynchronize(sl->s);  // a failed launch phase: let whatever was queued finish before the slot's reuse
+    cudaGetLastError();
   }
   call_release(c, sl);
   return rc;
