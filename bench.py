@@ -1103,25 +1103,39 @@ def gate_window_bytes(w, params):
     return int(np.maximum(hi - lo, 0)[keep].sum())
 
 
-def _timed_plans(ctx, plans, steps, warmup=3):
-    """Device time of one step = every plan run once, on one stream, L2 flushed before each step."""
+def _timed_plans(ctx, plans, steps, warmup=3, concurrent=False):
+    """Device time of one step = every plan run once, L2 flushed before each step; the plans run one after
+    the other on one stream, or (concurrent) each on its own stream forked from the timing stream and joined
+    back before the end event, as independent batches in flight together run."""
     import torch
     st = torch.cuda.Stream()
-    ctx.set_stream(st.cuda_stream)
+    side = [torch.cuda.Stream() for _ in plans] if concurrent else []
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        if not concurrent:
+            ctx.set_stream(st.cuda_stream)
+            for p in plans:
+                p.run()
+            return
+        for p, s_ in zip(plans, side):
+            s_.wait_stream(st)
+            ctx.set_stream(s_.cuda_stream)
+            p.run()
+        for s_ in side:
+            st.wait_stream(s_)
+
     ts = []
     with torch.cuda.stream(st):
         for _ in range(warmup):
-            for p in plans:
-                p.run()
-        st.synchronize()
+            step()
+        torch.cuda.synchronize()
         for _ in range(max(3, steps)):
             flush.zero_()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(st)
-            for p in plans:
-                p.run()
+            step()
             b.record(st)
             st.synchronize()
             ts.append(a.elapsed_time(b))
@@ -1184,7 +1198,8 @@ def long_mix_measure(ctx, args):
     """Config 4, the long/overflow mix: half BLOSUM62 (11/1) and half PSSM (44/4) pairs, targets 1,000-35,000
     residues (10% above 10,000), queries lognormal median 250 (30-2,000), 5% near-identical planted pairs, pairs
     with a length ratio above 4 scored in the band of radius 64 around the planted diagonal (0 when unplanted,
-    src/align.rs:439-447).  One step = both halves' plans.  Cells: m*n for full pairs plus the in-band cells of
+    src/align.rs:439-447).  One step = both halves' plans, in flight together on two streams (two gap settings,
+    two independent batches).  Cells: m*n for full pairs plus the in-band cells of
     banded pairs.  Every score is compared with the CPU oracle's (the scalar band rule for banded pairs, the AVX2
     port for full pairs)."""
     import torch
@@ -1214,7 +1229,7 @@ def long_mix_measure(ctx, args):
         outs.append((d_s, d_k))
         q_base += len(w.rows)
         t_base += len(w.db_offsets) - 1
-    ts = _timed_plans(ctx, plans, args.steps)
+    ts = _timed_plans(ctx, plans, args.steps, concurrent=True)
     stats = [p.stats() for p in plans]
     profiles = [[{"tile": (f"G{sh[0]}xR{sh[1]}xC{sh[2]}" if isinstance(sh, tuple) else sh), "cells": c, "ms": round(t, 3)}
                  for sh, c, t in p.profile()] for p in plans]
