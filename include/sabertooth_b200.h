@@ -82,8 +82,10 @@ int st_profiles_create(st_ctx* ctx, const int32_t* rows, const uint64_t* row_off
 
 /* ---- (G) Smith-Waterman-Gotoh score -------------------------------------- */
 /* Plain per-call drop-in for QueryProfile::sw_score_with (src/simd.rs:252-292)
- * and sw_score (src/simd.rs:245): one host target, one launch, blocking.
- * kernel may be NULL. */
+ * and sw_score (src/simd.rs:245): one host target, blocking (one upload, the
+ * packed 16-bit kernel and the exact 32-bit one on the calling thread's call
+ * slot). Safe to call from many host threads at once on one context: calls
+ * run side by side on their own streams. kernel may be NULL. */
 int st_sw_score(st_ctx* ctx, uint32_t profile, const uint8_t* target, uint32_t n, int32_t open, int32_t ext,
                 int32_t* score, uint32_t* kernel);
 
