@@ -844,7 +844,8 @@ def search_measure(ctx, args):
     same_scores = bool(same and np.array_equal(cpu_scores, gpu_s))
     ctx.free_profiles(ids)
     nq = len(ids)
-    serving = search_serving(ctx, w, params, gaps, rates=(100, 500, 1000, 2000, 3000), seconds=args.serving_seconds,
+    serving = search_serving(ctx, w, params, gaps, rates=(100, 500, 1000, 2000, 3000, 5000, 6500),
+                             seconds=args.serving_seconds,
                              seed=args.seed, batched_qps=nq / (t_pre + t_sw))
     return {"workload": f"config 5 searches: {nq} sequence queries against {len(tlen)} targets ({n_res / 1e6:.0f} M "
                         f"residues), 5 planted homologs per query; seed 111001101, k-mer score 22, cap 512, exact "
