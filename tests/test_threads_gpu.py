@@ -138,3 +138,28 @@ def test_per_call_scores_from_many_threads_at_once(ctx):
     ctx.free_profiles(ids)
     assert not errors, errors
     assert np.array_equal(got, want.astype(np.int64))
+
+
+def test_per_call_score_of_a_profile_created_just_before(ctx):
+    """A per-call score right after the profile it uses is created, round after round on one thread: the
+    call's stream must start after that profile's layouts are built (a call skips that wait only when no
+    profile changed since its call slot's last call).  Each round creates fresh profiles, at once scores one
+    pair of them through st_sw_score, and frees them; every score equals the oracle's.  Rows outside int8
+    and gap costs outside the 16-bit range (both on the 32-bit kernel) alternate with the packed path."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(77)
+    w = W.config3(seed=44, n_queries=6, db_residues=30_000, per_query=10)
+    targets = w.targets()
+    gap_sets = [(44, 4), (11, 1), (20000, 1)]
+    for rnd in range(24):
+        rows = [r if rnd % 2 == 0 else (r * 3).astype(np.int32) for r in w.rows]
+        op, ex = gap_sets[rnd % 3]
+        ids = ctx.create_profiles(rows)
+        k = int(rng.integers(0, w.n_pairs))
+        q, t = int(w.pair_q[k]), int(w.pair_t[k])
+        tt = np.ascontiguousarray(targets[t], dtype=np.uint8)
+        s_, k_ = C.c_int32(), C.c_uint32()
+        check(lib.st_sw_score(ctx.handle, int(ids[q]), tt.ctypes.data, tt.size, op, ex, C.byref(s_), C.byref(k_)))
+        want = O.gotoh_score(rows[q], targets[t], op, ex)
+        ctx.free_profiles(ids)
+        assert s_.value == want, (rnd, q, t, op, ex, s_.value, want)
