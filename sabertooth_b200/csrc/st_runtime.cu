@@ -3023,6 +3023,7 @@ extern "C" int st_sw_score(st_ctx* c, uint32_t profile, const uint8_t* target, u
   } else if (launch && sl->s) {
     cudaStreamSynchronize(sl->s);  // a failed launch phase: let whatever was queued finish before the slot's reuse
     cudaGetLastError();
+    sl->epoch = 0;  // its stream may not have waited for the context stream: the next call waits again
   }
   call_release(c, sl);
   return rc;
