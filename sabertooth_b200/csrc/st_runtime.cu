@@ -834,24 +834,29 @@ extern "C" int st_db_info(st_ctx* c, uint32_t* n_seqs, uint64_t* n_residues) {
 // profiles
 // ---------------------------------------------------------------------------
 // Builds the residue-major int8 and int32 layouts of many profiles from their
-// int32 [m][21] rows: one CTA per profile.
+// [m][21] rows, uploaded as int8 when every score of the profile fits int8 and
+// as int32 otherwise: one CTA per profile.
 struct ProfBuildDesc {
-  uint64_t src_row;  // first row in the uploaded rows
+  uint64_t src;      // first row value: a byte offset into the int8 rows, or an element offset into the int32 rows
   uint64_t o8, o32;  // byte offsets of the int8 / int32 layouts in the block
   uint32_t m, stride8, stride32, fits8;
 };
 
-__global__ void __launch_bounds__(256) build_profiles_kernel(const int32_t* __restrict__ rows,
+__global__ void __launch_bounds__(256) build_profiles_kernel(const int8_t* __restrict__ rows8,
+                                                             const int32_t* __restrict__ rows32,
                                                              const ProfBuildDesc* __restrict__ desc, char* base) {
   const ProfBuildDesc d = desc[blockIdx.x];
-  const int32_t* src = rows + d.src_row * kAlpha;
   int32_t* p32 = reinterpret_cast<int32_t*>(base + d.o32);
   int8_t* p8 = reinterpret_cast<int8_t*>(base + d.o8);
   const uint32_t total = kProfRows * d.stride32;
   for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const uint32_t r = idx / d.stride32;
     const uint32_t i = idx - r * d.stride32;
-    const int32_t v = (i < d.m && r < static_cast<uint32_t>(kAlpha)) ? src[static_cast<size_t>(i) * kAlpha + r] : 0;
+    int32_t v = 0;
+    if (i < d.m && r < static_cast<uint32_t>(kAlpha)) {
+      const size_t at = d.src + static_cast<size_t>(i) * kAlpha + r;
+      v = d.fits8 ? static_cast<int32_t>(rows8[at]) : rows32[at];
+    }
     p32[idx] = v;
     if (i < d.stride8) p8[static_cast<size_t>(r) * d.stride8 + i] = d.fits8 ? static_cast<int8_t>(v) : 0;
   }
@@ -877,7 +882,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   for (uint32_t k = 0; k < n_profiles; ++k) {
     ProfBuildDesc& x = desc[k];
     x.m = static_cast<uint32_t>(row_offsets[k + 1] - row_offsets[k]);
-    x.src_row = row_offsets[k] - row_offsets[0];
+    x.src = (row_offsets[k] - row_offsets[0]) * kAlpha;  // the profile's int8 slot (moved below if it is int32)
     x.stride8 = static_cast<uint32_t>(std::max<size_t>(up16(x.m), 16));
     x.stride32 = static_cast<uint32_t>(std::max<size_t>(up256(x.m), kSw32Rows));
     x.o32 = bytes32;
@@ -888,78 +893,108 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
     bytes8 += up16(static_cast<size_t>(kProfRows) * desc[k].stride8);
   }
   const size_t rows_total = row_offsets[n_profiles] - row_offsets[0];
-  const size_t src_bytes = rows_total * kAlpha * 4;
+  const size_t bytes_r8 = up16(rows_total * kAlpha);  // an int8 slot for every profile's rows
   const size_t desc_bytes = up16(n_profiles * sizeof(ProfBuildDesc));
   // the layouts are built on the side stream, beside kernels already queued on the
   // context's stream; work that reads profiles waits for prof_ev (sync_profiles)
   cudaStream_t bs = nullptr;
   ST_TRY(side_stream(c, &bs));
-  DevMem blk_mem, tmp;  // tmp: uploaded rows and descriptors, back to the pool once the layouts are built
+  // tmp: int8 rows and descriptors; tmp32: int32 rows of the profiles outside int8; both back to the pool
+  // once the layouts are built
+  DevMem blk_mem, tmp, tmp32;
   ST_TRY(pool_get(c, bytes32 + bytes8, blk_mem));
-  ST_TRY(pool_get(c, src_bytes + desc_bytes + 16, tmp));
+  ST_TRY(pool_get(c, bytes_r8 + desc_bytes + 16, tmp));
   struct Back {
     st_ctx* c;
     DevMem* m;
     cudaStream_t s;
     ~Back() { pool_put_after(c, std::move(*m), s); }
-  } back_tmp{c, &tmp, bs};
+  } back_tmp{c, &tmp, bs}, back_tmp32{c, &tmp32, bs};
   if (!c->copy_ev) ST_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
   if (!c->prof_ev) ST_CUDA(cudaEventCreateWithFlags(&c->prof_ev, cudaEventDisableTiming));
   tc.lap("alloc");
   char* base = blk_mem.as<char>();
-  int32_t* d_src = tmp.as<int32_t>();
-  ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + up16(src_bytes));
-  // The rows travel on the copy stream (beside any kernels still queued) while
-  // the host computes their score ranges; the build runs on the side stream
-  // after both. The call returns once the rows and descriptors are on
-  // the device (the caller may reuse them), not when the build is done: later
-  // work on the profiles is ordered after it.
-  // score range of profile k (residues >= 21 score 0); with dst, the rows are copied there in the same pass
-  auto range_of = [&](int64_t k, int32_t* dst) {
-    const uint64_t m = desc[k].m;
-    int32_t lo = 0, hi = 0;
-    const int32_t* r = rows + row_offsets[k] * kAlpha;
-    for (size_t i = 0; i < m * kAlpha; ++i) {
-      const int32_t v = r[i];
-      if (dst) dst[i] = v;
-      lo = std::min(lo, v);
-      hi = std::max(hi, v);
-    }
-    mx[k] = hi;
-    desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
+  int8_t* d_r8 = tmp.as<int8_t>();
+  ProfBuildDesc* d_desc = reinterpret_cast<ProfBuildDesc*>(tmp.as<char>() + bytes_r8);
+  // Host data goes up through the two pinned staging blocks in turn, each uploaded on the copy stream
+  // (beside any kernels still queued) while the next one fills; the build runs on the side stream after the
+  // uploads.  The call returns once everything is on the device (the caller may reuse the rows), not when
+  // the build is done: later work on the profiles is ordered after it.
+  constexpr size_t kChunk = 32ull << 20;
+  int slot = 0;
+  auto stage_slot = [&](size_t bytes, char** h) -> int {
+    Pinned& st = c->prof_stage[slot];
+    if (!c->prof_stage_ev[slot]) ST_CUDA(cudaEventCreateWithFlags(&c->prof_stage_ev[slot], cudaEventDisableTiming));
+    if (c->prof_stage_used[slot]) ST_CUDA(cudaEventSynchronize(c->prof_stage_ev[slot]));
+    ST_TRY(st.reserve(std::max(bytes, kChunk)));
+    *h = st.as<char>();
+    return ST_OK;
   };
-  if (src_bytes && host_pinned(rows)) {
-    ST_CUDA(cudaMemcpyAsync(d_src, rows + row_offsets[0] * kAlpha, src_bytes, cudaMemcpyHostToDevice, c->copy));
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) range_of(k, nullptr);
-  } else if (src_bytes) {
-    // pageable rows: copied (with the range pass) into two pinned blocks in
-    // turn, each uploaded while the next fills
-    constexpr size_t kChunk = 32ull << 20;
-    uint32_t k0 = 0;
-    int slot = 0;
-    while (k0 < n_profiles) {
-      uint32_t k1 = k0 + 1;
-      while (k1 < n_profiles && (row_offsets[k1 + 1] - row_offsets[k0]) * kAlpha * 4 <= kChunk) ++k1;
-      const size_t r0 = row_offsets[k0] - row_offsets[0];
-      const size_t bytes = (row_offsets[k1] - row_offsets[k0]) * kAlpha * 4;
-      Pinned& st = c->prof_stage[slot];
-      if (!c->prof_stage_ev[slot]) ST_CUDA(cudaEventCreateWithFlags(&c->prof_stage_ev[slot], cudaEventDisableTiming));
-      if (c->prof_stage_used[slot]) ST_CUDA(cudaEventSynchronize(c->prof_stage_ev[slot]));
-      ST_TRY(st.reserve(std::max(bytes, kChunk)));
-      int32_t* h = st.as<int32_t>();
+  auto stage_send = [&](void* dst, size_t bytes) -> int {
+    ST_CUDA(cudaMemcpyAsync(dst, c->prof_stage[slot].p, bytes, cudaMemcpyHostToDevice, c->copy));
+    ST_CUDA(cudaEventRecord(c->prof_stage_ev[slot], c->copy));
+    c->prof_stage_used[slot] = true;
+    slot ^= 1;
+    return ST_OK;
+  };
+  // 1. every profile's rows as int8 (a quarter of the bytes), its score range found in the same pass:
+  // residues >= 21 score 0, so the range starts at 0; a profile with a score outside int8 leaves its slot
+  // unused and goes up as int32 below
+  uint32_t k0 = 0;
+  while (k0 < n_profiles) {
+    uint32_t k1 = k0 + 1;
+    while (k1 < n_profiles && (row_offsets[k1 + 1] - row_offsets[k0]) * kAlpha <= kChunk) ++k1;
+    const size_t bytes = (row_offsets[k1] - row_offsets[k0]) * kAlpha;
+    char* h = nullptr;
+    ST_TRY(stage_slot(bytes, &h));
 #pragma omp parallel for schedule(dynamic, 4)
-      for (int64_t k = k0; k < static_cast<int64_t>(k1); ++k)
-        range_of(k, h + (row_offsets[k] - row_offsets[k0]) * kAlpha);
-      ST_CUDA(cudaMemcpyAsync(d_src + r0 * kAlpha, h, bytes, cudaMemcpyHostToDevice, c->copy));
-      ST_CUDA(cudaEventRecord(c->prof_stage_ev[slot], c->copy));
-      c->prof_stage_used[slot] = true;
-      slot ^= 1;
-      k0 = k1;
+    for (int64_t k = k0; k < static_cast<int64_t>(k1); ++k) {
+      const size_t cnt = static_cast<size_t>(desc[k].m) * kAlpha;
+      const int32_t* r = rows + row_offsets[k] * kAlpha;
+      int8_t* d8 = reinterpret_cast<int8_t*>(h) + (row_offsets[k] - row_offsets[k0]) * kAlpha;
+      int32_t lo = 0, hi = 0;
+      for (size_t i = 0; i < cnt; ++i) {
+        const int32_t v = r[i];
+        d8[i] = static_cast<int8_t>(v);
+        lo = std::min(lo, v);
+        hi = std::max(hi, v);
+      }
+      mx[k] = hi;
+      desc[k].fits8 = (lo >= -128 && hi <= 127) ? 1u : 0u;
     }
-  } else {
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int64_t k = 0; k < static_cast<int64_t>(n_profiles); ++k) range_of(k, nullptr);
+    if (bytes) ST_TRY(stage_send(d_r8 + (row_offsets[k0] - row_offsets[0]) * kAlpha, bytes));
+    k0 = k1;
+  }
+  // 2. the profiles outside int8, as int32
+  std::vector<uint32_t> wide;
+  size_t wide_rows = 0;
+  for (uint32_t k = 0; k < n_profiles; ++k)
+    if (!desc[k].fits8) {
+      desc[k].src = wide_rows * kAlpha;
+      wide_rows += desc[k].m;
+      wide.push_back(k);
+    }
+  int32_t* d_r32 = nullptr;
+  if (wide_rows) {
+    ST_TRY(pool_get(c, wide_rows * kAlpha * 4, tmp32));
+    d_r32 = tmp32.as<int32_t>();
+    size_t w0 = 0;
+    while (w0 < wide.size()) {
+      size_t w1 = w0 + 1, bytes = static_cast<size_t>(desc[wide[w0]].m) * kAlpha * 4;
+      while (w1 < wide.size() && bytes + static_cast<size_t>(desc[wide[w1]].m) * kAlpha * 4 <= kChunk)
+        bytes += static_cast<size_t>(desc[wide[w1++]].m) * kAlpha * 4;
+      char* h = nullptr;
+      ST_TRY(stage_slot(bytes, &h));
+      const uint64_t e0 = desc[wide[w0]].src;
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int64_t j = static_cast<int64_t>(w0); j < static_cast<int64_t>(w1); ++j) {
+        const uint32_t k = wide[j];
+        memcpy(reinterpret_cast<int32_t*>(h) + (desc[k].src - e0), rows + row_offsets[k] * kAlpha,
+               static_cast<size_t>(desc[k].m) * kAlpha * 4);
+      }
+      ST_TRY(stage_send(d_r32 + e0, bytes));
+      w0 = w1;
+    }
   }
   tc.lap("range");
   ST_TRY(c->prof_desc.reserve(n_profiles * sizeof(ProfBuildDesc)));
@@ -967,7 +1002,7 @@ extern "C" int st_profiles_create(st_ctx* c, const int32_t* rows, const uint64_t
   ST_CUDA(cudaMemcpyAsync(d_desc, c->prof_desc.p, n_profiles * sizeof(ProfBuildDesc), cudaMemcpyHostToDevice, c->copy));
   ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
   ST_CUDA(cudaStreamWaitEvent(bs, c->copy_ev, 0));
-  build_profiles_kernel<<<n_profiles, 256, 0, bs>>>(d_src, d_desc, base);
+  build_profiles_kernel<<<n_profiles, 256, 0, bs>>>(d_r8, d_r32, d_desc, base);
   ++c->launches;
   ST_CUDA(cudaGetLastError());
   ST_CUDA(cudaEventRecord(c->prof_ev, bs));
