@@ -1180,10 +1180,17 @@ def exhaustive_measure(ctx, args):
     plan.close()
     got = d_s.cpu().numpy()
     kern = d_k.cpu().numpy()
-    # end to end once: host pairs in, scores out (profiles resident)
-    t0 = time.perf_counter()
+    # end to end: host pairs in, scores out (profiles resident); one untimed call (its staging blocks and
+    # device arenas are allocated there), then the median of three
     e2e = ctx.sw_score_pairs(pairs, gaps)
-    t_e2e = time.perf_counter() - t0
+    e2e_ok = True
+    e2e_t = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        e2e_run = ctx.sw_score_pairs(pairs, gaps)
+        e2e_t.append(time.perf_counter() - t0)
+        e2e_ok &= bool(np.array_equal(e2e_run, e2e))
+    t_e2e = float(np.median(e2e_t))
     ctx.free_profiles(ids)
     cells = w.cells()
     t0 = time.perf_counter()
@@ -1194,9 +1201,11 @@ def exhaustive_measure(ctx, args):
                         f"({w.n_pairs:,} pairs, exhaustive), gaps 11/1",
             "cells": int(cells), "ms_per_step": round(ms, 3), "gcups": round(cells / (ms * 1e-3) / 1e9, 1),
             "e2e_gcups": round(cells / t_e2e / 1e9, 1), "e2e_how": "one st_sw_score_pairs call: host pairs in, "
-                                                                 "scores out, profiles and database resident",
+                                                                 "scores out, profiles and database resident; "
+                                                                 "median of three calls after an untimed one",
             "rescored_pairs": int(stats["rescored_pairs"]), "gpu32_pairs": int((kern == 2).sum()),
-            "matches_cpu_baseline": bool(np.array_equal(got, want)), "e2e_matches": bool(np.array_equal(e2e, want)),
+            "matches_cpu_baseline": bool(np.array_equal(got, want)),
+            "e2e_matches": bool(np.array_equal(e2e, want)) and e2e_ok,
             "cpu_baseline": {"value": round(cells / t_cpu / 1e9, 2), "unit": UNIT, "cores": os.cpu_count(),
                              "kind": "port", "sample": "the whole workload once: the reference's default AVX2 path "
                                                        "(u8 -> i16 striped -> scalar) restated in C"},

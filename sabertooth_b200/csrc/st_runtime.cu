@@ -2036,6 +2036,8 @@ static int bits_for(uint64_t x) {
 // context's stream, with one synchronisation to read the per-class totals
 // that size the rest. `work` holds the per-pair and per-query buffers and
 // must outlive the plan's runs; the plan owns the task arrays and scratch.
+static int upload_host(st_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open, int32_t ext, int32_t* d_scores,
                        uint32_t* d_kernels, uint32_t max_len, uint32_t max_m, DevMem& work, st_plan** out) {
   cudaStream_t st = c->stream;
@@ -2163,7 +2165,8 @@ static int dplan_build(st_ctx* c, const st_pair* pairs, uint64_t n, int32_t open
       hf[k] = pm.live && pm.fits8 ? 1 : 0;
     }
   }
-  ST_CUDA(cudaMemcpyAsync(b + o_pairs, pairs, n * 16, cudaMemcpyHostToDevice, c->copy));
+  // the pairs: straight from pinned memory, through the pinned staging blocks from pageable memory
+  ST_TRY(upload_host(c, b + o_pairs, pairs, n * 16, s1));
   ST_CUDA(cudaMemcpyAsync(b + o_sq, c->plan_meta.p, np1 * 4, cudaMemcpyHostToDevice, c->copy));
   ST_CUDA(cudaMemcpyAsync(b + o_sf, c->plan_meta.as<uint8_t>(np1 * 4), np1, cudaMemcpyHostToDevice, c->copy));
   ST_CUDA(cudaEventRecord(c->copy_ev, c->copy));
