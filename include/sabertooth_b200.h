@@ -76,7 +76,8 @@ int st_profiles_free(st_ctx* ctx, const uint32_t* ids, uint32_t n);
 /* Batch form: n_profiles profiles from one rows arena; row_offsets[k]..row_offsets[k+1]
  * are the rows of profile k; ids written to ids[0..n_profiles).  Returns once
  * the rows are on the device (they may be reused); the device layouts are built
- * on the context's stream, before any later work that uses them. */
+ * on the context's stream, before any later work that uses them.  The rows of a
+ * profile whose scores all fit int8 travel to the device as int8. */
 int st_profiles_create(st_ctx* ctx, const int32_t* rows, const uint64_t* row_offsets, uint32_t n_profiles,
                        uint32_t* ids);
 
